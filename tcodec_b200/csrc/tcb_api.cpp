@@ -1,0 +1,93 @@
+// tcb_api.cpp — utility entry points of include/tcodec.h (reference
+// src/tcodec.c:12-98, src/frame.c:12-89) and host frame buffers.
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <cuda_runtime.h>
+
+#include "../../include/tcodec.h"
+#include "tcb_encoder.h"
+
+extern "C" {
+
+// Host frame with 64-byte aligned strides (reference src/frame.c:19-43).
+// Pinned frames are used for the per-frame reconstruction copy.
+tc_frame_buf_t *tcb_host_frame_alloc(int width, int height, int pinned) {
+    tc_frame_buf_t *f = (tc_frame_buf_t *)calloc(1, sizeof(tc_frame_buf_t));
+    if (!f) return nullptr;
+    f->width = width;
+    f->height = height;
+    f->stride_y = ((width + 63) / 64) * 64;
+    f->stride_c = ((width / 2 + 63) / 64) * 64;
+    f->qp_avg = TC_QP_DEFAULT;
+    f->owned = pinned ? 2 : 1;
+    const size_t ys = (size_t)f->stride_y * height, cs = (size_t)f->stride_c * (height / 2);
+    if (pinned) {
+        if (cudaMallocHost(&f->y, ys ? ys : 1) != cudaSuccess || cudaMallocHost(&f->cb, cs ? cs : 1) != cudaSuccess ||
+            cudaMallocHost(&f->cr, cs ? cs : 1) != cudaSuccess) {
+            tcb_host_frame_free(f);
+            return nullptr;
+        }
+        memset(f->y, 0, ys); memset(f->cb, 0, cs); memset(f->cr, 0, cs);
+    } else {
+        f->y = (tc_pixel_t *)calloc(ys ? ys : 1, 1);
+        f->cb = (tc_pixel_t *)calloc(cs ? cs : 1, 1);
+        f->cr = (tc_pixel_t *)calloc(cs ? cs : 1, 1);
+        if (!f->y || !f->cb || !f->cr) { tcb_host_frame_free(f); return nullptr; }
+    }
+    return f;
+}
+
+void tcb_host_frame_free(tc_frame_buf_t *f) {
+    if (!f) return;
+    if (f->owned == 2) { cudaFreeHost(f->y); cudaFreeHost(f->cb); cudaFreeHost(f->cr); }
+    else if (f->owned == 1) { free(f->y); free(f->cb); free(f->cr); }
+    free(f);
+}
+
+const char *tc_error_string(tc_error_t err) {
+    switch (err) {
+        case TC_OK: return "OK";
+        case TC_ERR_MEMORY: return "Out of memory";
+        case TC_ERR_PARAM: return "Invalid parameter";
+        case TC_ERR_BITSTREAM: return "Bitstream error";
+        case TC_ERR_EOF: return "End of bitstream";
+        case TC_ERR_INTERNAL: return "Internal error";
+        default: return "Unknown error";
+    }
+}
+
+int tc_version(void) { return TCODEC_VERSION_INT; }
+const char *tc_version_string(void) { return TCODEC_VERSION_STRING; }
+
+void tc_config_defaults(tc_config_t *cfg, int32_t width, int32_t height) {
+    if (!cfg) return;
+    memset(cfg, 0, sizeof(*cfg));
+    cfg->width = width;
+    cfg->height = height;
+    cfg->preset = TC_PRESET_MEDIUM;
+    cfg->rc_method = TC_RC_CQP;
+    cfg->qp = TC_QP_DEFAULT;
+    cfg->fps_num = 60;
+    cfg->fps_den = 1;
+    cfg->keyframe_interval = 30;
+    cfg->bitstream_version = TC_VERSION_V1;
+    cfg->profile = TC_PROFILE_BASELINE_MOBILE;
+    cfg->level_idx = TC_LEVEL_AUTO;
+}
+
+double tc_psnr(const tc_pixel_t *a, int stride_a, const tc_pixel_t *b, int stride_b, int width,
+               int height) {
+    int64_t sse = 0;
+    for (int y = 0; y < height; ++y)
+        for (int x = 0; x < width; ++x) {
+            const int d = (int)a[(size_t)y * stride_a + x] - (int)b[(size_t)y * stride_b + x];
+            sse += d * d;
+        }
+    if (sse == 0) return 100.0;
+    const double mse = (double)sse / ((double)width * (double)height);
+    return 10.0 * log10(255.0 * 255.0 / mse);
+}
+
+}  // extern "C"

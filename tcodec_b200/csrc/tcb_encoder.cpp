@@ -1,0 +1,572 @@
+// tcb_encoder.cpp — tc_encoder_* (reference include/tcodec.h:27-57) on the
+// B200 pixel pipeline.
+//
+// Host responsibilities per frame (reference src/encoder.c:2625-3121
+// encode_poc_frame): frame type (key interval, scene cut on a device
+// histogram, B-frame schedule), QP / rate control, header and tool flags,
+// DPB bookkeeping, entropy coding of the device's CTU records, entry-point
+// tables and CRC.  Device responsibilities: everything that touches pixels.
+// Frames stay resident in HBM: the DPB is a ring of device frame buffers
+// and only the packet, the CTU records and the host copy of the
+// reconstruction (API contract: encoder->recon) come back each frame.
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/tcodec.h"
+#include "tcb_encoder.h"
+#include "tcb_entropy.h"
+#include "tcb_launch.h"
+
+using namespace tcb;
+
+namespace {
+
+int qscale(int qp) {
+    static const int t[64] = TCB_QSCALE_INIT;
+    return t[qp < 0 ? 0 : (qp > 63 ? 63 : qp)];
+}
+int jnd(int band) {
+    static const int t[4] = TCB_JND_INIT;
+    return t[band < 0 ? 0 : (band > 3 ? 3 : band)];
+}
+// Effective quant step (reference tcodec_common.h:226-230).
+int eff_scale(int qp, int band) {
+    const int e = (qscale(qp) * jnd(band) + 4) >> 3;
+    return e < 1 ? 1 : e;
+}
+
+// Rate control: CQP keeps the configured QP; CBR/VBR steer QP through the
+// logistic rho(QP) model and a one-second budget buffer (reference
+// src/ratectl.c:20-156).
+double rho_from_qp(int qp) { return 1.0 / (1.0 + exp(-((double)qp - 28.0) / 8.0)); }
+int qp_from_rho(double r) {
+    if (r <= 0.01) return 0;
+    if (r >= 0.99) return 63;
+    const double q = 28.0 + 8.0 * log(r / (1.0 - r));
+    return clampi((int)(q + 0.5), 0, 63);
+}
+
+}  // namespace
+
+void EncImpl::rc_init(const tc_config_t &c) {
+    rc_method = c.rc_method;
+    rc_qp = clampi(c.qp, 0, 63);
+    rc_base_qp = rc_qp;
+    const int fn = c.fps_num > 0 ? c.fps_num : 60, fd = c.fps_den > 0 ? c.fps_den : 1;
+    const double fps = (double)fn / (double)fd;
+    rc_frame_target = (c.target_bitrate > 0 && fps > 0) ? (long long)((double)c.target_bitrate / fps) : 0;
+    rc_buffer_size = (double)c.target_bitrate;
+    rc_buffer_level = 0.5;
+}
+
+void EncImpl::rc_frame_start() {
+    if (rc_method == TC_RC_CQP) { rc_qp = rc_base_qp; return; }
+    if (rc_method == TC_RC_CBR || rc_method == TC_RC_VBR) {
+        const double f = rc_buffer_level;
+        double adj = 0.0;
+        if (f > 0.8) adj = -2.0;
+        else if (f > 0.6) adj = -1.0;
+        else if (f < 0.2) adj = 2.0;
+        else if (f < 0.4) adj = 1.0;
+        double t = rho_from_qp(rc_qp) + adj * 0.05;
+        t = t < 0.05 ? 0.05 : (t > 0.95 ? 0.95 : t);
+        rc_qp = qp_from_rho(t);
+    }
+}
+
+void EncImpl::rc_frame_end(long long bits) {
+    if (rc_buffer_size > 0) {
+        rc_buffer_level += ((double)rc_frame_target - (double)bits) / rc_buffer_size;
+        rc_buffer_level = rc_buffer_level < 0.0 ? 0.0 : (rc_buffer_level > 1.0 ? 1.0 : rc_buffer_level);
+    }
+}
+
+#define CK(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { last_cuda_error = _e; return false; } } while (0)
+
+bool EncImpl::init(const tc_config_t &c) {
+    cfg = c;
+    W = c.width; H = c.height;
+    sy = ((W + 63) / 64) * 64;
+    sc = ((W / 2 + 63) / 64) * 64;
+    ctu_cols = (W + 63) / 64;
+    ctu_rows = (H + 63) / 64;
+    grid_w = (W + 7) / 8;
+    grid_h = (H + 7) / 8;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return false;
+    CK(cudaGetDevice(&device));
+    CK(init_device_tables());
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    const size_t ybytes = (size_t)sy * H + 64, cbytes = (size_t)sc * (H / 2) + 64;
+    for (int i = 0; i < NPOOL; ++i) {
+        CK(cudaMalloc(&pool[i].y, ybytes));
+        CK(cudaMalloc(&pool[i].cb, cbytes));
+        CK(cudaMalloc(&pool[i].cr, cbytes));
+        CK(cudaMemset(pool[i].y, 0, ybytes));
+        CK(cudaMemset(pool[i].cb, 0, cbytes));
+        CK(cudaMemset(pool[i].cr, 0, cbytes));
+    }
+    CK(cudaMalloc(&cur.y, ybytes));
+    CK(cudaMalloc(&cur.cb, cbytes));
+    CK(cudaMalloc(&cur.cr, cbytes));
+    CK(cudaMemset(cur.y, 0, ybytes));
+    CK(cudaMemset(cur.cb, 0, cbytes));
+    CK(cudaMemset(cur.cr, 0, cbytes));
+    for (int i = 0; i < 2; ++i) {
+        CK(cudaMalloc(&grid[i], sizeof(MvCell) * grid_w * grid_h));
+        std::vector<MvCell> init(grid_w * grid_h);
+        for (auto &g : init) { g.dx = 0; g.dy = 0; g.intra = 1; g.pad = 0; }
+        CK(cudaMemcpy(grid[i], init.data(), sizeof(MvCell) * init.size(), cudaMemcpyHostToDevice));
+    }
+    const int nctu = ctu_cols * ctu_rows;
+    CK(cudaMalloc(&d_out, sizeof(CtuOut) * nctu));
+    CK(cudaMallocHost(&h_out, sizeof(CtuOut) * nctu));
+    CK(cudaMalloc(&d_params, sizeof(FrameParams)));
+    CK(cudaMalloc(&d_hist, 16 * sizeof(int)));
+    CK(cudaMallocHost(&h_hist, 16 * sizeof(int)));
+    CK(cudaMalloc(&d_sse, sizeof(unsigned long long)));
+    CK(cudaMallocHost(&h_sse, sizeof(unsigned long long)));
+    CK(cudaMalloc(&d_err, sizeof(int)));
+    CK(cudaMemset(d_err, 0, sizeof(int)));
+    // Anti-diagonal wavefront item lists.
+    std::vector<int> items;
+    for (int d = 0; d < ctu_rows + ctu_cols - 1; ++d) {
+        diag_off.push_back((int)items.size());
+        for (int r = 0; r < ctu_rows; ++r) {
+            const int col = d - r;
+            if (col >= 0 && col < ctu_cols) items.push_back((r << 10) | col);
+        }
+        diag_cnt.push_back((int)items.size() - diag_off.back());
+    }
+    CK(cudaMalloc(&d_items, sizeof(int) * items.size()));
+    CK(cudaMemcpy(d_items, items.data(), sizeof(int) * items.size(), cudaMemcpyHostToDevice));
+    for (int i = 0; i < TC_REF_FRAMES; ++i) { dpb_slot[i] = -1; dpb_poc[i] = -1; }
+    out_buf_size = (size_t)W * H * 3;
+    out_buf = (uint8_t *)calloc(out_buf_size, 1);
+    if (!out_buf) return false;
+    rc_init(c);
+    bf_b_mode = c.enable_b_frames ? 1 : 0;
+    return true;
+}
+
+void EncImpl::release() {
+    if (st) cudaStreamSynchronize(st);
+    for (int i = 0; i < NPOOL; ++i) { cudaFree(pool[i].y); cudaFree(pool[i].cb); cudaFree(pool[i].cr); }
+    cudaFree(cur.y); cudaFree(cur.cb); cudaFree(cur.cr);
+    cudaFree(grid[0]); cudaFree(grid[1]);
+    cudaFree(d_out); cudaFreeHost(h_out);
+    cudaFree(d_params); cudaFree(d_hist); cudaFreeHost(h_hist);
+    cudaFree(d_sse); cudaFreeHost(h_sse); cudaFree(d_err); cudaFree(d_items);
+    for (auto &f : bf_frames) { cudaFree(f.y); cudaFree(f.cb); cudaFree(f.cr); }
+    bf_frames.clear();
+    if (st) cudaStreamDestroy(st);
+    free(out_buf);
+}
+
+int EncImpl::free_pool_slot() const {
+    for (int i = 0; i < NPOOL; ++i) {
+        bool used = false;
+        for (int k = 0; k < TC_REF_FRAMES; ++k) used |= dpb_slot[k] == i;
+        if (!used) return i;
+    }
+    return -1;
+}
+
+bool EncImpl::upload(const tc_pixel_t *y, int ys, const tc_pixel_t *cb, int cbs, const tc_pixel_t *cr,
+                     int crs, const DevFrame &dst) {
+    CK(cudaMemcpy2DAsync(dst.y, sy, y, ys, W, H, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpy2DAsync(dst.cb, sc, cb, cbs, W / 2, H / 2, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpy2DAsync(dst.cr, sc, cr, crs, W / 2, H / 2, cudaMemcpyHostToDevice, st));
+    return true;
+}
+
+// Device-side copy of a frame (B-frame reorder buffer <-> working input).
+bool EncImpl::dcopy(const DevFrame &dst, const DevFrame &src) {
+    CK(cudaMemcpy2DAsync(dst.y, sy, src.y, sy, W, H, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpy2DAsync(dst.cb, sc, src.cb, sc, W / 2, H / 2, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpy2DAsync(dst.cr, sc, src.cr, sc, W / 2, H / 2, cudaMemcpyDeviceToDevice, st));
+    return true;
+}
+
+tc_error_t EncImpl::encode_poc_frame(int poc, int b_layer_qp_off, tc_packet_t *pkt) {
+    // ---- frame type ----------------------------------------------------
+    const int kint = cfg.keyframe_interval > 0 ? cfg.keyframe_interval : 30;
+    int is_key;
+    if (bf_b_mode) {
+        is_key = force_keyframe || poc == 0 || (poc % kint == 0);
+    } else {
+        is_key = force_keyframe || frame_count == 0;
+        if (!is_key && frame_count % kint == 0) is_key = 1;
+        if (!is_key && frame_count > 0) {
+            if (launch_hist16(cur.y, W, H, sy, d_hist, st) != cudaSuccess) return TC_ERR_INTERNAL;
+            if (cudaMemcpyAsync(h_hist, d_hist, 16 * sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                return TC_ERR_INTERNAL;
+            if (prev_hist_valid) {
+                double dist = 0.0;
+                const double total = (double)W * H;
+                for (int i = 0; i < 16; ++i) {
+                    const double expected = (prev_hist[i] + h_hist[i]) / 2.0;
+                    if (expected > 0) {
+                        const double diff = (double)h_hist[i] - (double)prev_hist[i];
+                        dist += (diff * diff) / expected;
+                    }
+                }
+                if (dist / total > 0.5) is_key = 1;
+            }
+            memcpy(prev_hist, h_hist, sizeof(prev_hist));
+            prev_hist_valid = 1;
+        }
+    }
+    force_keyframe = 0;
+    const int frame_type = is_key ? 0 : (b_layer_qp_off > 0 ? 2 : 1);
+    rc_frame_start();
+    int qp = rc_qp;
+    if (frame_type == 2) qp = clampi(qp + b_layer_qp_off, 0, 63);
+
+    // ---- header fields ---------------------------------------------------
+    memset(out_buf, 0, out_buf_size);
+    BitWriter bw;
+    bw.init(out_buf, out_buf_size);
+    int profile = cfg.profile, level = cfg.level_idx;
+    if (profile > TC_PROFILE_MAX) profile = TC_PROFILE_BASELINE_MOBILE;
+    if (level > TC_LEVEL_MAX) level = TC_LEVEL_AUTO;
+    uint8_t flags = is_key ? TC_FLAG_KEY_FRAME : 0;
+    if (is_key) flags |= TC_FLAG_RAP;
+    if (cfg.enable_crc) flags |= TC_FLAG_CRC;
+    uint16_t tools = TC_TOOL_SKIP_MERGE | TC_TOOL_CFL_CHROMA | TC_TOOL_JND_WEIGHTING |
+                     TC_TOOL_MEDIAN_MV_PRED | TC_TOOL_SIX_TAP_INTERP;
+    if ((cfg.preset == TC_PRESET_SLOW || cfg.preset >= TC_PRESET_MEDIUM) && profile >= TC_PROFILE_STREAMING_MAIN)
+        tools |= TC_TOOL_MULTI_REF;
+    if (cfg.enable_entropy_coded) tools |= TC_TOOL_ENTROPY_CODED;
+    if (frame_type == 2) tools |= TC_TOOL_BIPRED;
+    tools |= TC_TOOL_SAO;
+    if (cfg.preset >= TC_PRESET_MEDIUM) tools |= TC_TOOL_FRESH_SKIP;
+    const int use_ep = !prev_v2_valid || prev_v2_rowbytes >= 256;
+    if (use_ep) tools |= TC_TOOL_ENTRY_POINTS;
+    if (bf_b_mode) flags |= TC_FLAG_EXT_HEADER;
+    // write_frame_header (reference src/encoder.c:2365-2399)
+    bw.put_bits(TC_MAGIC_0, 8); bw.put_bits(TC_MAGIC_1, 8); bw.put_bits(TC_MAGIC_2, 8);
+    bw.put_bits(TC_VERSION_V2, 8);
+    bw.put_bits((uint32_t)(uint16_t)W, 16); bw.put_bits((uint32_t)(uint16_t)H, 16);
+    bw.put_bits(flags, 8);
+    bw.put_bits((uint8_t)(int8_t)(qp - TC_QP_DEFAULT), 8);
+    bw.put_bits((uint8_t)(poc & 0xFF), 8);
+    bw.put_bits((uint8_t)((profile << 4) | (level & 0x0F)), 8);
+    bw.put_bits(tools, 16);
+    if (bf_b_mode) bw.put_bits(frame_type == 0 ? 0 : (frame_type == 2 ? 2 : 1), 8);
+    bw.align();
+
+    if (is_key && poc > 0) {
+        for (int i = 0; i < TC_REF_FRAMES; ++i) { dpb_slot[i] = -1; dpb_poc[i] = -1; }
+    }
+
+    // ---- device frame parameters ------------------------------------------
+    const int rs = free_pool_slot();
+    if (rs < 0) return TC_ERR_INTERNAL;
+    const DevFrame rec = pool[rs];
+    FrameParams &P = h_params;
+    memset(&P, 0, sizeof(P));
+    P.W = W; P.H = H; P.stride_y = sy; P.stride_c = sc;
+    P.ctu_cols = ctu_cols; P.ctu_rows = ctu_rows; P.grid_w = grid_w; P.grid_h = grid_h;
+    P.cur_y = cur.y; P.cur_cb = cur.cb; P.cur_cr = cur.cr;
+    P.rec_y = rec.y; P.rec_cb = rec.cb; P.rec_cr = rec.cr;
+    for (int i = 0; i < MAX_REFS; ++i) {
+        const int s = dpb_slot[i];
+        P.ref_valid[i] = s >= 0;
+        P.ref_poc[i] = dpb_poc[i];
+        const DevFrame &f = s >= 0 ? pool[s] : pool[rs];
+        P.ref_y[i] = f.y; P.ref_cb[i] = f.cb; P.ref_cr[i] = f.cr;
+    }
+    P.prev_grid = grid[1 - grid_cur];
+    P.cur_grid = grid[grid_cur];
+    P.out = d_out;
+    P.frame_type = frame_type;
+    P.poc = poc;
+    P.qp = qp;
+    P.qp_c = clampi(qp + 1, 0, 63);
+    P.preset = cfg.preset;
+    P.multiref = cfg.preset >= TC_PRESET_MEDIUM && profile >= TC_PROFILE_STREAMING_MAIN && frame_type == 1;
+    P.fresh_skip = cfg.preset >= TC_PRESET_MEDIUM;
+    P.prev_valid = prev_mv_valid;
+    P.glob_valid = 0;
+    long long lam = tc_lambda_host(qp);
+    if (frame_type == 0) lam = (lam * 3) / 4;
+    P.lambda = lam;
+    P.lambda_c = tc_lambda_host(P.qp_c);
+    P.lambda_sao = tc_lambda_host(qp);
+    for (int b = 0; b < 4; ++b) {
+        P.eff_l[b] = eff_scale(qp, b); P.rcp_l[b] = quant_rcp(P.eff_l[b]);
+        P.eff_c[b] = eff_scale(P.qp_c, b); P.rcp_c[b] = quant_rcp(P.eff_c[b]);
+    }
+    P.err = d_err;
+    if (cudaMemcpyAsync(d_params, &P, sizeof(P), cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return TC_ERR_INTERNAL;
+    if (frame_type == 1 && P.ref_valid[0]) {
+        if (launch_glob_mv(cur.y, P.ref_y[0], W, H, sy, d_params, st) != cudaSuccess) return TC_ERR_INTERNAL;
+    }
+    for (size_t d = 0; d < diag_off.size(); ++d)
+        if (launch_ctu_items(d_params, d_items + diag_off[d], diag_cnt[d], st) != cudaSuccess)
+            return TC_ERR_INTERNAL;
+    const int nctu = ctu_cols * ctu_rows;
+    if (cudaMemcpyAsync(h_out, d_out, sizeof(CtuOut) * nctu, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return TC_ERR_INTERNAL;
+    if (launch_frame_sse(cur.y, rec.y, W, H, sy, d_sse, st) != cudaSuccess) return TC_ERR_INTERNAL;
+    if (cudaMemcpyAsync(h_sse, d_sse, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return TC_ERR_INTERNAL;
+    if (recon_host) {
+        if (cudaMemcpy2DAsync(recon_host->y, recon_host->stride_y, rec.y, sy, W, H, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaMemcpy2DAsync(recon_host->cb, recon_host->stride_c, rec.cb, sc, W / 2, H / 2, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaMemcpy2DAsync(recon_host->cr, recon_host->stride_c, rec.cr, sc, W / 2, H / 2, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+            return TC_ERR_INTERNAL;
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) return TC_ERR_INTERNAL;
+
+    // ---- entropy coding of the CTU records ------------------------------
+    const int entropy = cfg.enable_entropy_coded ? 1 : 0;
+    const int multiref = P.multiref;
+    if (use_ep) {
+        const int nrows = ctu_rows;
+        bw.put_bits((uint32_t)nrows, 16);
+        const size_t ep_table = bw.byte_pos;
+        for (int i = 0; i < nrows; ++i) bw.put_bits(0, 32);
+        bw.align();
+        const size_t ep_payload = bw.byte_pos;
+        const size_t per_row = out_buf_size / (size_t)(nrows > 1 ? nrows : 1) + 1024;
+        if (nrows > 64) return TC_ERR_MEMORY;
+        std::vector<uint8_t> rbuf(per_row);
+        uint32_t row_off[64];
+        for (int r = 0; r < nrows; ++r) {
+            std::fill(rbuf.begin(), rbuf.end(), 0);
+            BitWriter rw;
+            rw.init(rbuf.data(), per_row);
+            RangeEncoder rc;
+            uint8_t ctx[TC_NUM_CONTEXTS_RC];
+            memset(ctx, 0, sizeof(ctx));
+            rc.init(&rw);
+            SyntaxSink sink{&rw, entropy ? &rc : nullptr, ctx};
+            for (int c = 0; c < ctu_cols; ++c) {
+                const CtuGeom g{c * 64, r * 64, W, H, frame_type, multiref};
+                write_ctu_syntax(sink, h_out[r * ctu_cols + c], g);
+            }
+            if (entropy) rc.flush();
+            rw.align();
+            if (rw.overflow) return TC_ERR_MEMORY;
+            const size_t rb = rw.bytes();
+            if (rb > per_row || bw.byte_pos + rb > out_buf_size) return TC_ERR_MEMORY;
+            row_off[r] = (uint32_t)(bw.byte_pos - ep_payload);
+            memcpy(out_buf + bw.byte_pos, rbuf.data(), rb);
+            bw.byte_pos += rb;
+        }
+        for (int i = 0; i < nrows; ++i) {
+            uint8_t *p = out_buf + ep_table + (size_t)i * 4;
+            p[0] = (uint8_t)(row_off[i] >> 24); p[1] = (uint8_t)(row_off[i] >> 16);
+            p[2] = (uint8_t)(row_off[i] >> 8);  p[3] = (uint8_t)row_off[i];
+        }
+    } else {
+        RangeEncoder rc;
+        uint8_t ctx[TC_NUM_CONTEXTS_RC];
+        memset(ctx, 0, sizeof(ctx));
+        rc.init(&bw);
+        SyntaxSink sink{&bw, entropy ? &rc : nullptr, ctx};
+        for (int r = 0; r < ctu_rows; ++r)
+            for (int c = 0; c < ctu_cols; ++c) {
+                const CtuGeom g{c * 64, r * 64, W, H, frame_type, multiref};
+                write_ctu_syntax(sink, h_out[r * ctu_cols + c], g);
+            }
+        if (entropy) rc.flush();
+        bw.align();
+    }
+    if (cfg.enable_crc) {
+        const size_t n = bw.bytes();
+        const uint16_t crc = crc16_ccitt(out_buf, n);
+        bw.put_bits(crc >> 8, 8);
+        bw.put_bits(crc & 0xFF, 8);
+    }
+    if (bw.overflow) return TC_ERR_MEMORY;
+    const size_t frame_bytes = bw.bytes();
+    rc_frame_end((long long)frame_bytes * 8);
+    if (ctu_rows > 0) { prev_v2_rowbytes = frame_bytes / (size_t)ctu_rows; prev_v2_valid = 1; }
+
+    // PSNR (reference src/tcodec.c:34-54) from the device SSE.
+    const unsigned long long sse = *h_sse;
+    double psnr = 100.0;
+    if (sse) {
+        const double mse = (double)sse / ((double)W * (double)H);
+        psnr = 10.0 * log10(255.0 * 255.0 / mse);
+    }
+    sum_psnr += psnr;
+
+    // ---- DPB shift: slot 3 falls out, the new reconstruction enters slot 0.
+    for (int i = TC_REF_FRAMES - 1; i > 0; --i) { dpb_slot[i] = dpb_slot[i - 1]; dpb_poc[i] = dpb_poc[i - 1]; }
+    dpb_slot[0] = rs;
+    dpb_poc[0] = poc;
+    last_rec = rs;
+
+    pkt->data = out_buf;
+    pkt->size = frame_bytes;
+    pkt->pts = poc;
+    pkt->key_frame = is_key;
+    total_bytes += (long long)frame_bytes;
+    total_frames++;
+    frame_count++;
+    grid_cur = 1 - grid_cur;   // this frame's grid becomes the temporal predictor
+    prev_mv_valid = 1;
+    return TC_OK;
+}
+
+long long tcb::tc_lambda_host(int qp) {
+    const long long s = qscale(qp);
+    long long l = (s * s * 200) >> 10;
+    if (l < 1) l = 1;
+    if (l > (1ll << 30)) l = 1ll << 30;
+    return l;
+}
+
+// ---------------------------------------------------------------------------
+// B-frame reorder (reference src/encoder.c:3132-3277): display-order inputs
+// wait in device buffers and are emitted in coding order A(0), then per
+// group A(4k), B(4k-2), B(4k-3), B(4k-1).
+// ---------------------------------------------------------------------------
+static int bf_schedule_poc(int p) {
+    if (p == 0) return 0;
+    const int k = (p + 3) / 4, c = (p - 1) % 4;
+    static const int off[4] = {0, -2, -3, -1};
+    return 4 * k + off[c];
+}
+static int bf_sched_qp_off(int p) {
+    if (p == 0) return 0;
+    const int c = (p - 1) % 4;
+    if (c == 1) return 1;
+    if (c == 2 || c == 3) return 2;
+    return 0;
+}
+static int bf_anchor_slot(int p) { return p == 0 ? 0 : p - ((p - 1) % 4); }
+
+int EncImpl::bf_find(int poc) const {
+    for (size_t i = 0; i < bf_pocs.size(); ++i)
+        if (bf_pocs[i] == poc) return (int)i;
+    return -1;
+}
+bool EncImpl::bf_can_emit() const {
+    if (bf_pocs.empty()) return false;
+    const int p = bf_emit_pos;
+    if (bf_find(bf_schedule_poc(p)) < 0) return false;
+    if (p == 0) return true;
+    if ((p - 1) % 4 == 0) return true;
+    return bf_emit_pos > bf_anchor_slot(p);
+}
+tc_error_t EncImpl::bf_emit_index(int idx, int poc, int qp_off, tc_packet_t *out) {
+    if (!dcopy(cur, bf_frames[idx])) return TC_ERR_INTERNAL;
+    const tc_error_t r = encode_poc_frame(poc, qp_off, out);
+    cudaFree(bf_frames[idx].y); cudaFree(bf_frames[idx].cb); cudaFree(bf_frames[idx].cr);
+    bf_frames.erase(bf_frames.begin() + idx);
+    bf_pocs.erase(bf_pocs.begin() + idx);
+    return r;
+}
+tc_error_t EncImpl::bf_emit_scheduled(tc_packet_t *out) {
+    const int p = bf_emit_pos;
+    const int poc = bf_schedule_poc(p);
+    const int idx = bf_find(poc);
+    bf_emit_pos++;
+    return bf_emit_index(idx, poc, bf_sched_qp_off(p), out);
+}
+tc_error_t EncImpl::bf_push_current() {
+    if (bf_pocs.size() >= 8) return TC_OK;
+    DevFrame f;
+    const size_t ybytes = (size_t)sy * H + 64, cbytes = (size_t)sc * (H / 2) + 64;
+    if (cudaMalloc(&f.y, ybytes) != cudaSuccess || cudaMalloc(&f.cb, cbytes) != cudaSuccess ||
+        cudaMalloc(&f.cr, cbytes) != cudaSuccess)
+        return TC_ERR_MEMORY;
+    if (!dcopy(f, cur)) return TC_ERR_INTERNAL;
+    bf_frames.push_back(f);
+    bf_pocs.push_back(bf_next_input);
+    return TC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Public API
+// ---------------------------------------------------------------------------
+extern "C" {
+
+tc_encoder_t *tc_encoder_create(const tc_config_t *config) {
+    if (!config) return nullptr;
+    if (!config->use_v2) return nullptr;   // this library implements the v2 bitstream
+    if (config->width <= 0 || config->height <= 0 || (config->width & 1) || (config->height & 1) ||
+        config->width > TC_MAX_WIDTH || config->height > TC_MAX_HEIGHT)
+        return nullptr;
+    tc_encoder_t *enc = (tc_encoder_t *)calloc(1, sizeof(tc_encoder_t));
+    if (!enc) return nullptr;
+    enc->cfg = *config;
+    enc->impl = new (std::nothrow) EncImpl();
+    if (!enc->impl || !enc->impl->init(*config)) {
+        tc_encoder_destroy(enc);
+        return nullptr;
+    }
+    enc->cur = tcb_host_frame_alloc(config->width, config->height, 0);
+    enc->recon = tcb_host_frame_alloc(config->width, config->height, 1);
+    if (!enc->cur || !enc->recon) { tc_encoder_destroy(enc); return nullptr; }
+    enc->impl->recon_host = enc->recon;
+    return enc;
+}
+
+void tc_encoder_destroy(tc_encoder_t *enc) {
+    if (!enc) return;
+    if (enc->impl) { enc->impl->release(); delete enc->impl; }
+    tcb_host_frame_free(enc->cur);
+    tcb_host_frame_free(enc->recon);
+    free(enc);
+}
+
+tc_error_t tc_encoder_encode(tc_encoder_t *enc, const tc_pixel_t *y, int stride_y,
+                             const tc_pixel_t *cb, int stride_cb, const tc_pixel_t *cr,
+                             int stride_cr, tc_packet_t *packet_out) {
+    if (!enc || !enc->impl || !y || !cb || !cr || !packet_out) return TC_ERR_PARAM;
+    EncImpl &e = *enc->impl;
+    if (cudaSetDevice(e.device) != cudaSuccess) return TC_ERR_INTERNAL;
+    if (!e.upload(y, stride_y, cb, stride_cb, cr, stride_cr, e.cur)) return TC_ERR_INTERNAL;
+    if (e.bf_b_mode) {
+        const tc_error_t r = e.bf_push_current();
+        if (r != TC_OK) return r;
+        e.bf_next_input++;
+        if (!e.bf_can_emit()) return TC_ERR_NEED_MORE;
+        return e.bf_emit_scheduled(packet_out);
+    }
+    return e.encode_poc_frame(e.frame_count, 0, packet_out);
+}
+
+tc_error_t tc_encoder_flush_tail(tc_encoder_t *enc, tc_packet_t *packet_out) {
+    if (!enc || !enc->impl || !packet_out) return TC_ERR_PARAM;
+    EncImpl &e = *enc->impl;
+    if (!e.bf_b_mode) return TC_ERR_EOF;
+    if (cudaSetDevice(e.device) != cudaSuccess) return TC_ERR_INTERNAL;
+    if (e.bf_can_emit()) return e.bf_emit_scheduled(packet_out);
+    if (!e.bf_pocs.empty()) {
+        int best = 0;
+        for (size_t i = 1; i < e.bf_pocs.size(); ++i)
+            if (e.bf_pocs[i] < e.bf_pocs[best]) best = (int)i;
+        return e.bf_emit_index(best, e.bf_pocs[best], 0, packet_out);
+    }
+    return TC_ERR_EOF;
+}
+
+void tc_encoder_force_keyframe(tc_encoder_t *enc) {
+    if (enc && enc->impl) enc->impl->force_keyframe = 1;
+}
+
+void tc_encoder_get_stats(tc_encoder_t *enc, int64_t *total_bytes, int32_t *total_frames,
+                          double *avg_psnr) {
+    if (!enc || !enc->impl) return;
+    const EncImpl &e = *enc->impl;
+    if (total_bytes) *total_bytes = (int32_t)e.total_bytes;
+    if (total_frames) *total_frames = e.total_frames;
+    if (avg_psnr) *avg_psnr = e.total_frames > 0 ? e.sum_psnr / e.total_frames : 0.0;
+}
+
+}  // extern "C"

@@ -1,0 +1,96 @@
+// tcb_encoder.h — private encoder state of libtcodec_b200.
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+#include <new>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/tcodec.h"
+#include "tcb_common.cuh"
+
+namespace tcb {
+
+struct DevFrame {
+    uint8_t *y = nullptr, *cb = nullptr, *cr = nullptr;
+};
+
+long long tc_lambda_host(int qp);
+
+struct EncImpl {
+    static constexpr int NPOOL = 6;   // 4 DPB slots + the frame being built + spare
+    tc_config_t cfg{};
+    int W = 0, H = 0, sy = 0, sc = 0, ctu_cols = 0, ctu_rows = 0, grid_w = 0, grid_h = 0;
+    int device = 0;
+    cudaStream_t st = nullptr;
+    cudaError_t last_cuda_error = cudaSuccess;
+    DevFrame pool[NPOOL];
+    DevFrame cur;
+    int dpb_slot[TC_REF_FRAMES]{}, dpb_poc[TC_REF_FRAMES]{};
+    int last_rec = -1;
+    MvCell *grid[2] = {nullptr, nullptr};
+    int grid_cur = 0;
+    CtuOut *d_out = nullptr, *h_out = nullptr;
+    FrameParams h_params{};
+    FrameParams *d_params = nullptr;
+    int *d_items = nullptr;
+    std::vector<int> diag_off, diag_cnt;
+    int *d_hist = nullptr, *h_hist = nullptr;
+    unsigned long long *d_sse = nullptr, *h_sse = nullptr;
+    int *d_err = nullptr;
+    tc_frame_buf_t *recon_host = nullptr;
+    uint8_t *out_buf = nullptr;
+    size_t out_buf_size = 0;
+    // sequence state
+    int frame_count = 0, force_keyframe = 0;
+    int prev_hist[16]{}, prev_hist_valid = 0, prev_mv_valid = 0;
+    size_t prev_v2_rowbytes = 0;
+    int prev_v2_valid = 0;
+    long long total_bytes = 0;
+    int total_frames = 0;
+    double sum_psnr = 0.0;
+    // rate control
+    int rc_method = 0, rc_qp = 32, rc_base_qp = 32;
+    long long rc_frame_target = 0;
+    double rc_buffer_size = 0.0, rc_buffer_level = 0.5;
+    // B-frame reorder
+    int bf_b_mode = 0, bf_emit_pos = 0, bf_next_input = 0;
+    std::vector<DevFrame> bf_frames;
+    std::vector<int> bf_pocs;
+
+    bool init(const tc_config_t &c);
+    void release();
+    int free_pool_slot() const;
+    bool upload(const tc_pixel_t *y, int ys, const tc_pixel_t *cb, int cbs, const tc_pixel_t *cr, int crs,
+                const DevFrame &dst);
+    bool dcopy(const DevFrame &dst, const DevFrame &src);
+    tc_error_t encode_poc_frame(int poc, int b_layer_qp_off, tc_packet_t *pkt);
+    void rc_init(const tc_config_t &c);
+    void rc_frame_start();
+    void rc_frame_end(long long bits);
+    int bf_find(int poc) const;
+    bool bf_can_emit() const;
+    tc_error_t bf_emit_scheduled(tc_packet_t *out);
+    tc_error_t bf_emit_index(int idx, int poc, int qp_off, tc_packet_t *out);
+    tc_error_t bf_push_current();
+};
+
+}  // namespace tcb
+
+// Public handle.  The first three members keep the reference's
+// tc_encoder_t prefix (tcodec_common.h:609-612) so callers that read
+// encoder->recon after an encode (the reference test suite does) see the
+// host copy of the reconstruction.
+struct tc_encoder {
+    tc_config_t cfg;
+    tc_frame_buf_t *cur;
+    tc_frame_buf_t *recon;
+    tcb::EncImpl *impl;
+};
+
+extern "C" {
+tc_frame_buf_t *tcb_host_frame_alloc(int width, int height, int pinned);
+void tcb_host_frame_free(tc_frame_buf_t *f);
+}

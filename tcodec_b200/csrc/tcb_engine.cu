@@ -1,0 +1,1224 @@
+// tcb_engine.cu — the v2 CTU rate-distortion engine on sm_100a.
+//
+// One 512-thread CTA encodes one 64x64 CTU end to end, keeping the CTU's
+// source, reconstruction, quadtree snapshots and candidate predictions in
+// shared memory:
+//
+//   decide pass  recursive quadtree RDO (reference src/encoder.c:1292-1397
+//                qt_split) over leaves (src/encoder.c:562-1290 qt_leaf);
+//                inside a leaf all candidates run concurrently: four motion
+//                searches on four warp groups, then every (candidate, TU
+//                size, TU) residual coding job on octets / quads of lanes,
+//                then an in-order strict-< scan that reproduces the
+//                reference's first-minimum tie rule;
+//   write pass   replays the chosen tree in z-order, emitting quantised
+//                coefficients (src/encoder.c:1450-1456);
+//   filters      deblocking of the CTU's inner edges (src/filter.c:175-237)
+//                and the luma SAO band-offset choice, rate gate and
+//                application (src/filter.c:245-319, src/encoder.c:1463-1506);
+//   exports      reconstruction, MV grid (src/encoder.c:1508-1521) and the
+//                CTU record the host range coder consumes.
+//
+// CTUs of one frame run as an anti-diagonal wavefront: CTU (r, c) reads the
+// filtered reconstruction of (r, c-1), (r-1, c) and (r-1, c-1) only, so all
+// CTUs with the same r + c are independent and go in one launch.
+#include "tcb_engine.cuh"
+#include "tcb_pixel.cuh"
+#include "tcb_launch.h"
+
+namespace tcb {
+
+// Motion search patterns (reference src/motion.c:347-367).
+__constant__ int8_t c_hex_large[7][2] = {{0, 0}, {-2, -4}, {2, -4}, {-4, 0}, {4, 0}, {-2, 4}, {2, 4}};
+__constant__ int8_t c_hex_small[7][2] = {{0, 0}, {-1, -2}, {1, -2}, {-2, 0}, {2, 0}, {-1, 2}, {1, 2}};
+__constant__ int8_t c_diamond[5][2] = {{0, 0}, {0, -1}, {-1, 0}, {1, 0}, {0, 1}};
+__constant__ int8_t c_qpel[9][2] = {{0, 0}, {1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, 1}, {1, -1}, {-1, -1}};
+
+#define SYNC() __syncthreads()
+
+__device__ __forceinline__ void group_bar(int g) {
+    asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(GT) : "memory");
+}
+
+__device__ __forceinline__ uint32_t ld4u(const uint8_t *p) {
+    const uintptr_t a = (uintptr_t)p;
+    const uint32_t *w = (const uint32_t *)(a & ~(uintptr_t)3);
+    const uint32_t lo = __ldg(w), hi = __ldg(w + 1);
+    return __funnelshift_r(lo, hi, (uint32_t)(a & 3) * 8);
+}
+
+__device__ __forceinline__ uint8_t &RY(Smem &S, int x, int y) {
+    return S.rec_y[(y + RY_OY) * RY_W + x + RY_OX];
+}
+__device__ __forceinline__ uint8_t &RC(Smem &S, int c, int x, int y) {
+    return S.rec_c[c][(y + RC_OY) * RC_W + x + RC_OX];
+}
+
+struct Leaf {
+    int depth, cx, cy, cu, lx, ly, px, py;
+    __device__ Leaf(const FrameParams &P, int ctu_x, int ctu_y, int d, int x, int y) {
+        depth = d; cx = x; cy = y; cu = 8 << (3 - d);
+        lx = x * 8; ly = y * 8; px = ctu_x + lx; py = ctu_y + ly;
+    }
+};
+
+// Minimum-magnitude MV predictor over left / above / above-right cells
+// (reference src/encoder.c:405-427 qt_mvp).
+__device__ void mvp_at(const MvCell *grid, int cx, int cy, int &mx, int &my) {
+    int ax = 0, ay = 0, bx = 0, by = 0, cxv = 0, cyv = 0;
+    bool ha = false, hb = false, hc = false;
+    if (cx > 0) { const MvCell m = grid[cy * 8 + cx - 1]; if (!m.intra) { ax = m.dx; ay = m.dy; ha = true; } }
+    if (cy > 0) { const MvCell m = grid[(cy - 1) * 8 + cx]; if (!m.intra) { bx = m.dx; by = m.dy; hb = true; } }
+    if (cy > 0 && cx < 7) { const MvCell m = grid[(cy - 1) * 8 + cx + 1]; if (!m.intra) { cxv = m.dx; cyv = m.dy; hc = true; } }
+    if (!ha && !hb && !hc) { mx = 0; my = 0; return; }
+    if (!ha) { ax = hb ? bx : cxv; ay = hb ? by : cyv; }
+    if (!hb) { bx = ha ? ax : cxv; by = ha ? ay : cyv; }
+    if (!hc) { cxv = ha ? ax : bx; cyv = ha ? ay : by; }
+    const long long qa = (long long)ax * ax + (long long)ay * ay;
+    const long long qb = (long long)bx * bx + (long long)by * by;
+    const long long qc = (long long)cxv * cxv + (long long)cyv * cyv;
+    if (qb < qa && qb <= qc) { mx = bx; my = by; }
+    else if (qc < qa && qc < qb) { mx = cxv; my = cyv; }
+    else { mx = ax; my = ay; }
+}
+
+// ====================================================================
+// Motion search on one warp group (reference src/motion.c:384-485).
+// ====================================================================
+
+// SADs of up to 7 integer candidates base + pat[p0 + k] * scale, k < K.
+// Out-of-frame candidates cost 0x7FFFFFFF (reference sad_at).
+__device__ void group_int_sads(Smem &S, int g, int gt, const uint8_t *ref, int s, int W, int H,
+                               const uint8_t *cur, int blk, int pat, int p0, int K,
+                               int bx, int by, int scale) {
+    const int wpr = blk >> 2, words = blk * wpr, total = K * words;
+    int acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int i = gt; i < total; i += GT) {
+        const int k = i / words, w = i - k * words, r = w / wpr, c4 = (w - r * wpr) * 4;
+        int dx, dy;
+        if (pat == 0) { dx = c_hex_large[p0 + k][0]; dy = c_hex_large[p0 + k][1]; }
+        else if (pat == 1) { dx = c_hex_small[p0 + k][0]; dy = c_hex_small[p0 + k][1]; }
+        else if (pat == 2) { dx = c_diamond[p0 + k][0]; dy = c_diamond[p0 + k][1]; }
+        else { dx = 0; dy = 0; }
+        const int x = bx + dx * scale, y = by + dy * scale;
+        int v = 0;
+        if (x >= 0 && y >= 0 && x + blk <= W && y + blk <= H)
+            v = (int)__vsadu4(ld4u(ref + (size_t)(y + r) * s + x + c4),
+                              *(const uint32_t *)(cur + r * 64 + c4));
+#pragma unroll
+        for (int kk = 0; kk < 7; ++kk) acc[kk] += (kk == k) ? v : 0;
+    }
+    const int wig = (gt >> 5), lane = gt & 31;
+#pragma unroll
+    for (int kk = 0; kk < 7; ++kk) {
+        if (kk < K) {
+            const int v = __reduce_add_sync(0xffffffffu, acc[kk]);
+            if (lane == 0) S.me[g].part[wig][kk] = v;
+        }
+    }
+    group_bar(g);
+    if (gt < K) {
+        int dx, dy;
+        if (pat == 0) { dx = c_hex_large[p0 + gt][0]; dy = c_hex_large[p0 + gt][1]; }
+        else if (pat == 1) { dx = c_hex_small[p0 + gt][0]; dy = c_hex_small[p0 + gt][1]; }
+        else if (pat == 2) { dx = c_diamond[p0 + gt][0]; dy = c_diamond[p0 + gt][1]; }
+        else { dx = 0; dy = 0; }
+        const int x = bx + dx * scale, y = by + dy * scale;
+        int sum = 0;
+#pragma unroll
+        for (int w = 0; w < GT / 32; ++w) sum += S.me[g].part[w][gt];
+        S.me[g].sad[gt] = (x >= 0 && y >= 0 && x + blk <= W && y + blk <= H) ? sum : 0x7FFFFFFF;
+    }
+    group_bar(g);
+}
+
+// One integer stage: `iters` passes over pattern points 1..npts, each point
+// taken relative to the running best (sequential commit, first improvement
+// wins; reference src/motion.c:398-448).
+__device__ void int_stage(Smem &S, int g, int gt, const uint8_t *ref, int s, int W, int H,
+                          const uint8_t *cur, int blk, int pat, int npts, int iters, int scale,
+                          int &bx, int &by, int &bsad) {
+    for (int it = 0; it < iters; ++it) {
+        bool improved = false;
+        int p0 = 1;
+        while (p0 <= npts) {
+            const int K = npts - p0 + 1;
+            group_int_sads(S, g, gt, ref, s, W, H, cur, blk, pat, p0, K, bx, by, scale);
+            int found = -1;
+            for (int k = 0; k < K; ++k)
+                if (S.me[g].sad[k] < bsad) { found = k; break; }
+            const int fs = found >= 0 ? S.me[g].sad[found] : 0;
+            group_bar(g);
+            if (found < 0) break;
+            int dx, dy;
+            const int p = p0 + found;
+            if (pat == 0) { dx = c_hex_large[p][0]; dy = c_hex_large[p][1]; }
+            else if (pat == 1) { dx = c_hex_small[p][0]; dy = c_hex_small[p][1]; }
+            else { dx = c_diamond[p][0]; dy = c_diamond[p][1]; }
+            bx += dx * scale; by += dy * scale; bsad = fs;
+            improved = true;
+            p0 = p + 1;
+        }
+        if (!improved) break;
+    }
+}
+
+// Sub-pel SAD of one candidate: six-tap diagonal interpolation where the
+// margins allow, else the bilinear sub-pel SAD (reference
+// src/motion.c:308-341 and 450-481).
+__device__ int group_subpel_sad(Smem &S, int g, int gt, const uint8_t *ref, int s,
+                                const uint8_t *cur, int blk, int qx, int qy, bool six) {
+    const int fx = qx >> 2, fy = qy >> 2, dx = qx & 3, dy = qy & 3;
+    int acc = 0;
+    const int total = blk * blk;
+    for (int i = gt; i < total; i += GT) {
+        const int yy = i / blk, xx = i - yy * blk;
+        int p;
+        if (six) {
+            p = luma_hv(ref, s, fx + xx, fy + yy, dx, dy);
+        } else {
+            const uint8_t *q = ref + (size_t)(fy + yy) * s + fx + xx;
+            const int top = interp_qpel(q[0], q[1], dx);
+            const int bot = interp_qpel(q[s], q[s + 1], dx);
+            p = interp_qpel(top, bot, dy);
+        }
+        acc += absi((int)cur[yy * 64 + xx] - p);
+    }
+    acc = __reduce_add_sync(0xffffffffu, acc);
+    if ((gt & 31) == 0) S.me[g].part[gt >> 5][0] = acc;
+    group_bar(g);
+    int sum = 0;
+#pragma unroll
+    for (int w = 0; w < GT / 32; ++w) sum += S.me[g].part[w][0];
+    group_bar(g);
+    return sum;
+}
+
+__device__ void me_run(Smem &S, int g, int gt, const uint8_t *ref, int s, int W, int H,
+                       int lx, int ly, int blk, int center_x, int center_y, int sr) {
+    const uint8_t *cur = S.cur_y + ly * 64 + lx;
+    int bx = clampi(center_x, 0, W - blk), by = clampi(center_y, 0, H - blk);
+    group_int_sads(S, g, gt, ref, s, W, H, cur, blk, 3, 0, 1, bx, by, 1);
+    int bsad = S.me[g].sad[0];
+    group_bar(g);
+    const int scale = maxi(1, sr / 4);
+    int_stage(S, g, gt, ref, s, W, H, cur, blk, 0, 6, 2, scale, bx, by, bsad);
+    int_stage(S, g, gt, ref, s, W, H, cur, blk, 1, 6, 3, 1, bx, by, bsad);
+    int_stage(S, g, gt, ref, s, W, H, cur, blk, 2, 4, 4, 1, bx, by, bsad);
+    int mx = bx * 4, my = by * 4;
+    for (int p = 1; p < 9; ++p) {
+        const int qx = mx + c_qpel[p][0], qy = my + c_qpel[p][1];
+        const int fx = qx >> 2, fy = qy >> 2;
+        if (fx < 0 || fy < 0 || fx + blk + 1 > W || fy + blk + 1 > H) continue;
+        const bool six = fx >= 2 && fy >= 2 && fx + blk + 2 < W && fy + blk + 2 < H;
+        const int sad = group_subpel_sad(S, g, gt, ref, s, cur, blk, qx, qy, six);
+        if (sad < bsad) { bsad = sad; mx = qx; my = qy; }
+    }
+    if (gt == 0) { S.me[g].mvx = mx; S.me[g].mvy = my; S.me[g].best = bsad; }
+}
+
+// ====================================================================
+// Leaf helpers
+// ====================================================================
+
+// v2 intra reference samples (reference src/predict.c:480-520): above-right
+// and below-left are replicated.  S.ra[0] / S.rl[0] hold the corner.
+__device__ void build_refs(Smem &S, const Leaf &L) {
+    const int N = L.cu;
+    const bool ha = L.py > 0, hl = L.px > 0;
+    for (int i = threadIdx.x; i <= 2 * N; i += NT) {
+        const int j = i < N ? i : N - 1;
+        int a, l;
+        if (ha) a = RY(S, L.lx + j, L.ly - 1);
+        else a = hl ? RY(S, L.lx - 1, L.ly) : 128;
+        if (hl) l = RY(S, L.lx - 1, L.ly + j);
+        else l = ha ? RY(S, L.lx, L.ly - 1) : 128;
+        S.ra[i + 1] = (uint8_t)a;
+        S.rl[i + 1] = (uint8_t)l;
+    }
+    if (threadIdx.x == 0) {
+        int tl;
+        if (ha && hl) tl = RY(S, L.lx - 1, L.ly - 1);
+        else if (ha) tl = RY(S, L.lx, L.ly - 1);
+        else if (hl) tl = RY(S, L.lx - 1, L.ly);
+        else tl = 128;
+        S.ra[0] = (uint8_t)tl;
+        S.rl[0] = (uint8_t)tl;
+    }
+    SYNC();
+    if (threadIdx.x < 32) {
+        // DC value (reference src/predict.c:140-161): samples 1..N of each run.
+        int sum = 0;
+        for (int i = threadIdx.x; i < N; i += 32) sum += S.ra[i + 2] + S.rl[i + 2];
+        sum = __reduce_add_sync(0xffffffffu, sum);
+        if (threadIdx.x == 0) S.dc = (sum + N) / (2 * N);
+    }
+    SYNC();
+}
+
+__device__ __forceinline__ int lpred(const Smem &S, int cu, int slot, int dc, int x, int y) {
+    if (slot < NPRED) return S.pred[slot][y * cu + x];
+    return intra_at(S.ra + 1, S.rl + 1, cu, slot - K_INTRA, dc, x, y);
+}
+
+// Luma residual jobs, 8x8 TUs: one octet per (candidate, TU).
+__device__ void luma_jobs8(Smem &S, const Leaf &L, int ncl, const QuantParams &qp,
+                           bool accum, bool wrec, int16_t *emit) {
+    const int cu = L.cu, ntu = cu >> 3, ntu2 = ntu * ntu, J = ncl * ntu2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, oct = lane >> 3, l8 = lane & 7;
+    int *scr = S.scratch[warp] + oct * 64;
+    const int dc = S.dc;
+    for (int base = 0; base < J; base += NW * 4) {
+        const int j = base + warp * 4 + oct;
+        const bool act = j < J;
+        const int jj = act ? j : 0;
+        const int k = jj / ntu2, t = jj - k * ntu2, ty = t / ntu, tx = t - ty * ntu;
+        const int slot = S.cl[k];
+        int res[8];
+        const int r = ty * 8 + l8;
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+            const int x = tx * 8 + n;
+            res[n] = clampi((int)S.cur_y[(L.ly + r) * 64 + L.lx + x] - lpred(S, cu, slot, dc, x, r), -512, 511);
+        }
+        int qc[8], rc[8];
+        const int bits = tu8_code(l8, res, scr, qp, qc, rc);
+        int sse = 0;
+        const int x = tx * 8 + l8;
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) {
+            const int y = ty * 8 + kk;
+            const int v = clampi(lpred(S, cu, slot, dc, x, y) + rc[kk], 0, 255);
+            const int d = (int)S.cur_y[(L.ly + y) * 64 + L.lx + x] - v;
+            sse += d * d;
+            if (act && wrec) RY(S, L.lx + x, L.ly + y) = (uint8_t)v;
+            if (act && emit) emit[t * 64 + kk * 8 + l8] = (int16_t)qc[kk];
+        }
+        sse = oct_sum(sse);
+        if (act && accum && l8 == 0) {
+            atomicAdd(&S.acc_sse[slot][0], sse);
+            atomicAdd(&S.acc_bits[slot][0], bits);
+        }
+    }
+}
+
+// Luma residual jobs, 4x4 TUs inside each 8x8 TU: one quad per
+// (candidate, TU, sub-block); the sub-block-0 quad adds the outer flag bit
+// (reference src/encoder.c:508-535).
+__device__ void luma_jobs4(Smem &S, const Leaf &L, int ncl, const QuantParams &qp,
+                           bool accum, bool wrec, int16_t *emit) {
+    const int cu = L.cu, ntu = cu >> 3, ntu2 = ntu * ntu, per = ntu2 * 4, J = ncl * per;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, qd = lane >> 2, l4 = lane & 3;
+    int *scr = S.scratch[warp] + qd * 16;
+    const int dc = S.dc;
+    for (int base = 0; base < J; base += NW * 8) {
+        const int j = base + warp * 8 + qd;
+        const bool act = j < J;
+        const int jj = act ? j : 0;
+        const int k = jj / per, rem = jj - k * per, t = rem >> 2, q = rem & 3;
+        const int ty = t / ntu, tx = t - ty * ntu;
+        const int sx = tx * 8 + (q & 1) * 4, sy = ty * 8 + (q & 2) * 2;
+        const int slot = S.cl[k];
+        int res[4];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            const int x = sx + n, y = sy + l4;
+            res[n] = clampi((int)S.cur_y[(L.ly + y) * 64 + L.lx + x] - lpred(S, cu, slot, dc, x, y), -512, 511);
+        }
+        int qc[4], rc[4];
+        int bits = tu4_code(l4, res, scr, qp, qc, rc);
+        if (q == 0) bits += 1;
+        int sse = 0;
+        const int x = sx + l4;
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+            const int y = sy + kk;
+            const int v = clampi(lpred(S, cu, slot, dc, x, y) + rc[kk], 0, 255);
+            const int d = (int)S.cur_y[(L.ly + y) * 64 + L.lx + x] - v;
+            sse += d * d;
+            if (act && wrec) RY(S, L.lx + x, L.ly + y) = (uint8_t)v;
+            if (act && emit) emit[t * 64 + q * 16 + kk * 4 + l4] = (int16_t)qc[kk];
+        }
+        sse = quad_sum(sse);
+        if (act && accum && l4 == 0) {
+            atomicAdd(&S.acc_sse[slot][1], sse);
+            atomicAdd(&S.acc_bits[slot][1], bits);
+        }
+    }
+}
+
+// Chroma residual jobs (reference src/encoder.c:429-475 qt_code_chroma):
+// 4x4 TUs, one quad per (option, component, TU).  Option o, component c
+// predicts from S.cpred[cbase + 2*o + c]; results accumulate in slot o.
+__device__ void chroma_jobs(Smem &S, const Leaf &L, int nopt, int cbase, const QuantParams &qp,
+                            bool accum, bool wrec, int16_t *emit) {
+    const int cs = L.cu >> 1, nt = cs >> 2, nt2 = nt * nt, per = 2 * nt2, J = nopt * per;
+    const int lxc = L.lx >> 1, lyc = L.ly >> 1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, qd = lane >> 2, l4 = lane & 3;
+    int *scr = S.scratch[warp] + qd * 16;
+    for (int base = 0; base < J; base += NW * 8) {
+        const int j = base + warp * 8 + qd;
+        const bool act = j < J;
+        const int jj = act ? j : 0;
+        const int o = jj / per, rem = jj - o * per, c = rem / nt2, t = rem - c * nt2;
+        const int ty = t / nt, tx = t - ty * nt;
+        const uint8_t *pr = S.cpred[cbase + 2 * o + c];
+        const uint8_t *org = S.cur_c[c];
+        int res[4];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            const int x = tx * 4 + n, y = ty * 4 + l4;
+            res[n] = clampi((int)org[(lyc + y) * 32 + lxc + x] - (int)pr[y * cs + x], -512, 511);
+        }
+        int qc[4], rc[4];
+        const int bits = tu4_code(l4, res, scr, qp, qc, rc);
+        int sse = 0;
+        const int x = tx * 4 + l4;
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+            const int y = ty * 4 + kk;
+            const int v = clampi((int)pr[y * cs + x] + rc[kk], 0, 255);
+            const int d = (int)org[(lyc + y) * 32 + lxc + x] - v;
+            sse += d * d;
+            if (act && wrec) RC(S, c, lxc + x, lyc + y) = (uint8_t)v;
+            if (act && emit) emit[c * cs * cs + t * 16 + kk * 4 + l4] = (int16_t)qc[kk];
+        }
+        sse = quad_sum(sse);
+        if (act && accum && l4 == 0) {
+            atomicAdd(&S.acc_sse[o][0], sse);
+            atomicAdd(&S.acc_bits[o][0], bits);
+        }
+    }
+}
+
+// Chroma DC predictor (reference src/predict.c:364-379) into cpred[dst+c].
+__device__ void chroma_dc_pred(Smem &S, const Leaf &L, int dst) {
+    const int cs = L.cu >> 1, lxc = L.lx >> 1, lyc = L.ly >> 1;
+    const bool ha = L.py > 0, hl = L.px > 0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp < 2) {
+        const int c = warp;
+        int sum = 0;
+        for (int i = lane; i < cs; i += 32) {
+            if (ha) sum += RC(S, c, lxc + i, lyc - 1);
+            if (hl) sum += RC(S, c, lxc - 1, lyc + i);
+        }
+        sum = __reduce_add_sync(0xffffffffu, sum);
+        const int n = (ha ? cs : 0) + (hl ? cs : 0);
+        if (lane == 0) S.sao[c] = n ? (sum + n / 2) / n : 128;
+    }
+    SYNC();
+    for (int i = threadIdx.x; i < 2 * cs * cs; i += NT) {
+        const int c = i / (cs * cs);
+        S.cpred[dst + c][i - c * cs * cs] = (uint8_t)S.sao[c];
+    }
+    SYNC();
+}
+
+// Chroma-from-luma blend over the DC prediction in cpred[dst+c]
+// (reference src/predict.c:390-462), reading fresh reconstructed luma.
+__device__ void cfl_blend(Smem &S, const Leaf &L, int dst) {
+    const int cs = L.cu >> 1, lxc = L.lx >> 1, lyc = L.ly >> 1;
+    const bool up = L.py > 0, left = L.px > 0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __shared__ int s_sign[2], s_shift[2];
+    if (warp < 2) {
+        const int c = warp;
+        long long sl = 0, sc = 0, slc = 0, sl2 = 0;
+        int n = 0;
+        for (int i = lane; i < cs; i += 32) {
+            if (up) {
+                const int la = (RY(S, L.lx + 2 * i, L.ly - 1) + RY(S, L.lx + 2 * i + 1, L.ly - 1) + 1) >> 1;
+                const int cv = RC(S, c, lxc + i, lyc - 1);
+                sl += la; sc += cv; slc += (long long)la * cv; sl2 += (long long)la * la;
+            }
+            if (left) {
+                const int la = (RY(S, L.lx - 2, L.ly + 2 * i) + RY(S, L.lx - 1, L.ly + 2 * i) +
+                                RY(S, L.lx - 2, L.ly + 2 * i + 1) + RY(S, L.lx - 1, L.ly + 2 * i + 1) + 2) >> 2;
+                const int cv = RC(S, c, lxc - 1, lyc + i);
+                sl += la; sc += cv; slc += (long long)la * cv; sl2 += (long long)la * la;
+            }
+        }
+        n = (up ? cs : 0) + (left ? cs : 0);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            sl += __shfl_xor_sync(0xffffffffu, sl, o);
+            sc += __shfl_xor_sync(0xffffffffu, sc, o);
+            slc += __shfl_xor_sync(0xffffffffu, slc, o);
+            sl2 += __shfl_xor_sync(0xffffffffu, sl2, o);
+        }
+        if (lane == 0) {
+            const long long nn = n;
+            const int sign = (nn == 0 || nn * slc >= sl * sc) ? 1 : -1;
+            int ash = 3;
+            const long long cov = nn * slc - sl * sc, vl = nn * sl2 - sl * sl;
+            if (nn > 0 && vl > 0 && cov != 0) {
+                const unsigned long long acov = cov < 0 ? (unsigned long long)(-cov) : (unsigned long long)cov;
+                const unsigned long long q = (unsigned long long)vl / acov;
+                int s = (q < 1) ? 2 : (q > 0xFFFFFFFFull) ? 5 : 31 - __clz((int)(unsigned)q);
+                ash = s < 2 ? 2 : (s > 5 ? 5 : s);
+            }
+            s_sign[c] = sign;
+            s_shift[c] = ash;
+        }
+    }
+    SYNC();
+    // Per 4x4 chroma tile: mean of the 2x2-averaged collocated luma.
+    const int nt = cs >> 2;
+    for (int i = threadIdx.x; i < 2 * cs * cs; i += NT) {
+        const int c = i / (cs * cs), p = i - c * cs * cs, y = p / cs, x = p - y * cs;
+        const int ty = (y >> 2) << 2, tx = (x >> 2) << 2;
+        int sum = 0;
+#pragma unroll
+        for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+            for (int xx = 0; xx < 4; ++xx) {
+                const int X = L.lx + 2 * (tx + xx), Y = L.ly + 2 * (ty + yy);
+                sum += (RY(S, X, Y) + RY(S, X + 1, Y) + RY(S, X, Y + 1) + RY(S, X + 1, Y + 1) + 2) >> 2;
+            }
+        const int avg = (sum + 8) / 16;
+        const int X = L.lx + 2 * x, Y = L.ly + 2 * y;
+        const int la = (RY(S, X, Y) + RY(S, X + 1, Y) + RY(S, X, Y + 1) + RY(S, X + 1, Y + 1) + 2) >> 2;
+        uint8_t &d = S.cpred[dst + c][p];
+        d = (uint8_t)clampi((int)d + s_sign[c] * ((la - avg) >> s_shift[c]), 0, 255);
+        (void)nt;
+    }
+    SYNC();
+}
+
+// Chroma MC of both components into cpred[dst+c] (or straight into the
+// recon tile when to_rec).
+__device__ void chroma_mc(Smem &S, const FrameParams &P, const Leaf &L, int refi, int mvx, int mvy,
+                          int dst, bool to_rec) {
+    const int cs = L.cu >> 1, Wc = P.W >> 1, Hc = P.H >> 1;
+    for (int i = threadIdx.x; i < 2 * cs * cs; i += NT) {
+        const int c = i / (cs * cs), p = i - c * cs * cs, y = p / cs, x = p - y * cs;
+        const uint8_t *ref = c ? P.ref_cr[refi] : P.ref_cb[refi];
+        const int v = chroma_mc_at(ref, P.stride_c, Wc, Hc, mvx, mvy, x, y);
+        if (to_rec) RC(S, c, (L.lx >> 1) + x, (L.ly >> 1) + y) = (uint8_t)v;
+        else S.cpred[dst + c][p] = (uint8_t)v;
+    }
+    SYNC();
+}
+
+// Luma MC of the listed (slot, ref, mv) predictions into S.pred[slot].
+__device__ void luma_mc_slots(Smem &S, const FrameParams &P, const Leaf &L, int nslots,
+                              const int *slots) {
+    const int cu = L.cu, n = cu * cu;
+    for (int i = threadIdx.x; i < nslots * n; i += NT) {
+        const int k = i / n, p = i - k * n, y = p / cu, x = p - y * cu;
+        const int slot = slots[k];
+        LumaMC m;
+        m.init(P.ref_y[S.cand_ref[slot]], P.stride_y, P.W, P.H, S.cand_mvx[slot], S.cand_mvy[slot], cu);
+        S.pred[slot][p] = (uint8_t)m.at(x, y);
+    }
+    SYNC();
+}
+
+__device__ void zero_acc(Smem &S) {
+    for (int i = threadIdx.x; i < NCAND * 2; i += NT) {
+        (&S.acc_sse[0][0])[i] = 0;
+        (&S.acc_bits[0][0])[i] = 0;
+    }
+    if (threadIdx.x < 4) S.acc64[threadIdx.x] = 0;
+}
+
+// Sum over the CU of |orig - pred| per listed slot into acc_sse[slot][0]
+// (fast-preset SAD proxy).
+__device__ void sad_jobs(Smem &S, const Leaf &L, int ncl) {
+    const int cu = L.cu, n = cu * cu, dc = S.dc;
+    for (int k = 0; k < ncl; ++k) {
+        const int slot = S.cl[k];
+        int acc = 0;
+        for (int p = threadIdx.x; p < n; p += NT) {
+            const int y = p / cu, x = p - y * cu;
+            acc += absi((int)S.cur_y[(L.ly + y) * 64 + L.lx + x] - lpred(S, cu, slot, dc, x, y));
+        }
+        acc = __reduce_add_sync(0xffffffffu, acc);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&S.acc_sse[slot][0], acc);
+    }
+}
+
+__device__ __forceinline__ long long best_of(const Smem &S, int slot, bool use4, long long lambda,
+                                             int &lb, int &dct) {
+    const long long d8 = S.acc_sse[slot][0];
+    const int b8 = S.acc_bits[slot][0];
+    if (use4) {
+        const long long d4 = S.acc_sse[slot][1];
+        const int b4 = S.acc_bits[slot][1];
+        if (d4 + lambda * b4 < d8 + lambda * b8) { lb = b4; dct = 0; return d4; }
+    }
+    lb = b8; dct = 1;
+    return d8;
+}
+
+// Snapshot / restore of a node's reconstruction and grid cells.
+template <int D>
+__device__ void snap(Smem &S, const Leaf &L, int which, bool save) {
+    constexpr int cu = 64 >> D, cs = cu >> 1, gc = cu >> 3;
+    uint8_t *ys = D == 0 ? S.snap_y0[which] : D == 1 ? S.snap_y1[which] : S.snap_y2[which];
+    uint8_t *c0 = D == 0 ? S.snap_c0[which][0] : D == 1 ? S.snap_c1[which][0] : S.snap_c2[which][0];
+    uint8_t *c1 = D == 0 ? S.snap_c0[which][1] : D == 1 ? S.snap_c1[which][1] : S.snap_c2[which][1];
+    MvCell *gs = S.snap_g[D][which];
+    for (int i = threadIdx.x; i < cu * cu; i += NT) {
+        const int y = i / cu, x = i - y * cu;
+        if (save) ys[i] = RY(S, L.lx + x, L.ly + y); else RY(S, L.lx + x, L.ly + y) = ys[i];
+    }
+    for (int i = threadIdx.x; i < cs * cs; i += NT) {
+        const int y = i / cs, x = i - y * cs;
+        if (save) { c0[i] = RC(S, 0, (L.lx >> 1) + x, (L.ly >> 1) + y); c1[i] = RC(S, 1, (L.lx >> 1) + x, (L.ly >> 1) + y); }
+        else { RC(S, 0, (L.lx >> 1) + x, (L.ly >> 1) + y) = c0[i]; RC(S, 1, (L.lx >> 1) + x, (L.ly >> 1) + y) = c1[i]; }
+    }
+    for (int i = threadIdx.x; i < gc * gc; i += NT) {
+        const int y = i / gc, x = i - y * gc;
+        if (save) gs[i] = S.grid[(L.cy + y) * 8 + L.cx + x]; else S.grid[(L.cy + y) * 8 + L.cx + x] = gs[i];
+    }
+    SYNC();
+}
+
+// Grid update after a leaf (reference src/encoder.c:1279-1288 / 760-780).
+__device__ void grid_update(Smem &S, const Leaf &L, const Node &nd, int mvpx, int mvpy) {
+    const int gc = L.cu >> 3;
+    for (int i = threadIdx.x; i < gc * gc; i += NT) {
+        const int y = i / gc, x = i - y * gc;
+        MvCell &g = S.grid[(L.cy + y) * 8 + L.cx + x];
+        if (nd.intra) g.intra = 1;
+        else {
+            g.intra = 0;
+            g.dx = (int16_t)(mvpx + ((nd.merge || nd.skip) ? 0 : nd.mvd_x));
+            g.dy = (int16_t)(mvpy + ((nd.merge || nd.skip) ? 0 : nd.mvd_y));
+        }
+    }
+    SYNC();
+}
+
+// ====================================================================
+// Leaf coding of a decided node: replay in the decide pass, syntax-order
+// coefficient emission in the write pass (reference src/encoder.c:587-781).
+// ====================================================================
+__device__ void leaf_code(Smem &S, const FrameParams &P, const Leaf &L, const QuantParams &ql,
+                          const QuantParams &qc, bool emit, CtuOut *out) {
+    const Node nd = S.nodes[qt_index(L.depth, L.cx, L.cy)];
+    int mvpx, mvpy;
+    mvp_at(S.grid, L.cx, L.cy, mvpx, mvpy);
+    const int cu = L.cu;
+    int16_t *el = emit ? out->coef + S.ncoef : nullptr;
+    int16_t *ec = emit ? el + cu * cu : nullptr;
+    bool coded = true;
+    if (nd.intra) {
+        build_refs(S, L);
+        if (threadIdx.x == 0) { S.cl[0] = K_INTRA + nd.intra_mode; }
+        SYNC();
+        if (nd.dct_size) luma_jobs8(S, L, 1, ql, false, true, el);
+        else luma_jobs4(S, L, 1, ql, false, true, el);
+        SYNC();
+        if (nd.ch_intra) {
+            chroma_dc_pred(S, L, 0);
+            cfl_blend(S, L, 0);
+        } else if (P.ref_valid[0]) {
+            chroma_mc(S, P, L, 0, mvpx + L.px * 4, mvpy + L.py * 4, 0, false);
+        } else {
+            chroma_dc_pred(S, L, 0);
+        }
+        chroma_jobs(S, L, 1, 0, qc, false, true, ec);
+    } else {
+        int mvx, mvy;
+        if (nd.merge || nd.skip) { mvx = mvpx + L.px * 4; mvy = mvpy + L.py * 4; }
+        else { mvx = mvpx + L.px * 4 + nd.mvd_x; mvy = mvpy + L.py * 4 + nd.mvd_y; }
+        if (P.frame_type == 2) {
+            // B replay handled by the B-frame path (forward-only fallback).
+        }
+        if (!nd.skip) {
+            const int ri = nd.ref_sel & 3;
+            const int r = (ri < MAX_REFS && P.ref_valid[ri]) ? ri : 0;
+            if (threadIdx.x == 0) {
+                S.cand_mvx[0] = mvx; S.cand_mvy[0] = mvy; S.cand_ref[0] = r; S.cl[0] = 0;
+            }
+            SYNC();
+            const int slots[1] = {0};
+            luma_mc_slots(S, P, L, 1, slots);
+            if (nd.dct_size) luma_jobs8(S, L, 1, ql, false, true, el);
+            else luma_jobs4(S, L, 1, ql, false, true, el);
+            SYNC();
+            if (nd.ch_intra) {
+                chroma_dc_pred(S, L, 0);
+            } else {
+                chroma_mc(S, P, L, r, mvx, mvy, 0, false);
+            }
+            chroma_jobs(S, L, 1, 0, qc, false, true, ec);
+        } else {
+            coded = false;
+            const int n = cu * cu;
+            for (int i = threadIdx.x; i < n; i += NT) {
+                const int y = i / cu, x = i - y * cu;
+                LumaMC m;
+                m.init(P.ref_y[0], P.stride_y, P.W, P.H, mvx, mvy, cu);
+                RY(S, L.lx + x, L.ly + y) = (uint8_t)m.at(x, y);
+            }
+            SYNC();
+            if (P.fresh_skip && P.frame_type == 1 && P.ref_valid[0])
+                chroma_mc(S, P, L, 0, mvx, mvy, 0, true);
+        }
+    }
+    SYNC();
+    if (emit && coded && threadIdx.x == 0) S.ncoef += cu * cu + (cu * cu >> 1);
+    grid_update(S, L, nd, mvpx, mvpy);
+}
+
+// ====================================================================
+// Leaf decision (reference src/encoder.c:784-1277).
+// ====================================================================
+__device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
+                                 const QuantParams &ql, const QuantParams &qc) {
+    const int cu = L.cu, tid = threadIdx.x;
+    const bool fast = P.preset <= 1;
+    const bool medium = P.preset >= 2;
+    const bool key = P.frame_type == 0;
+    const bool is_p = P.frame_type == 1;
+    int mvpx, mvpy;
+    mvp_at(S.grid, L.cx, L.cy, mvpx, mvpy);
+    build_refs(S, L);
+    zero_acc(S);
+
+    // ---- candidate set -------------------------------------------------
+    const int sr = fast ? 16 : 24;
+    bool has_glb = false, has_tmp = false, has_me1 = false;
+    int tdx = 0, tdy = 0;
+    if (is_p) {
+        has_me1 = !fast && P.multiref && P.ref_valid[1];
+        has_glb = !fast && P.glob_valid &&
+                  (P.glob_x > 16 || P.glob_x < -16 || P.glob_y > 16 || P.glob_y < -16);
+        if (!fast && P.ref_valid[0] && P.prev_valid) {
+            const int fx = L.px >> 3, fy = L.py >> 3;
+            if (fx < P.grid_w && fy < P.grid_h) {
+                const MvCell pg = P.prev_grid[fy * P.grid_w + fx];
+                if (!pg.intra) { has_tmp = true; tdx = pg.dx; tdy = pg.dy; }
+            }
+        }
+        // ---- motion searches on four warp groups ------------------------
+        const int g = tid / GT, gt = tid - g * GT;
+        const int cx0 = (mvpx + L.px * 4) >> 2, cy0 = (mvpy + L.py * 4) >> 2;
+        if (g == 0)
+            me_run(S, 0, gt, P.ref_y[0], P.stride_y, P.W, P.H, L.lx, L.ly, cu, cx0, cy0, sr);
+        else if (g == 1 && has_me1)
+            me_run(S, 1, gt, P.ref_y[1], P.stride_y, P.W, P.H, L.lx, L.ly, cu, cx0, cy0, sr);
+        else if (g == 2 && has_glb)
+            me_run(S, 2, gt, P.ref_y[0], P.stride_y, P.W, P.H, L.lx, L.ly, cu,
+                   (L.px * 4 + P.glob_x) >> 2, (L.py * 4 + P.glob_y) >> 2, sr);
+        else if (g == 3 && has_tmp)
+            me_run(S, 3, gt, P.ref_y[0], P.stride_y, P.W, P.H, L.lx, L.ly, cu,
+                   (L.px * 4 + tdx) >> 2, (L.py * 4 + tdy) >> 2, sr);
+        SYNC();
+        if (has_glb && S.me[2].mvx == S.me[0].mvx && S.me[2].mvy == S.me[0].mvy) has_glb = false;
+        if (has_tmp && S.me[3].mvx == S.me[0].mvx && S.me[3].mvy == S.me[0].mvy) has_tmp = false;
+        // ---- inter predictions ------------------------------------------
+        int slots[5], ns = 0;
+        slots[ns++] = K_ME0;
+        if (has_me1) slots[ns++] = K_ME1;
+        if (has_glb) slots[ns++] = K_GLB;
+        if (has_tmp) slots[ns++] = K_TMP;
+        if (medium) slots[ns++] = K_MRG;
+        if (tid == 0) {
+            S.cand_mvx[K_ME0] = S.me[0].mvx; S.cand_mvy[K_ME0] = S.me[0].mvy; S.cand_ref[K_ME0] = 0;
+            S.cand_mvx[K_ME1] = S.me[1].mvx; S.cand_mvy[K_ME1] = S.me[1].mvy; S.cand_ref[K_ME1] = 1;
+            S.cand_mvx[K_GLB] = S.me[2].mvx; S.cand_mvy[K_GLB] = S.me[2].mvy; S.cand_ref[K_GLB] = 0;
+            S.cand_mvx[K_TMP] = S.me[3].mvx; S.cand_mvy[K_TMP] = S.me[3].mvy; S.cand_ref[K_TMP] = 0;
+            S.cand_mvx[K_MRG] = mvpx + L.px * 4; S.cand_mvy[K_MRG] = mvpy + L.py * 4; S.cand_ref[K_MRG] = 0;
+        }
+        SYNC();
+        luma_mc_slots(S, P, L, ns, slots);
+    }
+
+    // ---- residual coding / SAD proxies for every candidate --------------
+    const bool try_intra = key || cu <= 16 || medium;
+    const int step = P.preset == 0 ? 6 : (P.preset == 1 ? 3 : 1);
+    const bool use4 = medium && cu <= 32;
+    if (tid == 0) {
+        int n = 0;
+        if (is_p) {
+            S.cl[n++] = K_ME0;
+            if (has_me1) S.cl[n++] = K_ME1;
+            if (has_glb) S.cl[n++] = K_GLB;
+            if (has_tmp) S.cl[n++] = K_TMP;
+        }
+        const int ninter = n;
+        if (try_intra)
+            for (int mi = 0; mi < 18; ++mi) {
+                const int m = mi * step;
+                if (m >= 18) break;
+                S.cl[n++] = K_INTRA + m;
+            }
+        S.ncl = n;
+        S.flag = ninter;
+    }
+    SYNC();
+    const int ncl = S.ncl, ninter = S.flag;
+    if (fast) {
+        sad_jobs(S, L, ncl);
+        SYNC();
+    } else {
+        luma_jobs8(S, L, ncl, ql, true, false, nullptr);
+        if (use4) luma_jobs4(S, L, ncl, ql, true, false, nullptr);
+        SYNC();
+        if (is_p && medium) {
+            // Merge: 8x8 only (reference src/encoder.c:1051-1057), placed
+            // after the list so the list above stays a prefix.
+            if (tid == 0) { S.cl[0] = K_MRG; }
+            SYNC();
+            luma_jobs8(S, L, 1, ql, true, false, nullptr);
+            // Skip pre-check: luma SSE of the merge prediction.
+            long long acc = 0;
+            for (int p = tid; p < cu * cu; p += NT) {
+                const int y = p / cu, x = p - y * cu;
+                const int d = (int)S.cur_y[(L.ly + y) * 64 + L.lx + x] - (int)S.pred[K_MRG][p];
+                acc += d * d;
+            }
+            acc = __reduce_add_sync(0xffffffffu, (unsigned)acc);
+            if ((tid & 31) == 0 && acc) atomicAdd((unsigned long long *)&S.acc64[0], (unsigned long long)acc);
+            SYNC();
+            if (S.acc64[0] == 0 && P.ref_valid[0]) {
+                chroma_mc(S, P, L, 0, mvpx + L.px * 4, mvpy + L.py * 4, 0, false);
+                const int cs = cu >> 1;
+                long long ac = 0;
+                for (int p = tid; p < cs * cs; p += NT) {
+                    const int y = p / cs, x = p - y * cs;
+                    const int db = (int)S.cur_c[0][((L.ly >> 1) + y) * 32 + (L.lx >> 1) + x] - (int)S.cpred[0][p];
+                    const int dr = (int)S.cur_c[1][((L.ly >> 1) + y) * 32 + (L.lx >> 1) + x] - (int)S.cpred[1][p];
+                    ac += db * db + dr * dr;
+                }
+                ac = __reduce_add_sync(0xffffffffu, (unsigned)ac);
+                if ((tid & 31) == 0 && ac) atomicAdd((unsigned long long *)&S.acc64[1], (unsigned long long)ac);
+                SYNC();
+            } else if (tid == 0) {
+                S.acc64[1] = 1;   // no skip candidate
+            }
+            SYNC();
+        }
+    }
+
+    // ---- in-order candidate scan (strict <, first minimum wins) ---------
+    if (tid == 0) {
+        const long long lam = P.lambda;
+        long long best = (long long)1 << 60;
+        int b_intra = 0, b_skip = 0, b_merge = 0, b_dct = 1, b_ref = 0, b_mvdx = 0, b_mvdy = 0;
+        int b_imode = 1, best_imode = 1;
+        if (is_p) {
+            const int base_x = mvpx + L.px * 4, base_y = mvpy + L.py * 4;
+            // Explicit inter from the MVP centre.
+            {
+                const int dx = S.cand_mvx[K_ME0] - base_x, dy = S.cand_mvy[K_ME0] - base_y;
+                long long dl; int lb, dct = 1;
+                if (fast) {
+                    const long long sad = S.acc_sse[K_ME0][0];
+                    dl = (sad * sad) / (long long)(cu * cu);
+                    lb = 3;
+                } else {
+                    dl = best_of(S, K_ME0, use4, lam, lb, dct);
+                }
+                int bits = 6 + se_bits(dx) + se_bits(dy) + lb + (P.multiref ? 2 : 0);
+                const long long cost = dl + lam * bits;
+                if (cost < best) { best = cost; b_dct = dct; b_mvdx = dx; b_mvdy = dy; b_ref = 0; }
+            }
+            if (has_me1) {
+                const int dx = S.cand_mvx[K_ME1] - base_x, dy = S.cand_mvy[K_ME1] - base_y;
+                int lb, dct;
+                const long long dl = best_of(S, K_ME1, use4, lam, lb, dct);
+                const int bits = 8 + se_bits(dx) + se_bits(dy) + lb;
+                const long long cost = dl + lam * bits;
+                if (cost < best) { best = cost; b_dct = dct; b_mvdx = dx; b_mvdy = dy; b_ref = 1; }
+            }
+            if (has_glb) {
+                const int dx = S.cand_mvx[K_GLB] - base_x, dy = S.cand_mvy[K_GLB] - base_y;
+                int lb, dct;
+                const long long dl = best_of(S, K_GLB, use4, lam, lb, dct);
+                const int bits = 6 + se_bits(dx) + se_bits(dy) + lb + (P.multiref ? 1 : 0);
+                const long long cost = dl + lam * bits;
+                if (cost < best) { best = cost; b_dct = dct; b_mvdx = dx; b_mvdy = dy; b_ref = 0; }
+            }
+            if (has_tmp) {
+                const int dx = S.cand_mvx[K_TMP] - base_x, dy = S.cand_mvy[K_TMP] - base_y;
+                int lb, dct;
+                const long long dl = best_of(S, K_TMP, use4, lam, lb, dct);
+                const int bits = 6 + se_bits(dx) + se_bits(dy) + lb + (P.multiref ? 2 : 0);
+                const long long cost = dl + lam * bits;
+                if (cost < best) { best = cost; b_dct = dct; b_mvdx = dx; b_mvdy = dy; b_ref = 0; }
+            }
+            if (medium) {
+                const long long dl = S.acc_sse[K_MRG][0];
+                const int bits = 6 + S.acc_bits[K_MRG][0];
+                const long long cost = dl + lam * bits;
+                if (cost < best) {
+                    best = cost; b_merge = 1; b_dct = 1; b_ref = 0;
+                    b_mvdx = S.cand_mvx[K_ME0] - base_x; b_mvdy = S.cand_mvy[K_ME0] - base_y;
+                }
+                if (!fast && P.ref_valid[0] && S.acc64[0] == 0 && S.acc64[1] == 0) {
+                    const long long cost_skip = lam * 2;
+                    if (cost_skip < best) {
+                        best = cost_skip; b_skip = 1; b_merge = 0; b_dct = 1; b_mvdx = 0; b_mvdy = 0; b_ref = 0;
+                    }
+                }
+            }
+        }
+        if (try_intra) {
+            for (int k = ninter; k < ncl; ++k) {
+                const int slot = S.cl[k], m = slot - K_INTRA;
+                long long dl; int lb, dct = 1;
+                if (fast) {
+                    const long long sad = S.acc_sse[slot][0];
+                    dl = (sad * sad) / (long long)(cu * cu);
+                    lb = 8;
+                } else {
+                    dl = best_of(S, slot, use4, lam, lb, dct);
+                }
+                const long long cost = dl + lam * (8 + lb);
+                if (cost < best) {
+                    best = cost; b_intra = 1; best_imode = m; b_dct = dct; b_skip = 0; b_merge = 0;
+                    b_mvdx = 0; b_mvdy = 0; b_ref = 0;
+                }
+            }
+            if (b_intra) b_imode = best_imode;
+        }
+        Node &nd = S.nodes[qt_index(L.depth, L.cx, L.cy)];
+        nd.intra = (uint8_t)b_intra; nd.skip = (uint8_t)b_skip; nd.merge = (uint8_t)b_merge; nd.bi = 0;
+        nd.intra_mode = (uint8_t)b_imode; nd.intra_cmode = 0; nd.ch_intra = 0;
+        nd.ref_sel = (uint8_t)b_ref; nd.dct_size = (uint8_t)b_dct;
+        nd.mvd_x = (int16_t)b_mvdx; nd.mvd_y = (int16_t)b_mvdy;
+        nd.split = 0;
+        S.best_cost = best;
+    }
+    SYNC();
+
+    // ---- intra chroma choice: MC vs CfL-blended DC (src/encoder.c:1194-1221)
+    const Node nd0 = S.nodes[qt_index(L.depth, L.cx, L.cy)];
+    if (nd0.intra && !fast && medium) {
+        if (tid == 0) S.cl[0] = K_INTRA + nd0.intra_mode;
+        SYNC();
+        if (nd0.dct_size) luma_jobs8(S, L, 1, ql, false, true, nullptr);
+        else luma_jobs4(S, L, 1, ql, false, true, nullptr);
+        SYNC();
+        if (P.ref_valid[0]) chroma_mc(S, P, L, 0, mvpx + L.px * 4, mvpy + L.py * 4, 0, false);
+        else chroma_dc_pred(S, L, 0);
+        chroma_dc_pred(S, L, 2);
+        cfl_blend(S, L, 2);
+        zero_acc(S);
+        SYNC();
+        chroma_jobs(S, L, 2, 0, qc, true, false, nullptr);
+        SYNC();
+        if (tid == 0) {
+            const long long lam = P.lambda;
+            const long long dmc = S.acc_sse[0][0], dcfl = S.acc_sse[1][0];
+            const int lbmc = S.acc_bits[0][0], lbcfl = S.acc_bits[1][0];
+            if (dcfl + lam * (lbcfl + 4) < dmc + lam * (lbmc + 1))
+                S.nodes[qt_index(L.depth, L.cx, L.cy)].ch_intra = 1;
+        }
+        SYNC();
+    }
+    const long long best = S.best_cost;
+    // ---- replay of the winner ------------------------------------------
+    leaf_code(S, P, L, ql, qc, false, nullptr);
+    return best;
+}
+
+// ====================================================================
+// Quadtree recursion (reference src/encoder.c:1292-1397).
+// ====================================================================
+template <int D>
+__device__ void qt_decide(Smem &S, const FrameParams &P, int ctu_x, int ctu_y, int cx, int cy,
+                          const QuantParams &ql, const QuantParams &qc) {
+    constexpr int cu = 64 >> D;
+    const int px = ctu_x + cx * 8, py = ctu_y + cy * 8;
+    const bool in_frame = px + cu <= P.W && py + cu <= P.H;
+    Node &nd = S.nodes[qt_index(D, cx, cy)];
+    if constexpr (D < 3) {
+        constexpr int h = 4 >> D;   // child offset in cells
+        if (!in_frame) {
+            for (int q = 0; q < 4; ++q)
+                qt_decide<D + 1>(S, P, ctu_x, ctu_y, cx + (q & 1) * h, cy + (q >> 1) * h, ql, qc);
+            return;
+        }
+        const int fast_leaf_depth = P.preset == 0 ? 3 : 2;
+        if (P.preset <= 1 && D < fast_leaf_depth) {
+            if (threadIdx.x == 0) nd.split = 1;
+            SYNC();
+            for (int q = 0; q < 4; ++q)
+                qt_decide<D + 1>(S, P, ctu_x, ctu_y, cx + (q & 1) * h, cy + (q >> 1) * h, ql, qc);
+            return;
+        }
+        const Leaf L(P, ctu_x, ctu_y, D, cx, cy);
+        snap<D>(S, L, 0, true);
+        const long long parent = leaf_decide(S, P, L, ql, qc);
+        snap<D>(S, L, 1, true);
+        snap<D>(S, L, 0, false);
+        long long child = 0;
+        for (int q = 0; q < 4; ++q) {
+            const Leaf C(P, ctu_x, ctu_y, D + 1, cx + (q & 1) * h, cy + (q >> 1) * h);
+            child += leaf_decide(S, P, C, ql, qc);
+        }
+        if (child <= parent) {
+            if (threadIdx.x == 0) nd.split = 1;
+            snap<D>(S, L, 0, false);
+            for (int q = 0; q < 4; ++q)
+                qt_decide<D + 1>(S, P, ctu_x, ctu_y, cx + (q & 1) * h, cy + (q >> 1) * h, ql, qc);
+        } else {
+            if (threadIdx.x == 0) nd.split = 0;
+            snap<D>(S, L, 1, false);
+        }
+    } else {
+        if (!in_frame) return;
+        const Leaf L(P, ctu_x, ctu_y, D, cx, cy);
+        leaf_decide(S, P, L, ql, qc);
+        if (threadIdx.x == 0) nd.split = 0;
+        SYNC();
+    }
+}
+
+template <int D>
+__device__ void qt_write(Smem &S, const FrameParams &P, int ctu_x, int ctu_y, int cx, int cy,
+                         const QuantParams &ql, const QuantParams &qc, CtuOut *out) {
+    constexpr int cu = 64 >> D;
+    const int px = ctu_x + cx * 8, py = ctu_y + cy * 8;
+    const bool in_frame = px + cu <= P.W && py + cu <= P.H;
+    if constexpr (D < 3) {
+        constexpr int h = 4 >> D;
+        if (!in_frame || S.nodes[qt_index(D, cx, cy)].split) {
+            if (!in_frame && false) return;
+            for (int q = 0; q < 4; ++q)
+                qt_write<D + 1>(S, P, ctu_x, ctu_y, cx + (q & 1) * h, cy + (q >> 1) * h, ql, qc, out);
+            return;
+        }
+    } else {
+        if (!in_frame) return;
+    }
+    const Leaf L(P, ctu_x, ctu_y, D, cx, cy);
+    leaf_code(S, P, L, ql, qc, true, out);
+}
+
+// ====================================================================
+// In-loop filters on the CTU tile.
+// ====================================================================
+__device__ void deblock_tile(Smem &S, int qp) {
+    const int tc = clampi(qp / 3, 1, 10);
+    const int cqp = clampi(qp - 1, 0, 63), ctc = clampi(cqp / 4, 1, 6);
+    // Luma vertical edges x = 4..60 and chroma (Cb) vertical edges x = 4..28.
+    for (int i = threadIdx.x; i < 15 * 64 + 7 * 32; i += NT) {
+        if (i < 15 * 64) {
+            const int e = i / 64 + 1, r = i - (e - 1) * 64, x = e * 4;
+            const int p1 = RY(S, x - 2, r), p0 = RY(S, x - 1, r), q0 = RY(S, x, r), q1 = RY(S, x + 1, r);
+            if (edge_strength(p0, q0, qp)) {
+                RY(S, x - 1, r) = (uint8_t)weak_filter(p1, p0, q0, q1, tc);
+                RY(S, x, r) = (uint8_t)weak_filter(q1, q0, p0, p1, tc);
+            }
+        } else {
+            const int k = i - 15 * 64, e = k / 32 + 1, r = k - (e - 1) * 32, x = e * 4;
+            const int p0 = RC(S, 0, x - 1, r), q0 = RC(S, 0, x, r);
+            if (edge_strength(p0, q0, cqp)) {
+                const int d = clampi((q0 - p0 + 1) >> 1, -ctc, ctc);
+                RC(S, 0, x - 1, r) = (uint8_t)clampi(p0 + d, 0, 255);
+                RC(S, 0, x, r) = (uint8_t)clampi(q0 - d, 0, 255);
+            }
+        }
+    }
+    SYNC();
+    // Luma horizontal edges; chroma horizontal edges filter rows y, y+1
+    // with the Cr strength for both planes (reference src/filter.c:212-236).
+    for (int i = threadIdx.x; i < 15 * 64 + 7 * 32; i += NT) {
+        if (i < 15 * 64) {
+            const int e = i / 64 + 1, c = i - (e - 1) * 64, y = e * 4;
+            const int p1 = RY(S, c, y - 2), p0 = RY(S, c, y - 1), q0 = RY(S, c, y), q1 = RY(S, c, y + 1);
+            if (edge_strength(p0, q0, qp)) {
+                RY(S, c, y - 1) = (uint8_t)weak_filter(p1, p0, q0, q1, tc);
+                RY(S, c, y) = (uint8_t)weak_filter(q1, q0, p0, p1, tc);
+            }
+        } else {
+            const int k = i - 15 * 64, e = k / 32 + 1, c = k - (e - 1) * 32, y = e * 4;
+            const int p0 = RC(S, 1, c, y), q0 = RC(S, 1, c, y + 1);
+            const int pb = RC(S, 0, c, y), qb = RC(S, 0, c, y + 1);
+            if (edge_strength(p0, q0, cqp)) {
+                int d = clampi((q0 - p0 + 1) >> 1, -ctc, ctc);
+                RC(S, 1, c, y) = (uint8_t)clampi(p0 + d, 0, 255);
+                RC(S, 1, c, y + 1) = (uint8_t)clampi(q0 - d, 0, 255);
+                d = clampi((qb - pb + 1) >> 1, -ctc, ctc);
+                RC(S, 0, c, y) = (uint8_t)clampi(pb + d, 0, 255);
+                RC(S, 0, c, y + 1) = (uint8_t)clampi(qb - d, 0, 255);
+            }
+        }
+    }
+    SYNC();
+}
+
+// Luma SAO band offset: choose (reference src/filter.c:269-319), rate gate
+// (src/encoder.c:1473-1493) and apply (src/filter.c:251-266).
+__device__ void sao_tile(Smem &S, int w, int h, int lambda_sao) {
+    if (threadIdx.x < 32) {
+        S.band_sum[threadIdx.x] = 0; S.band_cnt[threadIdx.x] = 0;
+        S.band_sq[threadIdx.x] = 0; S.band_new[threadIdx.x] = 0;
+    }
+    SYNC();
+    for (int i = threadIdx.x; i < w * h; i += NT) {
+        const int y = i / w, x = i - y * w;
+        const int o = S.cur_y[y * 64 + x], r = RY(S, x, y), d = o - r, b = r >> 3;
+        atomicAdd(&S.band_sum[b], d);
+        atomicAdd(&S.band_cnt[b], 1);
+        atomicAdd(&S.band_sq[b], d * d);
+    }
+    SYNC();
+    for (int i = threadIdx.x; i < w * h; i += NT) {
+        const int y = i / w, x = i - y * w;
+        const int o = S.cur_y[y * 64 + x], r = RY(S, x, y), b = r >> 3;
+        const int cnt = S.band_cnt[b], sum = S.band_sum[b];
+        int cand = (sum + (sum >= 0 ? cnt / 2 : -(cnt / 2))) / cnt;
+        cand = clampi(cand, -7, 7);
+        if (cand) {
+            const int d = o - clampi(r + cand, 0, 255);
+            atomicAdd(&S.band_new[b], d * d);
+        }
+    }
+    SYNC();
+    if (threadIdx.x == 0) {
+        long long base = 0;
+        for (int b = 0; b < 32; ++b) base += S.band_sq[b];
+        long long best = base;
+        int bb = 0, bo = 0;
+        for (int b = 0; b < 32; ++b) {
+            const int cnt = S.band_cnt[b];
+            if (!cnt) continue;
+            const int sum = S.band_sum[b];
+            int cand = clampi((sum + (sum >= 0 ? cnt / 2 : -(cnt / 2))) / cnt, -7, 7);
+            if (!cand) continue;
+            const long long sse = base - S.band_sq[b] + S.band_new[b];
+            if (sse < best) { best = sse; bb = b; bo = cand; }
+        }
+        int has = best < base;
+        if (has && best + (long long)lambda_sao * 6 >= base) has = 0;
+        S.sao[0] = has; S.sao[1] = has ? bb : 0; S.sao[2] = has ? bo : 0;
+    }
+    SYNC();
+    if (S.sao[0]) {
+        const int band = S.sao[1], off = S.sao[2];
+        for (int i = threadIdx.x; i < w * h; i += NT) {
+            const int y = i / w, x = i - y * w;
+            uint8_t &p = RY(S, x, y);
+            if ((p >> 3) == band) p = (uint8_t)clampi(p + off, 0, 255);
+        }
+    }
+    SYNC();
+}
+
+// ====================================================================
+// The CTU kernel.  items[i] = (stream << 20) | (row << 10) | col.
+// ====================================================================
+__global__ void __launch_bounds__(NT, 1)
+ctu_kernel(const FrameParams *__restrict__ params, const int *__restrict__ items) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    Smem &S = *reinterpret_cast<Smem *>(smem_raw);
+    __shared__ FrameParams P;
+    const int item = items[blockIdx.x];
+    const int sid = item >> 20, row = (item >> 10) & 1023, col = item & 1023;
+    if (threadIdx.x == 0) P = params[sid];
+    SYNC();
+    const int ctu_x = col * 64, ctu_y = row * 64;
+    const int w = mini(64, P.W - ctu_x), h = mini(64, P.H - ctu_y);
+    const int wc = w >> 1, hc = h >> 1;
+    // ---- load source and the filtered neighbour border ----------------
+    for (int i = threadIdx.x; i < 64 * 64; i += NT) {
+        const int y = i >> 6, x = i & 63;
+        S.cur_y[i] = (x < w && y < h) ? P.cur_y[(size_t)(ctu_y + y) * P.stride_y + ctu_x + x] : 0;
+    }
+    for (int i = threadIdx.x; i < 2 * 32 * 32; i += NT) {
+        const int c = i >> 10, p = i & 1023, y = p >> 5, x = p & 31;
+        const uint8_t *src = c ? P.cur_cr : P.cur_cb;
+        S.cur_c[c][p] = (x < wc && y < hc) ? src[(size_t)((ctu_y >> 1) + y) * P.stride_c + (ctu_x >> 1) + x] : 0;
+    }
+    if (ctu_y > 0) {
+        for (int x = threadIdx.x - 2; x < w; x += NT)
+            if (ctu_x + x >= 0) RY(S, x, -1) = P.rec_y[(size_t)(ctu_y - 1) * P.stride_y + ctu_x + x];
+        for (int i = threadIdx.x; i < 2 * 33; i += NT) {
+            const int c = i / 33, x = i - c * 33 - 1;
+            const uint8_t *src = c ? P.rec_cr : P.rec_cb;
+            if (x < wc && ctu_x / 2 + x >= 0)
+                RC(S, c, x, -1) = src[(size_t)((ctu_y >> 1) - 1) * P.stride_c + (ctu_x >> 1) + x];
+        }
+    }
+    if (ctu_x > 0) {
+        for (int i = threadIdx.x; i < 2 * h; i += NT) {
+            const int y = i >> 1, x = (i & 1) - 2;
+            RY(S, x, y) = P.rec_y[(size_t)(ctu_y + y) * P.stride_y + ctu_x + x];
+        }
+        for (int i = threadIdx.x; i < 2 * hc; i += NT) {
+            const int c = i / hc, y = i - c * hc;
+            const uint8_t *src = c ? P.rec_cr : P.rec_cb;
+            RC(S, c, -1, y) = src[(size_t)((ctu_y >> 1) + y) * P.stride_c + (ctu_x >> 1) - 1];
+        }
+    }
+    for (int i = threadIdx.x; i < 64; i += NT) {
+        S.grid[i].dx = 0; S.grid[i].dy = 0; S.grid[i].intra = 1; S.grid[i].pad = 0;
+    }
+    for (int i = threadIdx.x; i < QT_NODES; i += NT) {
+        Node z = {};
+        S.nodes[i] = z;
+    }
+    if (threadIdx.x == 0) S.ncoef = 0;
+    SYNC();
+
+    QuantParams ql, qc;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        ql.eff[b] = P.eff_l[b]; ql.rcp[b] = P.rcp_l[b];
+        qc.eff[b] = P.eff_c[b]; qc.rcp[b] = P.rcp_c[b];
+    }
+    ql.lambda = P.lambda;
+    qc.lambda = P.lambda_c;
+
+    // ---- decide, then write in syntax order ----------------------------
+    qt_decide<0>(S, P, ctu_x, ctu_y, 0, 0, ql, qc);
+    for (int i = threadIdx.x; i < 64; i += NT) {
+        S.grid[i].dx = 0; S.grid[i].dy = 0; S.grid[i].intra = 1;
+    }
+    SYNC();
+    CtuOut *out = P.out + row * P.ctu_cols + col;
+    qt_write<0>(S, P, ctu_x, ctu_y, 0, 0, ql, qc, out);
+    SYNC();
+    // ---- in-loop filters ------------------------------------------------
+    if (w == 64 && h == 64) deblock_tile(S, P.qp);
+    sao_tile(S, w, h, P.lambda_sao);
+    // ---- exports --------------------------------------------------------
+    for (int i = threadIdx.x; i < w * h; i += NT) {
+        const int y = i / w, x = i - y * w;
+        P.rec_y[(size_t)(ctu_y + y) * P.stride_y + ctu_x + x] = RY(S, x, y);
+    }
+    for (int i = threadIdx.x; i < 2 * wc * hc; i += NT) {
+        const int c = i / (wc * hc), p = i - c * wc * hc, y = p / wc, x = p - y * wc;
+        uint8_t *dst = c ? P.rec_cr : P.rec_cb;
+        dst[(size_t)((ctu_y >> 1) + y) * P.stride_c + (ctu_x >> 1) + x] = RC(S, c, x, y);
+    }
+    for (int i = threadIdx.x; i < 64; i += NT) {
+        const int gy = i >> 3, gx = i & 7;
+        const int fy = row * 8 + gy, fx = col * 8 + gx;
+        if (fy < P.grid_h && fx < P.grid_w) P.cur_grid[fy * P.grid_w + fx] = S.grid[i];
+    }
+    for (int i = threadIdx.x; i < QT_NODES; i += NT) out->nodes[i] = S.nodes[i];
+    if (threadIdx.x == 0) {
+        out->ncoef = S.ncoef;
+        out->sao_has = (int16_t)S.sao[0];
+        out->sao_band = (int16_t)S.sao[1];
+        out->sao_offset = (int16_t)S.sao[2];
+    }
+}
+
+cudaError_t init_engine_tables() {
+    cudaError_t e = upload_dct_tables();
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(ctu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(Smem));
+}
+
+size_t ctu_smem_bytes() { return sizeof(Smem); }
+
+cudaError_t launch_ctu_items(const FrameParams *d_params, const int *d_items, int n,
+                             cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    ctu_kernel<<<n, NT, sizeof(Smem), st>>>(d_params, d_items);
+    return cudaGetLastError();
+}
+
+}  // namespace tcb

@@ -1,0 +1,21 @@
+// tcb_launch.h — host-callable launch wrappers of the sm_100a kernels.
+#pragma once
+#include <math.h>
+#include <cuda_runtime.h>
+
+#include "tcb_common.cuh"
+
+namespace tcb {
+
+cudaError_t init_device_tables();
+cudaError_t init_engine_tables();
+cudaError_t init_unit_tables();
+size_t ctu_smem_bytes();
+cudaError_t launch_ctu_items(const FrameParams *d_params, const int *d_items, int n, cudaStream_t st);
+cudaError_t launch_glob_mv(const uint8_t *cur, const uint8_t *ref, int W, int H, int s,
+                           FrameParams *d_params, cudaStream_t st);
+cudaError_t launch_hist16(const uint8_t *y, int W, int H, int s, int *d_hist, cudaStream_t st);
+cudaError_t launch_frame_sse(const uint8_t *a, const uint8_t *b, int W, int H, int s,
+                             unsigned long long *d_out, cudaStream_t st);
+
+}  // namespace tcb

@@ -1,0 +1,247 @@
+// tcb_resid.cuh — fused residual path of one transform unit on a group of
+// lanes of one warp: forward DCT-II (14-bit, two rounded passes) -> JND-band
+// dead-zone quantisation -> RDOQ-lite (keep-vs-zero of |level| == 1) ->
+// bit-model estimate -> centroid dequantisation -> inverse DCT.
+//
+//   8x8 TU: an "octet" of 8 consecutive lanes, lane r owns row r on the
+//           row pass and column r afterwards.
+//   4x4 TU: a "quad" of 4 consecutive lanes, same ownership.
+//
+// The row<->column exchange goes through a 64-int (octet) / 16-int (quad)
+// shared-memory scratch private to the lane group.  All 32 lanes of the
+// warp must call these routines together (they use full-mask shuffles of
+// width 8 / 4); inactive groups pass dummy data and discard the results.
+//
+// Arithmetic follows reference src/transform.c:331-439 (dct4_point,
+// dct8_point2, tc_fdct*/tc_idct*_res), src/encoder.c:333-385 (rdoq_level1,
+// count_siglevel_bits, lastpos_cost) and tcodec_common.h:226-246
+// (quant/dequant).  Accumulators are 32-bit: encoder residuals are clipped
+// to [-512, 511], so |coef| <= 4096, |dequant| <= 4096 + eff/2 <= 8037, and
+// the largest inverse-pass sum is 8037 * 43284 / 2^14 * 43284 < 2^30.
+#pragma once
+#include <math.h>
+#include <cuda_runtime.h>
+#include "tcb_common.cuh"
+
+namespace tcb {
+
+// DCT matrices: one copy per translation unit (no relocatable device
+// code); each unit that launches kernels using them uploads its copy with
+// upload_dct_tables() before its first launch.
+static __constant__ int c_dct4[4][4];
+static __constant__ int c_dct8[8][8];
+
+// Orthonormal DCT-II matrix in 14-bit fixed point:
+// m[k][n] = round(2^14 * s_k * cos((2n+1) k pi / 2N)), s_0 = sqrt(1/N),
+// s_k = sqrt(2/N).  Equals the reference tables of src/transform.c:313-329.
+inline void dct_matrix(int N, int *m) {
+    const double pi = 3.14159265358979323846;
+    for (int k = 0; k < N; ++k)
+        for (int n = 0; n < N; ++n) {
+            const double s = k == 0 ? sqrt(1.0 / N) : sqrt(2.0 / N);
+            m[k * N + n] = (int)lround(16384.0 * s * cos((2 * n + 1) * k * pi / (2.0 * N)));
+        }
+}
+
+static inline cudaError_t upload_dct_tables() {
+    int d4[4][4], d8[8][8];
+    dct_matrix(4, &d4[0][0]);
+    dct_matrix(8, &d8[0][0]);
+    cudaError_t e = cudaMemcpyToSymbol(c_dct4, d4, sizeof(d4));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyToSymbol(c_dct8, d8, sizeof(d8));
+}
+
+struct QuantParams {
+    int eff[4];
+    uint32_t rcp[4];
+    long long lambda;     // RDOQ lambda
+};
+
+__device__ __forceinline__ int oct_sum(int v) {
+    v += __shfl_xor_sync(0xffffffffu, v, 4, 8);
+    v += __shfl_xor_sync(0xffffffffu, v, 2, 8);
+    v += __shfl_xor_sync(0xffffffffu, v, 1, 8);
+    return v;
+}
+__device__ __forceinline__ int oct_max(int v) {
+    v = max(v, __shfl_xor_sync(0xffffffffu, v, 4, 8));
+    v = max(v, __shfl_xor_sync(0xffffffffu, v, 2, 8));
+    v = max(v, __shfl_xor_sync(0xffffffffu, v, 1, 8));
+    return v;
+}
+__device__ __forceinline__ int quad_sum(int v) {
+    v += __shfl_xor_sync(0xffffffffu, v, 2, 4);
+    v += __shfl_xor_sync(0xffffffffu, v, 1, 4);
+    return v;
+}
+__device__ __forceinline__ int quad_max(int v) {
+    v = max(v, __shfl_xor_sync(0xffffffffu, v, 2, 4));
+    v = max(v, __shfl_xor_sync(0xffffffffu, v, 1, 4));
+    return v;
+}
+
+// Quantise + RDOQ-lite one coefficient at raster position `pos` of an
+// n-coefficient TU (reference src/encoder.c:333-355).
+__device__ __forceinline__ int quant_rdoq(int c, int pos, int n, const QuantParams &qp) {
+    const int band = freq_band(pos, n);
+    const int eff = qp.eff[band];
+    int q = quant_coeff(c, eff, qp.rcp[band]);
+    if (q == 1 || q == -1) {
+        const int dq = dequant_coeff(q, eff);
+        const long long dz = (long long)c * c + qp.lambda;
+        const long long dk = (long long)(c - dq) * (c - dq) + 2 * qp.lambda;
+        if (dz < dk) q = 0;
+    }
+    return q;
+}
+
+// Bit-model term of one quantised level (reference src/encoder.c:360-370).
+__device__ __forceinline__ int level_bits(int v) {
+    return v == 0 ? 1 : 2 + 2 * bitlen((unsigned)absi(v));
+}
+
+// 8x8 TU on an octet.  In: res_row = clipped residual row `l8`.
+// Out: q_col[k] = quantised level at (k, l8); r_col[k] = reconstructed
+// residual at (k, l8) (int16-wrapped like tc_coeff_t); returns the bit
+// estimate 1 + 2*nz + sig/level bits + last-position cost (uniform).
+__device__ __forceinline__ int tu8_code(int l8, const int res_row[8], int *scr,
+                                        const QuantParams &qp, int q_col[8], int r_col[8]) {
+    int t[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        int acc = 0;
+#pragma unroll
+        for (int n = 0; n < 8; ++n) acc += c_dct8[k][n] * res_row[n];
+        t[k] = (acc + 8192) >> 14;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) scr[l8 * 8 + k] = t[k];
+    __syncwarp();
+    int col[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) col[i] = scr[i * 8 + l8];
+    __syncwarp();
+    int nz = 0, last = -1;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        int acc = 0;
+#pragma unroll
+        for (int n = 0; n < 8; ++n) acc += c_dct8[k][n] * col[n];
+        const int c = (int16_t)((acc + 8192) >> 14);
+        const int pos = k * 8 + l8;
+        const int q = (int16_t)quant_rdoq(c, pos, 64, qp);
+        q_col[k] = q;
+        if (q) { ++nz; last = pos; }
+    }
+    nz = oct_sum(nz);
+    last = oct_max(last);
+    int lb = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        if (k * 8 + l8 <= last) lb += level_bits(q_col[k]);
+    lb = oct_sum(lb);
+    const int bits = 1 + 2 * nz + lb + lastpos_cost(last);
+    // Dequantise and hand columns back as rows for the inverse row pass.
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int pos = k * 8 + l8;
+        scr[pos] = (int16_t)dequant_coeff(q_col[k], qp.eff[freq_band(pos, 64)]);
+    }
+    __syncwarp();
+    int row[8];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) row[n] = scr[l8 * 8 + n];
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        int acc = 0;
+#pragma unroll
+        for (int n = 0; n < 8; ++n) acc += c_dct8[n][k] * row[n];
+        scr[l8 * 8 + k] = (acc + 8192) >> 14;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int n = 0; n < 8; ++n) col[n] = scr[n * 8 + l8];
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        int acc = 0;
+#pragma unroll
+        for (int n = 0; n < 8; ++n) acc += c_dct8[n][k] * col[n];
+        r_col[k] = (int16_t)((acc + 8192) >> 14);
+    }
+    return bits;
+}
+
+// 4x4 TU on a quad (lane l4 owns row / column l4).  Same contract as
+// tu8_code with n = 16 coefficients.
+__device__ __forceinline__ int tu4_code(int l4, const int res_row[4], int *scr,
+                                        const QuantParams &qp, int q_col[4], int r_col[4]) {
+    int t[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int acc = 0;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) acc += c_dct4[k][n] * res_row[n];
+        t[k] = (acc + 8192) >> 14;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) scr[l4 * 4 + k] = t[k];
+    __syncwarp();
+    int col[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) col[i] = scr[i * 4 + l4];
+    __syncwarp();
+    int nz = 0, last = -1;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int acc = 0;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) acc += c_dct4[k][n] * col[n];
+        const int c = (int16_t)((acc + 8192) >> 14);
+        const int pos = k * 4 + l4;
+        const int q = (int16_t)quant_rdoq(c, pos, 16, qp);
+        q_col[k] = q;
+        if (q) { ++nz; last = pos; }
+    }
+    nz = quad_sum(nz);
+    last = quad_max(last);
+    int lb = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (k * 4 + l4 <= last) lb += level_bits(q_col[k]);
+    lb = quad_sum(lb);
+    const int bits = 1 + 2 * nz + lb + lastpos_cost(last);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int pos = k * 4 + l4;
+        scr[pos] = (int16_t)dequant_coeff(q_col[k], qp.eff[freq_band(pos, 16)]);
+    }
+    __syncwarp();
+    int row[4];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) row[n] = scr[l4 * 4 + n];
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int acc = 0;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) acc += c_dct4[n][k] * row[n];
+        scr[l4 * 4 + k] = (acc + 8192) >> 14;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int n = 0; n < 4; ++n) col[n] = scr[n * 4 + l4];
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int acc = 0;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) acc += c_dct4[n][k] * col[n];
+        r_col[k] = (int16_t)((acc + 8192) >> 14);
+    }
+    return bits;
+}
+
+}  // namespace tcb

@@ -1,0 +1,129 @@
+"""Seeded synthetic 4:2:0 sources standing in for the benchmark clips.
+
+The reference's published numbers use real clips that are not available
+here; these generators reproduce the shapes, motion and value
+distributions the benchmark configurations describe:
+
+* ``sinusoid_clip`` — 128 + a sum of 8 random 2-D sinusoids (periods
+  8..64 px, amplitudes 10..40, random orientation and phase), translated
+  every frame by a fixed global motion with separable bicubic (Keys,
+  a = -0.5) resampling, plus Gaussian noise, clamped to [0, 255].  Chroma
+  is generated the same way at half resolution from a second seed with
+  half the motion.
+* ``moving_rects_clip`` — the sinusoid background plus 16 axis-aligned
+  rectangles (32..160 px sides) of uniform 0..255 noise texture, each with
+  its own velocity drawn from [-6, 6]^2 px/frame.
+
+Everything is deterministic in the seeds.
+"""
+from __future__ import annotations
+
+from typing import List, Tuple
+
+import numpy as np
+
+Frame = Tuple[np.ndarray, np.ndarray, np.ndarray]
+
+
+def _texture(h: int, w: int, seed: int, n_waves: int = 8) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    out = np.full((h, w), 128.0)
+    for _ in range(n_waves):
+        period = rng.uniform(8.0, 64.0)
+        amp = rng.uniform(10.0, 40.0)
+        theta = rng.uniform(0.0, np.pi)
+        phase = rng.uniform(0.0, 2.0 * np.pi)
+        out += amp * np.sin(2.0 * np.pi * (xx * np.cos(theta) + yy * np.sin(theta)) / period + phase)
+    return out
+
+
+def _keys(t: np.ndarray) -> np.ndarray:
+    a = -0.5
+    t = np.abs(t)
+    return np.where(t <= 1, (a + 2) * t ** 3 - (a + 3) * t ** 2 + 1,
+                    np.where(t < 2, a * t ** 3 - 5 * a * t ** 2 + 8 * a * t - 4 * a, 0.0))
+
+
+def _shift_axis(img: np.ndarray, d: float, axis: int) -> np.ndarray:
+    """Sample img at (index - d) along axis with bicubic weights, edges
+    replicated."""
+    n = img.shape[axis]
+    base = np.floor(-d)
+    frac = -d - base
+    idx = np.arange(n)
+    out = np.zeros_like(img)
+    for k in range(-1, 3):
+        w = float(_keys(np.array(frac - k)))
+        src = np.clip(idx + int(base) + k, 0, n - 1)
+        out += w * np.take(img, src, axis=axis)
+    return out
+
+
+def _shifted(base: np.ndarray, dx: float, dy: float, h: int, w: int, margin: int) -> np.ndarray:
+    """Window of `base` (rendered with `margin` on each side) moved by
+    (dx, dy) px, cropped to h x w."""
+    img = _shift_axis(_shift_axis(base, dx, 1), dy, 0)
+    return img[margin:margin + h, margin:margin + w]
+
+
+def sinusoid_clip(width: int, height: int, frames: int, motion=(1.25, -0.5), noise_sigma: float = 2.0,
+                  seed_luma: int = 1, seed_chroma: int = 2, seed_noise: int = 3) -> List[Frame]:
+    return _render(width, height, frames, motion, noise_sigma, seed_luma, seed_chroma, seed_noise, None)
+
+
+def moving_rects_clip(width: int, height: int, frames: int, motion=(2.5, 0.75), noise_sigma: float = 3.0,
+                      seed_luma: int = 1, seed_chroma: int = 2, seed_noise: int = 3, seed_rects: int = 11,
+                      n_rects: int = 16) -> List[Frame]:
+    rng = np.random.default_rng(seed_rects)
+    rects = []
+    for _ in range(n_rects):
+        rw, rh = int(rng.integers(32, 161)), int(rng.integers(32, 161))
+        rw, rh = min(rw, width), min(rh, height)
+        x0, y0 = rng.uniform(0, width - rw), rng.uniform(0, height - rh)
+        vx, vy = rng.uniform(-6.0, 6.0), rng.uniform(-6.0, 6.0)
+        tex_y = rng.integers(0, 256, size=(rh, rw)).astype(np.float64)
+        tex_c = rng.integers(0, 256, size=(2, (rh + 1) // 2, (rw + 1) // 2)).astype(np.float64)
+        rects.append((rw, rh, x0, y0, vx, vy, tex_y, tex_c))
+    return _render(width, height, frames, motion, noise_sigma, seed_luma, seed_chroma, seed_noise, rects)
+
+
+def _render(width, height, frames, motion, sigma, seed_l, seed_c, seed_n, rects) -> List[Frame]:
+    vx, vy = motion
+    span = int(np.ceil(max(abs(vx), abs(vy)) * frames)) + 4
+    m = span
+    base_y = _texture(height + 2 * m, width + 2 * m, seed_l)
+    mc = span // 2 + 4
+    base_c = [_texture(height // 2 + 2 * mc, width // 2 + 2 * mc, seed_c * 1000 + k) for k in range(2)]
+    noise = np.random.default_rng(seed_n)
+    out: List[Frame] = []
+    for t in range(frames):
+        y = _shifted(base_y, vx * t, vy * t, height, width, m)
+        cb = _shifted(base_c[0], vx * t / 2, vy * t / 2, height // 2, width // 2, mc)
+        cr = _shifted(base_c[1], vx * t / 2, vy * t / 2, height // 2, width // 2, mc)
+        if rects:
+            for rw, rh, x0, y0, rvx, rvy, tex_y, tex_c in rects:
+                px = int(round(x0 + rvx * t)) % max(1, width - rw + 1)
+                py = int(round(y0 + rvy * t)) % max(1, height - rh + 1)
+                y[py:py + rh, px:px + rw] = tex_y
+                cx, cy = px // 2, py // 2
+                ch, cw = tex_c.shape[1], tex_c.shape[2]
+                ch, cw = min(ch, height // 2 - cy), min(cw, width // 2 - cx)
+                cb[cy:cy + ch, cx:cx + cw] = tex_c[0, :ch, :cw]
+                cr[cy:cy + ch, cx:cx + cw] = tex_c[1, :ch, :cw]
+        y = y + noise.normal(0.0, sigma, size=y.shape)
+        cb = cb + noise.normal(0.0, sigma, size=cb.shape)
+        cr = cr + noise.normal(0.0, sigma, size=cr.shape)
+        out.append(tuple(np.clip(np.rint(p), 0, 255).astype(np.uint8) for p in (y, cb, cr)))
+    return out
+
+
+def workload(name: str, frames: int = None, width: int = None, height: int = None) -> List[Frame]:
+    """Named workloads: 'cfg0' (320x240 sinusoid, motion (+1.25, -0.5),
+    sigma 2) and 'cfg1' (1280x720 sinusoid + rectangles, motion
+    (+2.5, +0.75), sigma 3)."""
+    if name == "cfg0":
+        return sinusoid_clip(width or 320, height or 240, frames or 30)
+    if name == "cfg1":
+        return moving_rects_clip(width or 1280, height or 720, frames or 60)
+    raise ValueError(name)
