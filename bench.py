@@ -1,0 +1,439 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 v2 encoder on the headline workload.
+
+Workload (the 1080p configuration the metric is quoted
+on): 1920x1080 4:2:0, GOP4 hierarchical B-frames, CQP QP 32, preset MEDIUM,
+profile 1 (two searched references: the reference encoder's reachable form
+of "4 references"), deblocking + SAO.  Source: seeded synthetic sinusoid
+texture + 16 moving noise rectangles + 1-px high-contrast lines over 5% of
+the area (tcodec_b200.synth 'cfg2').
+
+Batched form (the headline): --streams independent 1080p streams per GPU
+(default 16; stream s encodes clip frames s, s+1, ...) advance together and
+share every CTU-engine launch (tcb_batch_encode).  A step = one input frame
+for every stream; frames/s counts packets emitted in the timed region (GOP4
+emits one packet per input in steady state).  Every step reads fresh input
+frames of a device-resident clip.
+
+  value      frames/s of the batch with inputs already in HBM
+  e2e        the same through host (pinned) buffers: host->device copies and
+             packet / reconstruction read-back inside the timed region
+  plain_gpu  one stream alone through the same kernels
+
+--impl reference times the reference C encoder (oracle/_ref, built from the
+reference sources) on all host cores: one encoder process per core, each
+on its own segment of the clip, one input frame per process per step.
+
+Multi-GPU: one process per GPU (torchrun); every rank encodes its own
+independent streams (replicas, weak scaling, no collective on the data
+path); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import hashlib
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W, H, QP, PRESET, PROFILE = 1920, 1080, 32, 2, 1
+METRIC = "1080p v2 encode frames/s (bit-exact), batched/served vs plain GPU; p50/p99 latency"
+UNIT = "frames/s"
+GOLDEN = os.path.join(ROOT, "tests", "golden", "bench_1080p_gop4b.json")
+TRAFFIC = os.path.join(ROOT, "profiles", "ctu_engine_traffic.json")
+
+
+def make_clip(n):
+    from tcodec_b200 import synth
+    return synth.workload("cfg2", frames=n)
+
+
+def make_cfg(lib):
+    from tcodec_b200 import api
+    return api.make_config(lib, W, H, qp=QP, preset=PRESET, profile=PROFILE, keyframe_interval=1000,
+                           b_frames=True)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            p = [x.strip() for x in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- reference arm
+def _ref_worker(args):
+    seg, frames_needed, barrier, q, steps, warmup = args
+    from oracle import tcref
+    from tcodec_b200 import api
+    lib = tcref.ref_lib()
+    frames = make_clip(frames_needed)[seg:]
+    enc = api.Encoder(lib, make_cfg(lib))
+    i = 0
+    for _ in range(warmup):
+        enc.encode(*frames[i % len(frames)])
+        i += 1
+    barrier.wait()
+    t0 = time.perf_counter()
+    n = 0
+    for _ in range(steps):
+        if enc.encode(*frames[i % len(frames)]) is not None:
+            n += 1
+        i += 1
+    t1 = time.perf_counter()
+    barrier.wait()
+    enc.close()
+    q.put((n, t0, t1))
+
+
+def run_reference(steps, warmup, procs):
+    """Reference encoder on `procs` host processes; returns (frames/s,
+    frames, seconds)."""
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(procs)
+    q = ctx.Queue()
+    need = warmup + steps + procs
+    ps = [ctx.Process(target=_ref_worker, args=((k, need, barrier, q, steps, warmup),)) for k in range(procs)]
+    for p in ps:
+        p.start()
+    res = [q.get() for _ in ps]
+    for p in ps:
+        p.join()
+    frames = sum(r[0] for r in res)
+    t0 = min(r[1] for r in res)
+    t1 = max(r[2] for r in res)
+    return frames / (t1 - t0), frames, t1 - t0
+
+
+def _cpu_sample_worker(args):
+    seg, q = args
+    from oracle import tcref
+    from tcodec_b200 import api
+    lib = tcref.ref_lib()
+    frames = make_clip(seg + 2)[seg:seg + 2]
+    enc = api.Encoder(lib, make_cfg(lib))
+    t0 = time.perf_counter()
+    n = sum(1 for f in frames if enc.encode(*f) is not None) + len(enc.flush())
+    q.put((n, time.perf_counter() - t0))
+    enc.close()
+
+
+def cpu_baseline(procs):
+    """Bounded sample: `procs` processes each encode 2 frames of the workload
+    (keyframe + tail-flushed P frame) with the reference encoder."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    t0 = time.perf_counter()
+    ps = [ctx.Process(target=_cpu_sample_worker, args=((k, q),)) for k in range(procs)]
+    for p in ps:
+        p.start()
+    res = [q.get() for _ in ps]
+    for p in ps:
+        p.join()
+    wall = time.perf_counter() - t0
+    frames = sum(r[0] for r in res)
+    per_proc = max(r[1] for r in res)
+    return {"value": frames / per_proc, "unit": UNIT, "cores": procs, "kind": "reference",
+            "sample": f"{procs} processes x 2 frames (keyframe + P) of the 1920x1080 workload, reference "
+                      f"C encoder (oracle/_ref, -O3 scalar); {per_proc:.1f} s encode, {wall:.1f} s wall"}
+
+
+# ---------------------------------------------------------------- B200 arm
+def run_b200(args, rank, world):
+    """Batched pass (device-resident and host inputs) and a plain
+    single-stream pass.  Stream s of the batch encodes clip frames s, s+1, ..."""
+    import torch
+    from tcodec_b200 import api
+    lib = api.bind_b200(api.load_library())
+    dev = torch.device("cuda", torch.cuda.current_device())
+    K, Wm, S = args.steps, args.warmup, args.streams
+    clip = make_clip(S + Wm + K)
+    dplanes = [tuple(torch.from_numpy(np.ascontiguousarray(p)).to(dev) for p in f) for f in clip]
+    torch.cuda.synchronize()
+
+    def timed(stream_ptr, fn_step, after_warmup=None):
+        stream = torch.cuda.ExternalStream(stream_ptr)
+        for t in range(Wm):
+            fn_step(t)
+        if after_warmup:
+            after_warmup()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        frames, nbytes, lat = 0, 0, []
+        for t in range(Wm, Wm + K):
+            t0 = time.perf_counter()
+            n, b = fn_step(t)
+            lat.append(time.perf_counter() - t0)
+            frames += n
+            nbytes += b
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        return ev0.elapsed_time(ev1), frames, nbytes, lat
+
+    def batch_pass(on_device):
+        batch = api.BatchEncoder(lib, [make_cfg(lib) for _ in range(S)])
+        lib.tcb_batch_set_timing(batch.h, 1)
+        pinned = None
+        if not on_device:
+            pinned = [tuple(torch.from_numpy(np.ascontiguousarray(p)).pin_memory().numpy() for p in f) for f in clip]
+        first = []
+
+        def step(t):
+            if on_device:
+                planes = [tuple((dplanes[s + t][k].data_ptr(), dplanes[s + t][k].shape[1]) for k in range(3))
+                          for s in range(S)]
+            else:
+                planes = [pinned[s + t] for s in range(S)]
+            pk = batch.encode(planes, on_device=on_device)
+            if pk[0] is not None:
+                first.append(pk[0])
+            got = [p for p in pk if p is not None]
+            return len(got), sum(len(p) for p in got)
+
+        st = (ctypes.c_double(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64())
+        reset = lambda: lib.tcb_batch_get_timing(batch.h, *[ctypes.byref(x) for x in st])
+        res = timed(lib.tcb_batch_stream(batch.h), step, reset)
+        reset()
+        tail = batch.flush()
+        batch.close()
+        ms, frames, nbytes, lat = res
+        return dict(ms=ms, frames=frames, bytes=nbytes, lat=lat, packets=first + tail[0], ctu_ms=st[0].value,
+                    ctu_launches=st[1].value, ctu_count=st[2].value, steps=st[3].value, launches=st[4].value)
+
+    def plain_pass():
+        enc = api.Encoder(lib, make_cfg(lib))
+
+        def step(t):
+            y, cb, cr = dplanes[t]
+            pkt = api.Packet()
+            r = lib.tcb_encoder_encode_device(enc.h, y.data_ptr(), W, cb.data_ptr(), W // 2, cr.data_ptr(), W // 2,
+                                              ctypes.byref(pkt))
+            if r == api.TC_ERR_NEED_MORE:
+                return 0, 0
+            if r != api.TC_OK:
+                raise RuntimeError(f"encode -> {r}")
+            return 1, pkt.size
+
+        ms, frames, nbytes, lat = timed(lib.tcb_encoder_stream(enc.h), step)
+        enc.close()
+        return dict(ms=ms, frames=frames)
+
+    clocks = ClockSampler(torch.cuda.current_device())
+    with clocks:
+        dev_run = batch_pass(True)
+    e2e_run = batch_pass(False)
+    plain = plain_pass() if not args.no_plain else None
+    return dev_run, e2e_run, plain, clocks.summary()
+
+
+def max_over_ranks(x, world):
+    if world <= 1:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world):
+    if world <= 1:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
+    return float(t.item())
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=16)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--streams", type=int, default=16, help="1080p streams per GPU in the batched form")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    config = {"workload": "1920x1080 4:2:0, GOP4 hierarchical B, CQP QP32, preset medium, profile 1 (2 searched "
+                          "refs), deblock+SAO, synthetic cfg2 source (sinusoids + 16 moving noise rectangles + "
+                          "1-px lines over 5% area)",
+              "streams_per_gpu": args.streams, "frames_per_step": f"one per stream ({args.streams})",
+              "l2": "fresh input frames every step from a device-resident clip (no reuse across steps)",
+              "parallelism": f"replicas x{args.gpus}: every GPU encodes its own {args.streams} streams"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from oracle import tcref
+        if not tcref.available():
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference build) is missing"}))
+            return
+        procs = max(1, os.cpu_count() or 1)
+        fps, frames, secs = run_reference(args.steps, args.warmup, procs)
+        line = {"metric": METRIC, "value": fps, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1000 * secs / max(1, args.steps), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic",
+                "config": config, "impl": "reference",
+                "cpu_baseline": {"value": fps, "unit": UNIT, "cores": procs, "kind": "reference",
+                                 "sample": f"{procs} reference encoder processes, one input frame each per step, "
+                                           f"{frames} frames in {secs:.1f} s"},
+                "e2e": {"value": fps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    if world > 1:
+        torch.cuda.set_device(local)
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev_run, e2e_run, plain, clocks = run_b200(args, rank, world)
+    ms = max_over_ranks(dev_run["ms"], world)
+    frames = sum_over_ranks(dev_run["frames"], world)
+    ms_e2e = max_over_ranks(e2e_run["ms"], world)
+    frames_e2e = sum_over_ranks(e2e_run["frames"], world)
+    if world > 1:
+        torch.distributed.barrier()
+    if rank != 0:
+        torch.distributed.destroy_process_group()
+        return
+
+    value = frames / (ms / 1000.0)
+    e2e = frames_e2e / (ms_e2e / 1000.0)
+    # Bit-exactness of this run's stream against the reference's committed
+    # answers for the same workload (first packets in coding order).
+    bit_exact = None
+    if os.path.exists(GOLDEN):
+        want = json.load(open(GOLDEN))["packets"]
+        got = [hashlib.sha256(p).hexdigest() for p in dev_run["packets"][:len(want)]]
+        bit_exact = got == want[:len(got)] and len(got) == len(want)
+        same_e2e = [hashlib.sha256(p).hexdigest() for p in e2e_run["packets"][:len(want)]] == got
+        bit_exact = bool(bit_exact and same_e2e)
+    # Roofline of the dominant kernel (the CTU engine).  Algorithmic bytes
+    # per frame: the stages it fuses at their standalone minimum traffic,
+    # MC 3WH + deblock 3WH + SAO 4WH = 10*W*H bytes.
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        peak, peak_src = 6650.0, "fallback"
+    steps = max(1, dev_run["steps"])
+    launches = max(1, dev_run["ctu_launches"])
+    per_launch_s = dev_run["ctu_ms"] / 1000.0 / launches
+    # frames the timed launches encoded (all CTUs of every stream per step)
+    nctu_frame = ((W + 63) // 64) * ((H + 63) // 64)
+    frames_in_launches = dev_run["ctu_count"] / nctu_frame
+    alg_bytes_per_launch = 10.0 * W * H * frames_in_launches / launches
+    achieved = alg_bytes_per_launch / per_launch_s / 1e9
+    traffic = None
+    if os.path.exists(TRAFFIC):
+        t = json.load(open(TRAFFIC))
+        traffic = t.get("dram_bytes_per_launch")
+    lat = sorted(dev_run["lat"])
+    p50 = lat[len(lat) // 2] * 1000 if lat else None
+    p99 = lat[min(len(lat) - 1, int(0.99 * len(lat)))] * 1000 if lat else None
+    nctu = ((W + 63) // 64) * ((H + 63) // 64)
+    S = args.streams
+    import_rec = 1.5 * W * H * S
+    rec_bytes = (13504 * nctu + 1.5 * W * H) * S
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic", "config": config,
+        "bit_exact": bit_exact, "frames_timed": int(frames),
+        "latency_ms": {"p50": p50, "p99": p99, "what": "per-step batch call latency (one frame of every stream), "
+                       "device-resident input"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "kernel": "ctu_kernel (CTU RDO engine)",
+                     "peak_source": peak_src,
+                     "note": "algorithmic bytes 10*W*H per frame (MC 3WH + deblock 3WH + SAO 4WH) spread over "
+                             "the frame's wavefront launches; the engine is latency / integer-pipe bound"},
+        "ctu_engine": {"ms_per_step": dev_run["ctu_ms"] / steps, "launches_per_step": launches / steps,
+                       "ctus_per_launch": dev_run["ctu_count"] / launches},
+        "batch": {"streams_per_gpu": args.streams, "form": "batched: every stream's CTUs on anti-diagonal d share "
+                  "one launch (tcb_batch_encode)"},
+        "plain_gpu": (None if plain is None else {"value": plain["frames"] / (plain["ms"] / 1000.0), "unit": UNIT,
+                      "what": "one stream alone through the same kernels (tcb_encoder_encode_device)"}),
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(import_rec),
+                "d2h_bytes_per_step": int(rec_bytes + e2e_run["bytes"] / max(1, args.steps))},
+        "gpu_launches": int(dev_run["launches"]),
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        try:
+            from oracle import tcref
+            if tcref.available():
+                line["cpu_baseline"] = cpu_baseline(min(8, os.cpu_count() or 1))
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                                    "sample": f"failed: {e}"}
+    print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

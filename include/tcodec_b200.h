@@ -1,0 +1,86 @@
+/*
+ * tcodec_b200.h — B200-specific C ABI next to include/tcodec.h.
+ *
+ * Part 1: encoder extensions that have no counterpart in the reference
+ *         (device-resident input, stream handle, kernel timing).
+ * Part 2: batched standalone kernels of the v2 pixel pipeline.  Each one
+ *         replaces a reference routine (cited per entry point) with an
+ *         sm_100a kernel that processes many independent items per launch.
+ *         All pointers are DEVICE pointers, all launches go on `stream`
+ *         (a cudaStream_t, NULL = legacy default stream) and are
+ *         asynchronous; the return value reports launch errors only
+ *         (0 = OK, TC_ERR_PARAM for invalid sizes, TC_ERR_INTERNAL for a
+ *         CUDA error).
+ */
+#ifndef TCODEC_B200_H
+#define TCODEC_B200_H
+
+#include "tcodec.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------
+ * Part 1: encoder extensions (no reference counterpart).
+ * ------------------------------------------------------------------- */
+
+/* Same as tc_encoder_encode (reference tcodec.h:39-43) but the planes are
+ * device pointers already resident in HBM; no host->device copy happens. */
+tc_error_t tcb_encoder_encode_device(tc_encoder_t *enc,
+                                     const tc_pixel_t *d_y, int stride_y,
+                                     const tc_pixel_t *d_cb, int stride_cb,
+                                     const tc_pixel_t *d_cr, int stride_cr,
+                                     tc_packet_t *packet_out);
+
+/* The CUDA stream (cudaStream_t) the encoder launches all its work on. */
+void *tcb_encoder_stream(tc_encoder_t *enc);
+
+/* Kernel timing: when enabled, CUDA events bracket every frame's
+ * CTU-engine launches; totals accumulate until read (reading resets
+ * them).  kernel_launches counts every kernel this encoder launched. */
+void tcb_encoder_set_timing(tc_encoder_t *enc, int enabled);
+void tcb_encoder_get_timing(tc_encoder_t *enc, double *ctu_ms, int64_t *ctu_launches,
+                            int64_t *ctu_count, int64_t *frames, int64_t *kernel_launches);
+
+/* Skip the per-frame device->host copy of the reconstruction into
+ * encoder->recon (default on, as the reference keeps it current). */
+void tcb_encoder_set_recon_readback(tc_encoder_t *enc, int enabled);
+
+/* ---------------------------------------------------------------------
+ * Batched form (no reference counterpart): N independent v2 streams that
+ * advance one frame per call and share every CTU-engine launch.  Each
+ * stream is an ordinary tc_encoder_t (tcb_batch_encoder) with its own
+ * configuration, DPB and bitstream; packets are bit-identical to encoding
+ * that stream alone.
+ * ------------------------------------------------------------------- */
+typedef struct tcb_batch tcb_batch_t;
+
+/* One encoder per configs[i]; NULL on invalid config or device failure. */
+tcb_batch_t *tcb_batch_create(const tc_config_t *configs, int n);
+void tcb_batch_destroy(tcb_batch_t *batch);
+int tcb_batch_size(tcb_batch_t *batch);
+tc_encoder_t *tcb_batch_encoder(tcb_batch_t *batch, int i);
+void *tcb_batch_stream(tcb_batch_t *batch);
+
+/* Feed one frame to every stream i with y[i] != NULL (host pointers, or
+ * device pointers when on_device != 0).  status[i] is TC_OK with
+ * packets[i] filled, TC_ERR_NEED_MORE (no input or B-frame buffering), or
+ * an error.  Packet data stays valid until the stream's next packet. */
+tc_error_t tcb_batch_encode(tcb_batch_t *batch, const tc_pixel_t *const *y, const int *stride_y,
+                            const tc_pixel_t *const *cb, const int *stride_cb,
+                            const tc_pixel_t *const *cr, const int *stride_cr, int on_device,
+                            tc_packet_t *packets, int *status);
+/* Drain B-frame tails: TC_OK while any stream emitted (status per stream,
+ * TC_ERR_EOF for drained ones), TC_ERR_EOF once all are drained. */
+tc_error_t tcb_batch_flush(tcb_batch_t *batch, tc_packet_t *packets, int *status);
+
+void tcb_batch_set_timing(tcb_batch_t *batch, int enabled);
+void tcb_batch_get_timing(tcb_batch_t *batch, double *ctu_ms, int64_t *ctu_launches, int64_t *ctu_count,
+                          int64_t *steps, int64_t *kernel_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TCODEC_B200_H */

@@ -80,6 +80,22 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.tc_encoder_get_stats.restype = None
     lib.tc_error_string.argtypes = [ctypes.c_int]
     lib.tc_error_string.restype = ctypes.c_char_p
+    pp = P(P(ctypes.c_uint8))
+    ip = P(ctypes.c_int)
+    lib.tc_decoder_create.argtypes = [ctypes.c_int32, ctypes.c_int32]
+    lib.tc_decoder_create.restype = ctypes.c_void_p
+    lib.tc_decoder_destroy.argtypes = [ctypes.c_void_p]
+    lib.tc_decoder_destroy.restype = None
+    lib.tc_decoder_decode.argtypes = [ctypes.c_void_p, u8p, ctypes.c_size_t, pp, ip, pp, ip, pp, ip]
+    lib.tc_decoder_decode.restype = ctypes.c_int
+    lib.tc_decoder_flush_tail.argtypes = [ctypes.c_void_p, pp, ip, pp, ip, pp, ip]
+    lib.tc_decoder_flush_tail.restype = ctypes.c_int
+    lib.tc_decoder_crc_valid.argtypes = [ctypes.c_void_p]
+    lib.tc_decoder_crc_valid.restype = ctypes.c_int
+    lib.tc_decoder_entropy_coded.argtypes = [ctypes.c_void_p]
+    lib.tc_decoder_entropy_coded.restype = ctypes.c_int
+    lib.tc_decoder_get_info.argtypes = [ctypes.c_void_p, P(ctypes.c_int32), P(ctypes.c_int32)]
+    lib.tc_decoder_get_info.restype = None
     return lib
 
 
@@ -188,6 +204,180 @@ class Encoder:
 
         return (plane(fb.y, fb.stride_y, w, h), plane(fb.cb, fb.stride_c, w // 2, h // 2),
                 plane(fb.cr, fb.stride_c, w // 2, h // 2))
+
+
+class Decoder:
+    """One decode session through the C ABI (tc_decoder_*)."""
+
+    def __init__(self, lib: ctypes.CDLL, width: int = 0, height: int = 0):
+        self.lib = lib
+        self.h = lib.tc_decoder_create(width, height)
+        if not self.h:
+            raise RuntimeError("tc_decoder_create failed")
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.tc_decoder_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _planes(self, y, ys, cb, cbs, cr, crs):
+        w, h = ctypes.c_int32(), ctypes.c_int32()
+        self.lib.tc_decoder_get_info(self.h, ctypes.byref(w), ctypes.byref(h))
+        W, H = w.value, h.value
+
+        def plane(p, stride, pw, ph):
+            buf = ctypes.string_at(p, stride * ph)
+            return np.frombuffer(buf, dtype=np.uint8).reshape(ph, stride)[:, :pw].copy()
+
+        return (plane(y, ys.value, W, H), plane(cb, cbs.value, W // 2, H // 2),
+                plane(cr, crs.value, W // 2, H // 2))
+
+    def decode(self, packet: bytes):
+        """Returns (y, cb, cr), None while a B-frame reorder waits, or
+        raises on an error code (the code is in the exception args)."""
+        P = ctypes.POINTER(ctypes.c_uint8)
+        y, cb, cr = P(), P(), P()
+        ys, cbs, crs = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        buf = (ctypes.c_uint8 * max(1, len(packet))).from_buffer_copy(packet or b"\0")
+        r = self.lib.tc_decoder_decode(self.h, buf, len(packet), ctypes.byref(y), ctypes.byref(ys),
+                                       ctypes.byref(cb), ctypes.byref(cbs), ctypes.byref(cr), ctypes.byref(crs))
+        if r == TC_ERR_NEED_MORE:
+            return None
+        if r != TC_OK:
+            raise RuntimeError("tc_decoder_decode", r)
+        return self._planes(y, ys, cb, cbs, cr, crs)
+
+    def flush(self):
+        out = []
+        P = ctypes.POINTER(ctypes.c_uint8)
+        while True:
+            y, cb, cr = P(), P(), P()
+            ys, cbs, crs = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+            r = self.lib.tc_decoder_flush_tail(self.h, ctypes.byref(y), ctypes.byref(ys), ctypes.byref(cb),
+                                               ctypes.byref(cbs), ctypes.byref(cr), ctypes.byref(crs))
+            if r != TC_OK:
+                return out
+            out.append(self._planes(y, ys, cb, cbs, cr, crs))
+
+    def crc_valid(self) -> int:
+        return self.lib.tc_decoder_crc_valid(self.h)
+
+
+def bind_b200(lib: ctypes.CDLL) -> ctypes.CDLL:
+    """Attach argtypes of the include/tcodec_b200.h encoder extensions."""
+    vp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)
+    lib.tcb_encoder_encode_device.argtypes = [vp] + [vp, ctypes.c_int] * 3 + [ctypes.POINTER(Packet)]
+    lib.tcb_encoder_encode_device.restype = ctypes.c_int
+    lib.tcb_encoder_stream.argtypes = [vp]
+    lib.tcb_encoder_stream.restype = vp
+    lib.tcb_encoder_set_timing.argtypes = [vp, ctypes.c_int]
+    lib.tcb_encoder_get_timing.argtypes = [vp] + [vp] * 5
+    lib.tcb_encoder_set_recon_readback.argtypes = [vp, ctypes.c_int]
+    lib.tcb_batch_create.argtypes = [ctypes.POINTER(Config), ctypes.c_int]
+    lib.tcb_batch_create.restype = vp
+    lib.tcb_batch_destroy.argtypes = [vp]
+    lib.tcb_batch_encoder.argtypes = [vp, ctypes.c_int]
+    lib.tcb_batch_encoder.restype = vp
+    lib.tcb_batch_stream.argtypes = [vp]
+    lib.tcb_batch_stream.restype = vp
+    lib.tcb_batch_encode.argtypes = [vp, ctypes.POINTER(vp), ip, ctypes.POINTER(vp), ip, ctypes.POINTER(vp), ip,
+                                     ctypes.c_int, ctypes.POINTER(Packet), ip]
+    lib.tcb_batch_encode.restype = ctypes.c_int
+    lib.tcb_batch_flush.argtypes = [vp, ctypes.POINTER(Packet), ip]
+    lib.tcb_batch_flush.restype = ctypes.c_int
+    lib.tcb_batch_set_timing.argtypes = [vp, ctypes.c_int]
+    lib.tcb_batch_get_timing.argtypes = [vp] + [vp] * 5
+    return lib
+
+
+class BatchEncoder:
+    """N independent v2 streams sharing every CTU-engine launch
+    (tcb_batch_*).  `encode(frames)` takes one (y, cb, cr) per stream —
+    numpy arrays (host) or (ptr, stride) device-pointer triples — or None
+    to skip a stream; returns a list of packets (None while buffering)."""
+
+    def __init__(self, lib: ctypes.CDLL, cfgs: List[Config]):
+        self.lib = bind_b200(lib)
+        self.n = len(cfgs)
+        arr = (Config * self.n)(*cfgs)
+        self.h = lib.tcb_batch_create(arr, self.n)
+        if not self.h:
+            raise RuntimeError("tcb_batch_create failed")
+        self.cfgs = cfgs
+
+    def close(self):
+        if self.h:
+            self.lib.tcb_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _call(self, planes, on_device):
+        n = self.n
+        VP = ctypes.c_void_p * n
+        I = ctypes.c_int * n
+        y, cb, cr, sy, scb, scr = VP(), VP(), VP(), I(), I(), I()
+        keep = []
+        for i, f in enumerate(planes):
+            if f is None:
+                continue
+            if on_device:
+                (y[i], sy[i]), (cb[i], scb[i]), (cr[i], scr[i]) = f
+            else:
+                a = [np.ascontiguousarray(p, dtype=np.uint8) for p in f]
+                keep.append(a)
+                y[i], cb[i], cr[i] = (p.ctypes.data for p in a)
+                sy[i], scb[i], scr[i] = (p.shape[1] for p in a)
+        pk = (Packet * n)()
+        st = I()
+        r = self.lib.tcb_batch_encode(self.h, y, sy, cb, scb, cr, scr, 1 if on_device else 0, pk, st)
+        return r, pk, st
+
+    def encode(self, planes, on_device: bool = False):
+        r, pk, st = self._call(planes, on_device)
+        if r not in (TC_OK, TC_ERR_NEED_MORE):
+            raise RuntimeError(f"tcb_batch_encode -> {r}", list(st))
+        return [ctypes.string_at(pk[i].data, pk[i].size) if st[i] == TC_OK else None for i in range(self.n)]
+
+    def flush(self):
+        """All remaining packets, per stream."""
+        out = [[] for _ in range(self.n)]
+        while True:
+            pk = (Packet * self.n)()
+            st = (ctypes.c_int * self.n)()
+            r = self.lib.tcb_batch_flush(self.h, pk, st)
+            if r == TC_ERR_EOF:
+                return out
+            if r != TC_OK:
+                raise RuntimeError(f"tcb_batch_flush -> {r}")
+            for i in range(self.n):
+                if st[i] == TC_OK:
+                    out[i].append(ctypes.string_at(pk[i].data, pk[i].size))
+
+
+def decode_sequence(lib: ctypes.CDLL, packets, width: int = 0, height: int = 0):
+    """Decode packets (coding order) into display-order frames."""
+    dec = Decoder(lib, width, height)
+    out = []
+    try:
+        for p in packets:
+            f = dec.decode(p)
+            if f is not None:
+                out.append(f)
+        out.extend(dec.flush())
+    finally:
+        dec.close()
+    return out
 
 
 def encode_sequence(lib: ctypes.CDLL, cfg: Config, frames, with_recon: bool = False):

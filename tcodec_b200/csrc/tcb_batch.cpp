@@ -1,0 +1,247 @@
+// tcb_batch.cpp — batched form of the v2 encoder: N independent streams
+// (any mix of resolutions, QPs, presets) advance one frame per call and
+// share every CTU-engine launch.  Step d of the call launches, in ONE
+// kernel, the CTUs on anti-diagonal d of every participating stream, so a
+// 1080p stream's ~11 CTUs per diagonal are joined by everyone else's and
+// the 148 SMs fill up.  Per-stream host work (frame type, header, entropy
+// coding) runs on host threads in parallel; all device work is ordered on
+// the batch's CUDA stream.
+#include <string.h>
+
+#include <algorithm>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/tcodec_b200.h"
+#include "tcb_encoder.h"
+#include "tcb_launch.h"
+
+using namespace tcb;
+
+struct tcb_batch {
+    std::vector<tc_encoder_t *> encs;
+    cudaStream_t st = nullptr;
+    FrameParams *d_params = nullptr;         // [n] contiguous for the kernel
+    int *d_items = nullptr;
+    int *d_ctrl = nullptr;
+    int num_sms = 148;
+    size_t items_cap = 0;
+    std::vector<int> h_items;
+    std::vector<std::vector<std::vector<int>>> stream_diag;   // [s][d] item words
+    int max_diag = 0;
+    bool timing = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double ctu_ms = 0.0;
+    long long ctu_launches = 0, ctu_count = 0, steps = 0, kernel_launches = 0;
+    int device = 0;
+};
+
+namespace {
+
+void release(tcb_batch *b) {
+    if (b->st) cudaStreamSynchronize(b->st);
+    for (tc_encoder_t *e : b->encs) {
+        if (e && e->impl) e->impl->st = e->impl->own_st;
+        tc_encoder_destroy(e);
+    }
+    cudaFree(b->d_params);
+    cudaFree(b->d_items);
+    cudaFree(b->d_ctrl);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+}
+
+// Run stage_a..stage_d for the streams whose plan produced a frame.
+tc_error_t run_step(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkts, int *status) {
+    const int n = (int)b->encs.size();
+    for (int s : part) {
+        EncImpl &e = *b->encs[s]->impl;
+        const tc_error_t r = e.stage_a(e.pend.poc, e.pend.qp_off);
+        if (r != TC_OK) return r;
+    }
+    bool need_sync = false;
+    for (int s : part) need_sync |= b->encs[s]->impl->pend.need_hist != 0;
+    if (need_sync && cudaStreamSynchronize(b->st) != cudaSuccess) return TC_ERR_INTERNAL;
+    for (int s : part) {
+        EncImpl &e = *b->encs[s]->impl;
+        const tc_error_t r = e.stage_b();
+        if (r != TC_OK) return r;
+        b->kernel_launches += 0;
+        if (cudaMemcpyAsync(b->d_params + s, e.d_params, sizeof(FrameParams), cudaMemcpyDeviceToDevice, b->st) !=
+            cudaSuccess)
+            return TC_ERR_INTERNAL;
+    }
+    // Merged anti-diagonal item lists of the participating streams.
+    std::vector<int> off(b->max_diag), cnt(b->max_diag);
+    b->h_items.clear();
+    for (int d = 0; d < b->max_diag; ++d) {
+        off[d] = (int)b->h_items.size();
+        for (int s : part) {
+            const auto &sd = b->stream_diag[s];
+            if (d < (int)sd.size()) b->h_items.insert(b->h_items.end(), sd[d].begin(), sd[d].end());
+        }
+        cnt[d] = (int)b->h_items.size() - off[d];
+    }
+    if (b->h_items.size() > b->items_cap) {
+        cudaFree(b->d_items);
+        b->items_cap = b->h_items.size();
+        if (cudaMalloc(&b->d_items, sizeof(int) * b->items_cap) != cudaSuccess) return TC_ERR_MEMORY;
+    }
+    if (cudaMemcpyAsync(b->d_items, b->h_items.data(), sizeof(int) * b->h_items.size(), cudaMemcpyHostToDevice,
+                        b->st) != cudaSuccess)
+        return TC_ERR_INTERNAL;
+    // One persistent launch drains the merged queue (per-stream publish
+    // flags keep every stream's wavefront order).
+    if (b->timing) cudaEventRecord(b->ev0, b->st);
+    const bool persistent = b->encs[part[0]]->impl->persistent;
+    if (persistent) {
+        if (cudaMemsetAsync(b->d_ctrl, 0, 2 * sizeof(int), b->st) != cudaSuccess ||
+            launch_ctu_persistent(b->d_params, b->d_items, (int)b->h_items.size(), b->d_ctrl, b->num_sms, b->st) !=
+                cudaSuccess)
+            return TC_ERR_INTERNAL;
+        b->kernel_launches += 1;
+    } else {
+        for (int d = 0; d < b->max_diag; ++d)
+            if (cnt[d] && launch_ctu_items(b->d_params, b->d_items + off[d], cnt[d], b->st) != cudaSuccess)
+                return TC_ERR_INTERNAL;
+        for (int d = 0; d < b->max_diag; ++d) b->kernel_launches += cnt[d] ? 1 : 0;
+    }
+    if (b->timing) cudaEventRecord(b->ev1, b->st);
+    for (int s : part) {
+        const tc_error_t r = b->encs[s]->impl->stage_c();
+        if (r != TC_OK) return r;
+        // the queue's error word is the batch's
+        if (persistent && cudaMemcpyAsync(b->encs[s]->impl->h_ctrl, b->d_ctrl, 2 * sizeof(int),
+                                          cudaMemcpyDeviceToHost, b->st) != cudaSuccess)
+            return TC_ERR_INTERNAL;
+    }
+    if (cudaStreamSynchronize(b->st) != cudaSuccess) return TC_ERR_INTERNAL;
+    if (b->timing) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+        b->ctu_ms += ms;
+        b->ctu_launches += b->max_diag;
+        b->steps++;
+        b->ctu_count += (long long)b->h_items.size();
+    }
+    // Entropy coding in parallel, one host thread per stream.
+    std::vector<std::thread> th;
+    std::vector<tc_error_t> rs(n, TC_OK);
+    for (int s : part)
+        th.emplace_back([&, s]() { rs[s] = b->encs[s]->impl->stage_d(&pkts[s]); });
+    for (auto &t : th) t.join();
+    tc_error_t worst = TC_OK;
+    for (int s : part) {
+        status[s] = rs[s];
+        b->kernel_launches += b->encs[s]->impl->kernel_launches;
+        b->encs[s]->impl->kernel_launches = 0;
+        if (rs[s] != TC_OK) worst = rs[s];
+    }
+    return worst;
+}
+
+}  // namespace
+
+extern "C" {
+
+tcb_batch_t *tcb_batch_create(const tc_config_t *configs, int n) {
+    if (!configs || n <= 0 || n > MAX_STREAMS) return nullptr;
+    tcb_batch *b = new (std::nothrow) tcb_batch();
+    if (!b) return nullptr;
+    if (cudaGetDevice(&b->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+        cudaMalloc(&b->d_params, sizeof(FrameParams) * n) != cudaSuccess ||
+        cudaMalloc(&b->d_ctrl, 2 * sizeof(int)) != cudaSuccess ||
+        cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess) {
+        release(b);
+        return nullptr;
+    }
+    for (int s = 0; s < n; ++s) {
+        tc_encoder_t *e = tc_encoder_create(&configs[s]);
+        if (!e) { release(b); return nullptr; }
+        b->encs.push_back(e);
+        EncImpl &im = *e->impl;
+        im.st = b->st;                      // all device work on the batch stream
+        std::vector<std::vector<int>> diags(im.diag_off.size());
+        for (int d = 0; d < (int)im.diag_off.size(); ++d)
+            for (int r = 0; r < im.ctu_rows; ++r) {
+                const int c = d - r;
+                if (c >= 0 && c < im.ctu_cols) diags[d].push_back((s << 20) | (r << 10) | c);
+            }
+        b->max_diag = std::max(b->max_diag, (int)diags.size());
+        b->stream_diag.push_back(std::move(diags));
+    }
+    return b;
+}
+
+void tcb_batch_destroy(tcb_batch_t *b) {
+    if (b) release(b);
+}
+
+int tcb_batch_size(tcb_batch_t *b) { return b ? (int)b->encs.size() : 0; }
+
+tc_encoder_t *tcb_batch_encoder(tcb_batch_t *b, int i) {
+    return (b && i >= 0 && i < (int)b->encs.size()) ? b->encs[i] : nullptr;
+}
+
+void *tcb_batch_stream(tcb_batch_t *b) { return b ? (void *)b->st : nullptr; }
+
+tc_error_t tcb_batch_encode(tcb_batch_t *b, const tc_pixel_t *const *y, const int *stride_y,
+                            const tc_pixel_t *const *cb, const int *stride_cb, const tc_pixel_t *const *cr,
+                            const int *stride_cr, int on_device, tc_packet_t *packets, int *status) {
+    if (!b || !y || !cb || !cr || !stride_y || !stride_cb || !stride_cr || !packets || !status) return TC_ERR_PARAM;
+    if (cudaSetDevice(b->device) != cudaSuccess) return TC_ERR_INTERNAL;
+    const int n = (int)b->encs.size();
+    std::vector<int> part;
+    for (int s = 0; s < n; ++s) {
+        status[s] = TC_ERR_NEED_MORE;
+        memset(&packets[s], 0, sizeof(tc_packet_t));
+        if (!y[s] || !cb[s] || !cr[s]) continue;
+        EncImpl &e = *b->encs[s]->impl;
+        if (!e.upload(y[s], stride_y[s], cb[s], stride_cb[s], cr[s], stride_cr[s], e.cur,
+                      on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice))
+            return TC_ERR_INTERNAL;
+        const tc_error_t r = e.plan_input();
+        if (r == TC_OK) part.push_back(s);
+        else if (r != TC_ERR_NEED_MORE) { status[s] = r; return r; }
+    }
+    if (part.empty()) return TC_OK;
+    return run_step(b, part, packets, status);
+}
+
+tc_error_t tcb_batch_flush(tcb_batch_t *b, tc_packet_t *packets, int *status) {
+    if (!b || !packets || !status) return TC_ERR_PARAM;
+    if (cudaSetDevice(b->device) != cudaSuccess) return TC_ERR_INTERNAL;
+    const int n = (int)b->encs.size();
+    std::vector<int> part;
+    for (int s = 0; s < n; ++s) {
+        status[s] = TC_ERR_EOF;
+        memset(&packets[s], 0, sizeof(tc_packet_t));
+        const tc_error_t r = b->encs[s]->impl->plan_flush();
+        if (r == TC_OK) part.push_back(s);
+        else if (r != TC_ERR_EOF) { status[s] = r; return r; }
+    }
+    if (part.empty()) return TC_ERR_EOF;
+    return run_step(b, part, packets, status);
+}
+
+void tcb_batch_set_timing(tcb_batch_t *b, int enabled) {
+    if (b) b->timing = enabled != 0;
+}
+
+void tcb_batch_get_timing(tcb_batch_t *b, double *ctu_ms, int64_t *ctu_launches, int64_t *ctu_count,
+                          int64_t *steps, int64_t *kernel_launches) {
+    if (!b) return;
+    if (ctu_ms) *ctu_ms = b->ctu_ms;
+    if (ctu_launches) *ctu_launches = b->ctu_launches;
+    if (ctu_count) *ctu_count = b->ctu_count;
+    if (steps) *steps = b->steps;
+    if (kernel_launches) *kernel_launches = b->kernel_launches;
+    b->ctu_ms = 0.0; b->ctu_launches = 0; b->ctu_count = 0; b->steps = 0; b->kernel_launches = 0;
+}
+
+}  // extern "C"

@@ -45,6 +45,7 @@ struct CtuOut {
     Node     nodes[QT_NODES];
     int32_t  ncoef;
     int16_t  sao_has, sao_band, sao_offset, pad;
+    uint64_t tu8mask;                 // bit gy*8+gx: that 8x8 luma region uses one 8x8 TU
     int16_t  coef[CTU_COEF_MAX];
 };
 
@@ -75,6 +76,8 @@ struct FrameParams {
     int eff_l[4], eff_c[4];                    // per-band quant steps
     uint32_t rcp_l[4], rcp_c[4];               // exact reciprocals of eff
     int32_t *err;                              // device error word
+    int *done;                                 // per-CTU publish flags (persistent wavefront)
+    int epoch;                                 // value this frame publishes in `done`
 };
 
 // ---------------------------------------------------------------------

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/tcodec.h"
+#include "../../include/tcodec_b200.h"
 #include "tcb_encoder.h"
 #include "tcb_entropy.h"
 #include "tcb_launch.h"
@@ -103,6 +104,9 @@ bool EncImpl::init(const tc_config_t &c) {
     CK(cudaGetDevice(&device));
     CK(init_device_tables());
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    own_st = st;
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
     const size_t ybytes = (size_t)sy * H + 64, cbytes = (size_t)sc * (H / 2) + 64;
     for (int i = 0; i < NPOOL; ++i) {
         CK(cudaMalloc(&pool[i].y, ybytes));
@@ -134,6 +138,15 @@ bool EncImpl::init(const tc_config_t &c) {
     CK(cudaMallocHost(&h_sse, sizeof(unsigned long long)));
     CK(cudaMalloc(&d_err, sizeof(int)));
     CK(cudaMemset(d_err, 0, sizeof(int)));
+    CK(cudaMalloc(&d_done, sizeof(int) * ctu_cols * ctu_rows));
+    CK(cudaMemset(d_done, 0, sizeof(int) * ctu_cols * ctu_rows));
+    CK(cudaMalloc(&d_ctrl, 2 * sizeof(int)));
+    CK(cudaMallocHost(&h_ctrl, 2 * sizeof(int)));
+    CK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+    {
+        const char *wf = getenv("TCB_WAVEFRONT");
+        persistent = !(wf && strcmp(wf, "diagonal") == 0);
+    }
     // Anti-diagonal wavefront item lists.
     std::vector<int> items;
     for (int d = 0; d < ctu_rows + ctu_cols - 1; ++d) {
@@ -157,15 +170,19 @@ bool EncImpl::init(const tc_config_t &c) {
 
 void EncImpl::release() {
     if (st) cudaStreamSynchronize(st);
+    if (own_st) cudaStreamSynchronize(own_st);
     for (int i = 0; i < NPOOL; ++i) { cudaFree(pool[i].y); cudaFree(pool[i].cb); cudaFree(pool[i].cr); }
     cudaFree(cur.y); cudaFree(cur.cb); cudaFree(cur.cr);
     cudaFree(grid[0]); cudaFree(grid[1]);
     cudaFree(d_out); cudaFreeHost(h_out);
     cudaFree(d_params); cudaFree(d_hist); cudaFreeHost(h_hist);
     cudaFree(d_sse); cudaFreeHost(h_sse); cudaFree(d_err); cudaFree(d_items);
+    cudaFree(d_done); cudaFree(d_ctrl); cudaFreeHost(h_ctrl);
     for (auto &f : bf_frames) { cudaFree(f.y); cudaFree(f.cb); cudaFree(f.cr); }
     bf_frames.clear();
-    if (st) cudaStreamDestroy(st);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (own_st) cudaStreamDestroy(own_st);
     free(out_buf);
 }
 
@@ -179,10 +196,10 @@ int EncImpl::free_pool_slot() const {
 }
 
 bool EncImpl::upload(const tc_pixel_t *y, int ys, const tc_pixel_t *cb, int cbs, const tc_pixel_t *cr,
-                     int crs, const DevFrame &dst) {
-    CK(cudaMemcpy2DAsync(dst.y, sy, y, ys, W, H, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpy2DAsync(dst.cb, sc, cb, cbs, W / 2, H / 2, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpy2DAsync(dst.cr, sc, cr, crs, W / 2, H / 2, cudaMemcpyHostToDevice, st));
+                     int crs, const DevFrame &dst, cudaMemcpyKind kind) {
+    CK(cudaMemcpy2DAsync(dst.y, sy, y, ys, W, H, kind, st));
+    CK(cudaMemcpy2DAsync(dst.cb, sc, cb, cbs, W / 2, H / 2, kind, st));
+    CK(cudaMemcpy2DAsync(dst.cr, sc, cr, crs, W / 2, H / 2, kind, st));
     return true;
 }
 
@@ -194,7 +211,35 @@ bool EncImpl::dcopy(const DevFrame &dst, const DevFrame &src) {
     return true;
 }
 
-tc_error_t EncImpl::encode_poc_frame(int poc, int b_layer_qp_off, tc_packet_t *pkt) {
+// ---------------------------------------------------------------------------
+// Frame driver, in stages so that many streams can share each CTU-engine
+// launch (batched form): plan (B-frame schedule) -> stage_a (scene-cut
+// histogram) -> stage_b (frame type, header, device parameters, global
+// motion hint) -> wavefront launches -> stage_c (copy-back) -> stage_d
+// (entropy coding, DPB update).  Single-stream encodes run the same stages
+// back to back (reference src/encoder.c:2625-3121 encode_poc_frame).
+// ---------------------------------------------------------------------------
+tc_error_t EncImpl::stage_a(int poc, int b_layer_qp_off) {
+    pend.poc = poc;
+    pend.qp_off = b_layer_qp_off;
+    pend.need_hist = 0;
+    if (!bf_b_mode) {
+        const int kint = cfg.keyframe_interval > 0 ? cfg.keyframe_interval : 30;
+        int is_key = force_keyframe || frame_count == 0;
+        if (!is_key && frame_count % kint == 0) is_key = 1;
+        if (!is_key && frame_count > 0) {
+            if (launch_hist16(cur.y, W, H, sy, d_hist, st) != cudaSuccess) return TC_ERR_INTERNAL;
+            ++kernel_launches;
+            if (cudaMemcpyAsync(h_hist, d_hist, 16 * sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+                return TC_ERR_INTERNAL;
+            pend.need_hist = 1;
+        }
+    }
+    return TC_OK;
+}
+
+tc_error_t EncImpl::stage_b() {
+    const int poc = pend.poc, b_layer_qp_off = pend.qp_off;
     // ---- frame type ----------------------------------------------------
     const int kint = cfg.keyframe_interval > 0 ? cfg.keyframe_interval : 30;
     int is_key;
@@ -203,11 +248,9 @@ tc_error_t EncImpl::encode_poc_frame(int poc, int b_layer_qp_off, tc_packet_t *p
     } else {
         is_key = force_keyframe || frame_count == 0;
         if (!is_key && frame_count % kint == 0) is_key = 1;
-        if (!is_key && frame_count > 0) {
-            if (launch_hist16(cur.y, W, H, sy, d_hist, st) != cudaSuccess) return TC_ERR_INTERNAL;
-            if (cudaMemcpyAsync(h_hist, d_hist, 16 * sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-                cudaStreamSynchronize(st) != cudaSuccess)
-                return TC_ERR_INTERNAL;
+        if (pend.need_hist) {
+            // Scene cut: chi-square distance of 16-bin input histograms
+            // (reference src/encoder.c:2650-2678).
             if (prev_hist_valid) {
                 double dist = 0.0;
                 const double total = (double)W * H;
@@ -230,10 +273,10 @@ tc_error_t EncImpl::encode_poc_frame(int poc, int b_layer_qp_off, tc_packet_t *p
     int qp = rc_qp;
     if (frame_type == 2) qp = clampi(qp + b_layer_qp_off, 0, 63);
 
-    // ---- header fields ---------------------------------------------------
+    // ---- header (reference src/encoder.c:2713-2819, 2365-2399) ---------
     memset(out_buf, 0, out_buf_size);
-    BitWriter bw;
-    bw.init(out_buf, out_buf_size);
+    fbw.init(out_buf, out_buf_size);
+    BitWriter &bw = fbw;
     int profile = cfg.profile, level = cfg.level_idx;
     if (profile > TC_PROFILE_MAX) profile = TC_PROFILE_BASELINE_MOBILE;
     if (level > TC_LEVEL_MAX) level = TC_LEVEL_AUTO;
@@ -242,8 +285,7 @@ tc_error_t EncImpl::encode_poc_frame(int poc, int b_layer_qp_off, tc_packet_t *p
     if (cfg.enable_crc) flags |= TC_FLAG_CRC;
     uint16_t tools = TC_TOOL_SKIP_MERGE | TC_TOOL_CFL_CHROMA | TC_TOOL_JND_WEIGHTING |
                      TC_TOOL_MEDIAN_MV_PRED | TC_TOOL_SIX_TAP_INTERP;
-    if ((cfg.preset == TC_PRESET_SLOW || cfg.preset >= TC_PRESET_MEDIUM) && profile >= TC_PROFILE_STREAMING_MAIN)
-        tools |= TC_TOOL_MULTI_REF;
+    if (cfg.preset >= TC_PRESET_MEDIUM && profile >= TC_PROFILE_STREAMING_MAIN) tools |= TC_TOOL_MULTI_REF;
     if (cfg.enable_entropy_coded) tools |= TC_TOOL_ENTROPY_CODED;
     if (frame_type == 2) tools |= TC_TOOL_BIPRED;
     tools |= TC_TOOL_SAO;
@@ -251,7 +293,6 @@ tc_error_t EncImpl::encode_poc_frame(int poc, int b_layer_qp_off, tc_packet_t *p
     const int use_ep = !prev_v2_valid || prev_v2_rowbytes >= 256;
     if (use_ep) tools |= TC_TOOL_ENTRY_POINTS;
     if (bf_b_mode) flags |= TC_FLAG_EXT_HEADER;
-    // write_frame_header (reference src/encoder.c:2365-2399)
     bw.put_bits(TC_MAGIC_0, 8); bw.put_bits(TC_MAGIC_1, 8); bw.put_bits(TC_MAGIC_2, 8);
     bw.put_bits(TC_VERSION_V2, 8);
     bw.put_bits((uint32_t)(uint16_t)W, 16); bw.put_bits((uint32_t)(uint16_t)H, 16);
@@ -263,9 +304,8 @@ tc_error_t EncImpl::encode_poc_frame(int poc, int b_layer_qp_off, tc_packet_t *p
     if (bf_b_mode) bw.put_bits(frame_type == 0 ? 0 : (frame_type == 2 ? 2 : 1), 8);
     bw.align();
 
-    if (is_key && poc > 0) {
+    if (is_key && poc > 0)
         for (int i = 0; i < TC_REF_FRAMES; ++i) { dpb_slot[i] = -1; dpb_poc[i] = -1; }
-    }
 
     // ---- device frame parameters ------------------------------------------
     const int rs = free_pool_slot();
@@ -306,32 +346,69 @@ tc_error_t EncImpl::encode_poc_frame(int poc, int b_layer_qp_off, tc_packet_t *p
         P.eff_c[b] = eff_scale(P.qp_c, b); P.rcp_c[b] = quant_rcp(P.eff_c[b]);
     }
     P.err = d_err;
+    P.done = d_done;
+    P.epoch = ++epoch;
     if (cudaMemcpyAsync(d_params, &P, sizeof(P), cudaMemcpyHostToDevice, st) != cudaSuccess)
         return TC_ERR_INTERNAL;
     if (frame_type == 1 && P.ref_valid[0]) {
         if (launch_glob_mv(cur.y, P.ref_y[0], W, H, sy, d_params, st) != cudaSuccess) return TC_ERR_INTERNAL;
+        ++kernel_launches;
     }
-    for (size_t d = 0; d < diag_off.size(); ++d)
-        if (launch_ctu_items(d_params, d_items + diag_off[d], diag_cnt[d], st) != cudaSuccess)
+    pend.is_key = is_key;
+    pend.frame_type = frame_type;
+    pend.qp = qp;
+    pend.use_ep = use_ep;
+    pend.rs = rs;
+    pend.multiref = P.multiref;
+    return TC_OK;
+}
+
+tc_error_t EncImpl::launch_own() {
+    if (timing) cudaEventRecord(ev0, st);
+    if (persistent) {
+        if (cudaMemsetAsync(d_ctrl, 0, 2 * sizeof(int), st) != cudaSuccess ||
+            launch_ctu_persistent(d_params, d_items, ctu_cols * ctu_rows, d_ctrl, num_sms, st) != cudaSuccess)
             return TC_ERR_INTERNAL;
+        kernel_launches += 1;
+    } else {
+        for (size_t d = 0; d < diag_off.size(); ++d)
+            if (launch_ctu_items(d_params, d_items + diag_off[d], diag_cnt[d], st) != cudaSuccess)
+                return TC_ERR_INTERNAL;
+        kernel_launches += (long long)diag_off.size();
+    }
+    if (timing) cudaEventRecord(ev1, st);
+    return TC_OK;
+}
+
+tc_error_t EncImpl::stage_c() {
+    const DevFrame rec = pool[pend.rs];
     const int nctu = ctu_cols * ctu_rows;
     if (cudaMemcpyAsync(h_out, d_out, sizeof(CtuOut) * nctu, cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return TC_ERR_INTERNAL;
     if (launch_frame_sse(cur.y, rec.y, W, H, sy, d_sse, st) != cudaSuccess) return TC_ERR_INTERNAL;
-    if (cudaMemcpyAsync(h_sse, d_sse, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    ++kernel_launches;
+    if (cudaMemcpyAsync(h_sse, d_sse, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(h_ctrl, d_ctrl, 2 * sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return TC_ERR_INTERNAL;
-    if (recon_host) {
+    if (recon_host && recon_readback) {
         if (cudaMemcpy2DAsync(recon_host->y, recon_host->stride_y, rec.y, sy, W, H, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaMemcpy2DAsync(recon_host->cb, recon_host->stride_c, rec.cb, sc, W / 2, H / 2, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaMemcpy2DAsync(recon_host->cr, recon_host->stride_c, rec.cr, sc, W / 2, H / 2, cudaMemcpyDeviceToHost, st) != cudaSuccess)
             return TC_ERR_INTERNAL;
     }
-    if (cudaStreamSynchronize(st) != cudaSuccess) return TC_ERR_INTERNAL;
+    return TC_OK;
+}
 
-    // ---- entropy coding of the CTU records ------------------------------
+// Entropy coding of the CTU records and sequence bookkeeping; the stream
+// must be synchronised (host copies complete).
+tc_error_t EncImpl::stage_d(tc_packet_t *pkt) {
+    if (persistent && h_ctrl[1]) return TC_ERR_INTERNAL;   // a bounded wait expired on the device
+    const int poc = pend.poc, is_key = pend.is_key, frame_type = pend.frame_type, qp = pend.qp;
+    const int use_ep = pend.use_ep, rs = pend.rs, multiref = pend.multiref;
+    BitWriter &bw = fbw;
     const int entropy = cfg.enable_entropy_coded ? 1 : 0;
-    const int multiref = P.multiref;
     if (use_ep) {
+        // Entry-point rows (reference src/encoder.c:2906-2965).
         const int nrows = ctu_rows;
         bw.put_bits((uint32_t)nrows, 16);
         const size_t ep_table = bw.byte_pos;
@@ -340,12 +417,11 @@ tc_error_t EncImpl::encode_poc_frame(int poc, int b_layer_qp_off, tc_packet_t *p
         const size_t ep_payload = bw.byte_pos;
         const size_t per_row = out_buf_size / (size_t)(nrows > 1 ? nrows : 1) + 1024;
         if (nrows > 64) return TC_ERR_MEMORY;
-        std::vector<uint8_t> rbuf(per_row);
+        if (row_buf.size() < per_row) row_buf.resize(per_row);
         uint32_t row_off[64];
         for (int r = 0; r < nrows; ++r) {
-            std::fill(rbuf.begin(), rbuf.end(), 0);
             BitWriter rw;
-            rw.init(rbuf.data(), per_row);
+            rw.init(row_buf.data(), per_row);
             RangeEncoder rc;
             uint8_t ctx[TC_NUM_CONTEXTS_RC];
             memset(ctx, 0, sizeof(ctx));
@@ -361,7 +437,7 @@ tc_error_t EncImpl::encode_poc_frame(int poc, int b_layer_qp_off, tc_packet_t *p
             const size_t rb = rw.bytes();
             if (rb > per_row || bw.byte_pos + rb > out_buf_size) return TC_ERR_MEMORY;
             row_off[r] = (uint32_t)(bw.byte_pos - ep_payload);
-            memcpy(out_buf + bw.byte_pos, rbuf.data(), rb);
+            memcpy(out_buf + bw.byte_pos, row_buf.data(), rb);
             bw.byte_pos += rb;
         }
         for (int i = 0; i < nrows; ++i) {
@@ -384,8 +460,7 @@ tc_error_t EncImpl::encode_poc_frame(int poc, int b_layer_qp_off, tc_packet_t *p
         bw.align();
     }
     if (cfg.enable_crc) {
-        const size_t n = bw.bytes();
-        const uint16_t crc = crc16_ccitt(out_buf, n);
+        const uint16_t crc = crc16_ccitt(out_buf, bw.bytes());
         bw.put_bits(crc >> 8, 8);
         bw.put_bits(crc & 0xFF, 8);
     }
@@ -394,7 +469,7 @@ tc_error_t EncImpl::encode_poc_frame(int poc, int b_layer_qp_off, tc_packet_t *p
     rc_frame_end((long long)frame_bytes * 8);
     if (ctu_rows > 0) { prev_v2_rowbytes = frame_bytes / (size_t)ctu_rows; prev_v2_valid = 1; }
 
-    // PSNR (reference src/tcodec.c:34-54) from the device SSE.
+    // PSNR statistic (reference src/tcodec.c:34-54) from the device SSE.
     const unsigned long long sse = *h_sse;
     double psnr = 100.0;
     if (sse) {
@@ -403,11 +478,12 @@ tc_error_t EncImpl::encode_poc_frame(int poc, int b_layer_qp_off, tc_packet_t *p
     }
     sum_psnr += psnr;
 
-    // ---- DPB shift: slot 3 falls out, the new reconstruction enters slot 0.
+    // DPB shift: slot 3 falls out, the new reconstruction enters slot 0
+    // (reference src/encoder.c:3085-3097).
     for (int i = TC_REF_FRAMES - 1; i > 0; --i) { dpb_slot[i] = dpb_slot[i - 1]; dpb_poc[i] = dpb_poc[i - 1]; }
     dpb_slot[0] = rs;
     dpb_poc[0] = poc;
-    last_rec = rs;
+    (void)qp;
 
     pkt->data = out_buf;
     pkt->size = frame_bytes;
@@ -418,7 +494,33 @@ tc_error_t EncImpl::encode_poc_frame(int poc, int b_layer_qp_off, tc_packet_t *p
     frame_count++;
     grid_cur = 1 - grid_cur;   // this frame's grid becomes the temporal predictor
     prev_mv_valid = 1;
+    if (pend.bf_idx >= 0) {
+        DevFrame &f = bf_frames[pend.bf_idx];
+        cudaFree(f.y); cudaFree(f.cb); cudaFree(f.cr);
+        bf_frames.erase(bf_frames.begin() + pend.bf_idx);
+        bf_pocs.erase(bf_pocs.begin() + pend.bf_idx);
+        pend.bf_idx = -1;
+    }
     return TC_OK;
+}
+
+tc_error_t EncImpl::encode_planned(tc_packet_t *pkt) {
+    tc_error_t r = stage_a(pend.poc, pend.qp_off);
+    if (r != TC_OK) return r;
+    if (pend.need_hist && cudaStreamSynchronize(st) != cudaSuccess) return TC_ERR_INTERNAL;
+    if ((r = stage_b()) != TC_OK) return r;
+    if ((r = launch_own()) != TC_OK) return r;
+    if ((r = stage_c()) != TC_OK) return r;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return TC_ERR_INTERNAL;
+    if (timing) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        ctu_ms += ms;
+        ctu_launches += (long long)diag_off.size();
+        ctu_count += (long long)ctu_cols * ctu_rows;
+        frames_timed++;
+    }
+    return stage_d(pkt);
 }
 
 long long tcb::tc_lambda_host(int qp) {
@@ -462,21 +564,6 @@ bool EncImpl::bf_can_emit() const {
     if ((p - 1) % 4 == 0) return true;
     return bf_emit_pos > bf_anchor_slot(p);
 }
-tc_error_t EncImpl::bf_emit_index(int idx, int poc, int qp_off, tc_packet_t *out) {
-    if (!dcopy(cur, bf_frames[idx])) return TC_ERR_INTERNAL;
-    const tc_error_t r = encode_poc_frame(poc, qp_off, out);
-    cudaFree(bf_frames[idx].y); cudaFree(bf_frames[idx].cb); cudaFree(bf_frames[idx].cr);
-    bf_frames.erase(bf_frames.begin() + idx);
-    bf_pocs.erase(bf_pocs.begin() + idx);
-    return r;
-}
-tc_error_t EncImpl::bf_emit_scheduled(tc_packet_t *out) {
-    const int p = bf_emit_pos;
-    const int poc = bf_schedule_poc(p);
-    const int idx = bf_find(poc);
-    bf_emit_pos++;
-    return bf_emit_index(idx, poc, bf_sched_qp_off(p), out);
-}
 tc_error_t EncImpl::bf_push_current() {
     if (bf_pocs.size() >= 8) return TC_OK;
     DevFrame f;
@@ -488,6 +575,61 @@ tc_error_t EncImpl::bf_push_current() {
     bf_frames.push_back(f);
     bf_pocs.push_back(bf_next_input);
     return TC_OK;
+}
+
+// Schedule the next coding-order frame from the reorder buffer into `cur`.
+tc_error_t EncImpl::bf_plan_scheduled() {
+    const int p = bf_emit_pos;
+    const int poc = bf_schedule_poc(p);
+    const int idx = bf_find(poc);
+    bf_emit_pos++;
+    if (!dcopy(cur, bf_frames[idx])) return TC_ERR_INTERNAL;
+    pend.poc = poc;
+    pend.qp_off = bf_sched_qp_off(p);
+    pend.bf_idx = idx;
+    return TC_OK;
+}
+
+// One input frame is staged in `cur`: decide whether it produces a coded
+// frame now (TC_OK, pend filled) or waits for the B-frame schedule
+// (TC_ERR_NEED_MORE) (reference src/encoder.c:3181-3212).
+tc_error_t EncImpl::plan_input() {
+    pend.bf_idx = -1;
+    if (bf_b_mode) {
+        const tc_error_t r = bf_push_current();
+        if (r != TC_OK) return r;
+        bf_next_input++;
+        if (!bf_can_emit()) return TC_ERR_NEED_MORE;
+        return bf_plan_scheduled();
+    }
+    pend.poc = frame_count;
+    pend.qp_off = 0;
+    return TC_OK;
+}
+
+// Tail drain (reference src/encoder.c:3256-3277): TC_OK with pend filled,
+// or TC_ERR_EOF.
+tc_error_t EncImpl::plan_flush() {
+    pend.bf_idx = -1;
+    if (!bf_b_mode) return TC_ERR_EOF;
+    if (bf_can_emit()) return bf_plan_scheduled();
+    if (!bf_pocs.empty()) {
+        int best = 0;
+        for (size_t i = 1; i < bf_pocs.size(); ++i)
+            if (bf_pocs[i] < bf_pocs[best]) best = (int)i;
+        if (!dcopy(cur, bf_frames[best])) return TC_ERR_INTERNAL;
+        pend.poc = bf_pocs[best];
+        pend.qp_off = 0;
+        pend.bf_idx = best;
+        return TC_OK;
+    }
+    return TC_ERR_EOF;
+}
+
+tc_error_t EncImpl::encode_input(tc_packet_t *out) {
+    const tc_error_t r = plan_input();
+    if (r != TC_OK) return r;
+    return encode_planned(out);
 }
 
 // ---------------------------------------------------------------------------
@@ -531,14 +673,41 @@ tc_error_t tc_encoder_encode(tc_encoder_t *enc, const tc_pixel_t *y, int stride_
     EncImpl &e = *enc->impl;
     if (cudaSetDevice(e.device) != cudaSuccess) return TC_ERR_INTERNAL;
     if (!e.upload(y, stride_y, cb, stride_cb, cr, stride_cr, e.cur)) return TC_ERR_INTERNAL;
-    if (e.bf_b_mode) {
-        const tc_error_t r = e.bf_push_current();
-        if (r != TC_OK) return r;
-        e.bf_next_input++;
-        if (!e.bf_can_emit()) return TC_ERR_NEED_MORE;
-        return e.bf_emit_scheduled(packet_out);
-    }
-    return e.encode_poc_frame(e.frame_count, 0, packet_out);
+    return e.encode_input(packet_out);
+}
+
+tc_error_t tcb_encoder_encode_device(tc_encoder_t *enc, const tc_pixel_t *d_y, int stride_y,
+                                     const tc_pixel_t *d_cb, int stride_cb, const tc_pixel_t *d_cr,
+                                     int stride_cr, tc_packet_t *packet_out) {
+    if (!enc || !enc->impl || !d_y || !d_cb || !d_cr || !packet_out) return TC_ERR_PARAM;
+    EncImpl &e = *enc->impl;
+    if (cudaSetDevice(e.device) != cudaSuccess) return TC_ERR_INTERNAL;
+    if (!e.upload(d_y, stride_y, d_cb, stride_cb, d_cr, stride_cr, e.cur, cudaMemcpyDeviceToDevice))
+        return TC_ERR_INTERNAL;
+    return e.encode_input(packet_out);
+}
+
+void *tcb_encoder_stream(tc_encoder_t *enc) { return enc && enc->impl ? (void *)enc->impl->st : nullptr; }
+
+void tcb_encoder_set_timing(tc_encoder_t *enc, int enabled) {
+    if (enc && enc->impl) enc->impl->timing = enabled != 0;
+}
+
+void tcb_encoder_get_timing(tc_encoder_t *enc, double *ctu_ms, int64_t *ctu_launches, int64_t *ctu_count,
+                            int64_t *frames, int64_t *kernel_launches) {
+    if (!enc || !enc->impl) return;
+    EncImpl &e = *enc->impl;
+    if (kernel_launches) *kernel_launches = e.kernel_launches;
+    e.kernel_launches = 0;
+    if (ctu_ms) *ctu_ms = e.ctu_ms;
+    if (ctu_launches) *ctu_launches = e.ctu_launches;
+    if (ctu_count) *ctu_count = e.ctu_count;
+    if (frames) *frames = e.frames_timed;
+    e.ctu_ms = 0.0; e.ctu_launches = 0; e.ctu_count = 0; e.frames_timed = 0;
+}
+
+void tcb_encoder_set_recon_readback(tc_encoder_t *enc, int enabled) {
+    if (enc && enc->impl) enc->impl->recon_readback = enabled != 0;
 }
 
 tc_error_t tc_encoder_flush_tail(tc_encoder_t *enc, tc_packet_t *packet_out) {
@@ -546,14 +715,9 @@ tc_error_t tc_encoder_flush_tail(tc_encoder_t *enc, tc_packet_t *packet_out) {
     EncImpl &e = *enc->impl;
     if (!e.bf_b_mode) return TC_ERR_EOF;
     if (cudaSetDevice(e.device) != cudaSuccess) return TC_ERR_INTERNAL;
-    if (e.bf_can_emit()) return e.bf_emit_scheduled(packet_out);
-    if (!e.bf_pocs.empty()) {
-        int best = 0;
-        for (size_t i = 1; i < e.bf_pocs.size(); ++i)
-            if (e.bf_pocs[i] < e.bf_pocs[best]) best = (int)i;
-        return e.bf_emit_index(best, e.bf_pocs[best], 0, packet_out);
-    }
-    return TC_ERR_EOF;
+    const tc_error_t r = e.plan_flush();
+    if (r != TC_OK) return r;
+    return e.encode_planned(packet_out);
 }
 
 void tc_encoder_force_keyframe(tc_encoder_t *enc) {

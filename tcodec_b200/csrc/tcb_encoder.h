@@ -10,6 +10,7 @@
 
 #include "../../include/tcodec.h"
 #include "tcb_common.cuh"
+#include "tcb_entropy.h"
 
 namespace tcb {
 
@@ -24,7 +25,8 @@ struct EncImpl {
     tc_config_t cfg{};
     int W = 0, H = 0, sy = 0, sc = 0, ctu_cols = 0, ctu_rows = 0, grid_w = 0, grid_h = 0;
     int device = 0;
-    cudaStream_t st = nullptr;
+    cudaStream_t st = nullptr;         // stream all work is issued on
+    cudaStream_t own_st = nullptr;     // the encoder's own stream
     cudaError_t last_cuda_error = cudaSuccess;
     DevFrame pool[NPOOL];
     DevFrame cur;
@@ -40,7 +42,17 @@ struct EncImpl {
     int *d_hist = nullptr, *h_hist = nullptr;
     unsigned long long *d_sse = nullptr, *h_sse = nullptr;
     int *d_err = nullptr;
+    // persistent wavefront: per-CTU publish flags, queue counter + error word
+    int *d_done = nullptr, *d_ctrl = nullptr, *h_ctrl = nullptr;
+    int epoch = 0, num_sms = 148;
+    bool persistent = true;
     tc_frame_buf_t *recon_host = nullptr;
+    bool recon_readback = true;
+    // optional CTU-engine timing
+    bool timing = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double ctu_ms = 0.0;
+    long long ctu_launches = 0, ctu_count = 0, frames_timed = 0, kernel_launches = 0;
     uint8_t *out_buf = nullptr;
     size_t out_buf_size = 0;
     // sequence state
@@ -63,17 +75,31 @@ struct EncImpl {
     bool init(const tc_config_t &c);
     void release();
     int free_pool_slot() const;
+    tc_error_t encode_input(tc_packet_t *out);
     bool upload(const tc_pixel_t *y, int ys, const tc_pixel_t *cb, int cbs, const tc_pixel_t *cr, int crs,
-                const DevFrame &dst);
+                const DevFrame &dst, cudaMemcpyKind kind = cudaMemcpyHostToDevice);
     bool dcopy(const DevFrame &dst, const DevFrame &src);
-    tc_error_t encode_poc_frame(int poc, int b_layer_qp_off, tc_packet_t *pkt);
+    // staged frame driver
+    struct Pending {
+        int poc = 0, qp_off = 0, need_hist = 0, is_key = 0, frame_type = 0, qp = 0, use_ep = 0,
+            rs = -1, multiref = 0, bf_idx = -1;
+    } pend;
+    BitWriter fbw;
+    std::vector<uint8_t> row_buf;
+    tc_error_t plan_input();
+    tc_error_t plan_flush();
+    tc_error_t stage_a(int poc, int b_layer_qp_off);
+    tc_error_t stage_b();
+    tc_error_t launch_own();
+    tc_error_t stage_c();
+    tc_error_t stage_d(tc_packet_t *pkt);
+    tc_error_t encode_planned(tc_packet_t *pkt);
+    tc_error_t bf_plan_scheduled();
     void rc_init(const tc_config_t &c);
     void rc_frame_start();
     void rc_frame_end(long long bits);
     int bf_find(int poc) const;
     bool bf_can_emit() const;
-    tc_error_t bf_emit_scheduled(tc_packet_t *out);
-    tc_error_t bf_emit_index(int idx, int poc, int qp_off, tc_packet_t *out);
     tc_error_t bf_push_current();
 };
 

@@ -262,7 +262,7 @@ __device__ __forceinline__ int lpred(const Smem &S, int cu, int slot, int dc, in
 }
 
 // Luma residual jobs, 8x8 TUs: one octet per (candidate, TU).
-__device__ void luma_jobs8(Smem &S, const Leaf &L, int ncl, const QuantParams &qp,
+__device__ void luma_jobs8(Smem &S, const Leaf &L, const int *cl, int ncl, const QuantParams &qp,
                            bool accum, bool wrec, int16_t *emit) {
     const int cu = L.cu, ntu = cu >> 3, ntu2 = ntu * ntu, J = ncl * ntu2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, oct = lane >> 3, l8 = lane & 7;
@@ -273,7 +273,7 @@ __device__ void luma_jobs8(Smem &S, const Leaf &L, int ncl, const QuantParams &q
         const bool act = j < J;
         const int jj = act ? j : 0;
         const int k = jj / ntu2, t = jj - k * ntu2, ty = t / ntu, tx = t - ty * ntu;
-        const int slot = S.cl[k];
+        const int slot = cl[k];
         int res[8];
         const int r = ty * 8 + l8;
 #pragma unroll
@@ -305,7 +305,7 @@ __device__ void luma_jobs8(Smem &S, const Leaf &L, int ncl, const QuantParams &q
 // Luma residual jobs, 4x4 TUs inside each 8x8 TU: one quad per
 // (candidate, TU, sub-block); the sub-block-0 quad adds the outer flag bit
 // (reference src/encoder.c:508-535).
-__device__ void luma_jobs4(Smem &S, const Leaf &L, int ncl, const QuantParams &qp,
+__device__ void luma_jobs4(Smem &S, const Leaf &L, const int *cl, int ncl, const QuantParams &qp,
                            bool accum, bool wrec, int16_t *emit) {
     const int cu = L.cu, ntu = cu >> 3, ntu2 = ntu * ntu, per = ntu2 * 4, J = ncl * per;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, qd = lane >> 2, l4 = lane & 3;
@@ -318,7 +318,7 @@ __device__ void luma_jobs4(Smem &S, const Leaf &L, int ncl, const QuantParams &q
         const int k = jj / per, rem = jj - k * per, t = rem >> 2, q = rem & 3;
         const int ty = t / ntu, tx = t - ty * ntu;
         const int sx = tx * 8 + (q & 1) * 4, sy = ty * 8 + (q & 2) * 2;
-        const int slot = S.cl[k];
+        const int slot = cl[k];
         int res[4];
 #pragma unroll
         for (int n = 0; n < 4; ++n) {
@@ -510,7 +510,16 @@ __device__ void luma_mc_slots(Smem &S, const FrameParams &P, const Leaf &L, int 
         const int slot = slots[k];
         LumaMC m;
         m.init(P.ref_y[S.cand_ref[slot]], P.stride_y, P.W, P.H, S.cand_mvx[slot], S.cand_mvy[slot], cu);
-        S.pred[slot][p] = (uint8_t)m.at(x, y);
+        int v = m.at(x, y);
+        const int r2 = S.cand_ref2[slot];
+        if (r2 >= 0) {
+            // Bi-average with the mirrored (negated absolute) MV on the
+            // second reference (reference src/encoder.c:642-647, 855-859).
+            LumaMC m2;
+            m2.init(P.ref_y[r2], P.stride_y, P.W, P.H, -S.cand_mvx[slot], -S.cand_mvy[slot], cu);
+            v = (v + m2.at(x, y) + 1) >> 1;
+        }
+        S.pred[slot][p] = (uint8_t)v;
     }
     SYNC();
 }
@@ -525,10 +534,10 @@ __device__ void zero_acc(Smem &S) {
 
 // Sum over the CU of |orig - pred| per listed slot into acc_sse[slot][0]
 // (fast-preset SAD proxy).
-__device__ void sad_jobs(Smem &S, const Leaf &L, int ncl) {
+__device__ void sad_jobs(Smem &S, const Leaf &L, const int *cl, int ncl) {
     const int cu = L.cu, n = cu * cu, dc = S.dc;
     for (int k = 0; k < ncl; ++k) {
-        const int slot = S.cl[k];
+        const int slot = cl[k];
         int acc = 0;
         for (int p = threadIdx.x; p < n; p += NT) {
             const int y = p / cu, x = p - y * cu;
@@ -593,6 +602,37 @@ __device__ void grid_update(Smem &S, const Leaf &L, const Node &nd, int mvpx, in
 }
 
 // ====================================================================
+// Reference selection for B-frames (reference src/encoder.c:204-228):
+// forward = largest POC below the current one, backward = smallest above.
+// ====================================================================
+__device__ __forceinline__ int dpb_fwd(const FrameParams &P) {
+    int best = -1, bp = -1;
+    for (int i = 0; i < MAX_REFS; ++i)
+        if (P.ref_valid[i] && P.ref_poc[i] >= 0 && P.ref_poc[i] < P.poc && P.ref_poc[i] > bp) { bp = P.ref_poc[i]; best = i; }
+    return best;
+}
+__device__ __forceinline__ int dpb_bwd(const FrameParams &P) {
+    int best = -1, bp = 0x7FFFFFFF;
+    for (int i = 0; i < MAX_REFS; ++i)
+        if (P.ref_valid[i] && P.ref_poc[i] >= 0 && P.ref_poc[i] > P.poc && P.ref_poc[i] < bp) { bp = P.ref_poc[i]; best = i; }
+    return best;
+}
+
+// Chroma MC of both components, averaged over two references when r2 >= 0
+// (second reference with the mirrored MV; reference src/encoder.c:673-699).
+__device__ void chroma_mc_bi(Smem &S, const FrameParams &P, const Leaf &L, int r1, int r2, int mvx, int mvy) {
+    const int cs = L.cu >> 1, Wc = P.W >> 1, Hc = P.H >> 1;
+    for (int i = threadIdx.x; i < 2 * cs * cs; i += NT) {
+        const int c = i / (cs * cs), p = i - c * cs * cs, y = p / cs, x = p - y * cs;
+        int v = chroma_mc_at(c ? P.ref_cr[r1] : P.ref_cb[r1], P.stride_c, Wc, Hc, mvx, mvy, x, y);
+        if (r2 >= 0)
+            v = (v + chroma_mc_at(c ? P.ref_cr[r2] : P.ref_cb[r2], P.stride_c, Wc, Hc, -mvx, -mvy, x, y) + 1) >> 1;
+        S.cpred[c][p] = (uint8_t)v;
+    }
+    SYNC();
+}
+
+// ====================================================================
 // Leaf coding of a decided node: replay in the decide pass, syntax-order
 // coefficient emission in the write pass (reference src/encoder.c:587-781).
 // ====================================================================
@@ -607,10 +647,10 @@ __device__ void leaf_code(Smem &S, const FrameParams &P, const Leaf &L, const Qu
     bool coded = true;
     if (nd.intra) {
         build_refs(S, L);
-        if (threadIdx.x == 0) { S.cl[0] = K_INTRA + nd.intra_mode; }
+        if (threadIdx.x == 0) { S.cl2[0] = K_INTRA + nd.intra_mode; }
         SYNC();
-        if (nd.dct_size) luma_jobs8(S, L, 1, ql, false, true, el);
-        else luma_jobs4(S, L, 1, ql, false, true, el);
+        if (nd.dct_size) luma_jobs8(S, L, S.cl2, 1, ql, false, true, el);
+        else luma_jobs4(S, L, S.cl2, 1, ql, false, true, el);
         SYNC();
         if (nd.ch_intra) {
             chroma_dc_pred(S, L, 0);
@@ -625,26 +665,51 @@ __device__ void leaf_code(Smem &S, const FrameParams &P, const Leaf &L, const Qu
         int mvx, mvy;
         if (nd.merge || nd.skip) { mvx = mvpx + L.px * 4; mvy = mvpy + L.py * 4; }
         else { mvx = mvpx + L.px * 4 + nd.mvd_x; mvy = mvpy + L.py * 4 + nd.mvd_y; }
-        if (P.frame_type == 2) {
-            // B replay handled by the B-frame path (forward-only fallback).
+        const bool bidir = P.frame_type == 2;
+        // Luma / chroma reference choice.
+        int r1 = 0, r2 = -1, cr1 = 0, cr2 = -1;
+        bool flat = false, cflat = false;   // no reference at all: 128 / chroma DC
+        if (bidir) {
+            const int rf = dpb_fwd(P), rb = dpb_bwd(P);
+            if (nd.bi) {
+                if (rf >= 0 && rb >= 0) { r1 = rf; r2 = rb; }
+                else if (rf >= 0) r1 = rf;
+                else if (rb >= 0) r1 = rb;
+                else flat = true;
+                if (rf >= 0 && rb >= 0) { cr1 = rf; cr2 = rb; }
+                else if (rf >= 0 || rb >= 0) cr1 = rf >= 0 ? rf : rb;
+                else cflat = true;
+            } else {
+                int rr = nd.ref_sel ? rb : rf;
+                if (rr < 0) rr = rf >= 0 ? rf : rb;
+                if (rr >= 0) r1 = rr; else flat = true;
+                int rc = nd.ref_sel ? rb : rf;
+                if (rc < 0) rc = 0;
+                cr1 = rc;
+            }
+        } else {
+            const int ri = nd.ref_sel & 3;
+            r1 = (ri < MAX_REFS && P.ref_valid[ri]) ? ri : 0;
+            cr1 = r1;
         }
         if (!nd.skip) {
-            const int ri = nd.ref_sel & 3;
-            const int r = (ri < MAX_REFS && P.ref_valid[ri]) ? ri : 0;
             if (threadIdx.x == 0) {
-                S.cand_mvx[0] = mvx; S.cand_mvy[0] = mvy; S.cand_ref[0] = r; S.cl[0] = 0;
+                S.cand_mvx[0] = mvx; S.cand_mvy[0] = mvy; S.cand_ref[0] = r1; S.cand_ref2[0] = r2;
+                S.cl2[0] = 0;
             }
             SYNC();
-            const int slots[1] = {0};
-            luma_mc_slots(S, P, L, 1, slots);
-            if (nd.dct_size) luma_jobs8(S, L, 1, ql, false, true, el);
-            else luma_jobs4(S, L, 1, ql, false, true, el);
-            SYNC();
-            if (nd.ch_intra) {
-                chroma_dc_pred(S, L, 0);
+            if (flat) {
+                for (int i = threadIdx.x; i < cu * cu; i += NT) S.pred[0][i] = 128;
+                SYNC();
             } else {
-                chroma_mc(S, P, L, r, mvx, mvy, 0, false);
+                const int slots[1] = {0};
+                luma_mc_slots(S, P, L, 1, slots);
             }
+            if (nd.dct_size) luma_jobs8(S, L, S.cl2, 1, ql, false, true, el);
+            else luma_jobs4(S, L, S.cl2, 1, ql, false, true, el);
+            SYNC();
+            if (nd.ch_intra || cflat) chroma_dc_pred(S, L, 0);
+            else chroma_mc_bi(S, P, L, cr1, cr2, mvx, mvy);
             chroma_jobs(S, L, 1, 0, qc, false, true, ec);
         } else {
             coded = false;
@@ -661,7 +726,14 @@ __device__ void leaf_code(Smem &S, const FrameParams &P, const Leaf &L, const Qu
         }
     }
     SYNC();
-    if (emit && coded && threadIdx.x == 0) S.ncoef += cu * cu + (cu * cu >> 1);
+    if (emit && coded && threadIdx.x == 0) {
+        S.ncoef += cu * cu + (cu * cu >> 1);
+        if (nd.dct_size) {
+            const int gc = cu >> 3;
+            for (int gy = 0; gy < gc; ++gy)
+                for (int gx = 0; gx < gc; ++gx) S.tu8mask |= 1ull << ((L.cy + gy) * 8 + L.cx + gx);
+        }
+    }
     grid_update(S, L, nd, mvpx, mvpy);
 }
 
@@ -675,16 +747,21 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
     const bool medium = P.preset >= 2;
     const bool key = P.frame_type == 0;
     const bool is_p = P.frame_type == 1;
+    const bool is_b = P.frame_type == 2;
     int mvpx, mvpy;
     mvp_at(S.grid, L.cx, L.cy, mvpx, mvpy);
     build_refs(S, L);
     zero_acc(S);
 
     // ---- candidate set -------------------------------------------------
-    const int sr = fast ? 16 : 24;
     bool has_glb = false, has_tmp = false, has_me1 = false;
+    int n8only = 0;          // merges coded with 8x8 TUs only, in S.cl2
     int tdx = 0, tdy = 0;
+    const int rf = is_b ? dpb_fwd(P) : -1, rb = is_b ? dpb_bwd(P) : -1;
+    const int g = tid / GT, gt = tid - g * GT;
+    const int cx0 = (mvpx + L.px * 4) >> 2, cy0 = (mvpy + L.py * 4) >> 2;
     if (is_p) {
+        const int sr = fast ? 16 : 24;
         has_me1 = !fast && P.multiref && P.ref_valid[1];
         has_glb = !fast && P.glob_valid &&
                   (P.glob_x > 16 || P.glob_x < -16 || P.glob_y > 16 || P.glob_y < -16);
@@ -696,8 +773,6 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
             }
         }
         // ---- motion searches on four warp groups ------------------------
-        const int g = tid / GT, gt = tid - g * GT;
-        const int cx0 = (mvpx + L.px * 4) >> 2, cy0 = (mvpy + L.py * 4) >> 2;
         if (g == 0)
             me_run(S, 0, gt, P.ref_y[0], P.stride_y, P.W, P.H, L.lx, L.ly, cu, cx0, cy0, sr);
         else if (g == 1 && has_me1)
@@ -711,7 +786,6 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
         SYNC();
         if (has_glb && S.me[2].mvx == S.me[0].mvx && S.me[2].mvy == S.me[0].mvy) has_glb = false;
         if (has_tmp && S.me[3].mvx == S.me[0].mvx && S.me[3].mvy == S.me[0].mvy) has_tmp = false;
-        // ---- inter predictions ------------------------------------------
         int slots[5], ns = 0;
         slots[ns++] = K_ME0;
         if (has_me1) slots[ns++] = K_ME1;
@@ -724,7 +798,42 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
             S.cand_mvx[K_GLB] = S.me[2].mvx; S.cand_mvy[K_GLB] = S.me[2].mvy; S.cand_ref[K_GLB] = 0;
             S.cand_mvx[K_TMP] = S.me[3].mvx; S.cand_mvy[K_TMP] = S.me[3].mvy; S.cand_ref[K_TMP] = 0;
             S.cand_mvx[K_MRG] = mvpx + L.px * 4; S.cand_mvy[K_MRG] = mvpy + L.py * 4; S.cand_ref[K_MRG] = 0;
+            for (int k = 0; k < NPRED; ++k) S.cand_ref2[k] = -1;
+            S.cl2[0] = K_MRG;
         }
+        if (medium) n8only = 1;
+        SYNC();
+        luma_mc_slots(S, P, L, ns, slots);
+    } else if (is_b) {
+        // Forward / backward searches (reference src/encoder.c:795-852).
+        const int sr = fast ? 16 : 32;
+        if (g == 0 && rf >= 0)
+            me_run(S, 0, gt, P.ref_y[rf], P.stride_y, P.W, P.H, L.lx, L.ly, cu, cx0, cy0, sr);
+        else if (g == 1 && rb >= 0)
+            me_run(S, 1, gt, P.ref_y[rb], P.stride_y, P.W, P.H, L.lx, L.ly, cu, cx0, cy0, sr);
+        SYNC();
+        int slots[5], ns = 0;
+        if (rf >= 0) slots[ns++] = K_B0 + 0;
+        if (rb >= 0) slots[ns++] = K_B0 + 1;
+        const bool mrg = medium && !fast;
+        if (mrg && rf >= 0 && rb >= 0) slots[ns++] = K_B0 + 2;
+        if (mrg && rf >= 0) slots[ns++] = K_B0 + 3;
+        if (mrg && rb >= 0) slots[ns++] = K_B0 + 4;
+        if (tid == 0) {
+            const int mmx = mvpx + L.px * 4, mmy = mvpy + L.py * 4;
+            for (int k = 0; k < NPRED; ++k) S.cand_ref2[k] = -1;
+            S.cand_mvx[K_B0 + 0] = S.me[0].mvx; S.cand_mvy[K_B0 + 0] = S.me[0].mvy; S.cand_ref[K_B0 + 0] = rf < 0 ? 0 : rf;
+            S.cand_mvx[K_B0 + 1] = S.me[1].mvx; S.cand_mvy[K_B0 + 1] = S.me[1].mvy; S.cand_ref[K_B0 + 1] = rb < 0 ? 0 : rb;
+            S.cand_mvx[K_B0 + 2] = mmx; S.cand_mvy[K_B0 + 2] = mmy; S.cand_ref[K_B0 + 2] = rf < 0 ? 0 : rf;
+            S.cand_ref2[K_B0 + 2] = rb;
+            S.cand_mvx[K_B0 + 3] = mmx; S.cand_mvy[K_B0 + 3] = mmy; S.cand_ref[K_B0 + 3] = rf < 0 ? 0 : rf;
+            S.cand_mvx[K_B0 + 4] = mmx; S.cand_mvy[K_B0 + 4] = mmy; S.cand_ref[K_B0 + 4] = rb < 0 ? 0 : rb;
+            int n = 0;
+            if (mrg && rf >= 0 && rb >= 0) S.cl2[n++] = K_B0 + 2;
+            if (mrg && rf >= 0) S.cl2[n++] = K_B0 + 3;
+            if (mrg && rb >= 0) S.cl2[n++] = K_B0 + 4;
+        }
+        n8only = (mrg && rf >= 0 && rb >= 0) + (mrg && rf >= 0) + (mrg && rb >= 0);
         SYNC();
         luma_mc_slots(S, P, L, ns, slots);
     }
@@ -740,6 +849,9 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
             if (has_me1) S.cl[n++] = K_ME1;
             if (has_glb) S.cl[n++] = K_GLB;
             if (has_tmp) S.cl[n++] = K_TMP;
+        } else if (is_b) {
+            if (rf >= 0) S.cl[n++] = K_B0 + 0;
+            if (rb >= 0) S.cl[n++] = K_B0 + 1;
         }
         const int ninter = n;
         if (try_intra)
@@ -754,19 +866,16 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
     SYNC();
     const int ncl = S.ncl, ninter = S.flag;
     if (fast) {
-        sad_jobs(S, L, ncl);
+        sad_jobs(S, L, S.cl, ncl);
         SYNC();
     } else {
-        luma_jobs8(S, L, ncl, ql, true, false, nullptr);
-        if (use4) luma_jobs4(S, L, ncl, ql, true, false, nullptr);
+        luma_jobs8(S, L, S.cl, ncl, ql, true, false, nullptr);
+        if (use4) luma_jobs4(S, L, S.cl, ncl, ql, true, false, nullptr);
+        if (n8only) luma_jobs8(S, L, S.cl2, n8only, ql, true, false, nullptr);
         SYNC();
         if (is_p && medium) {
-            // Merge: 8x8 only (reference src/encoder.c:1051-1057), placed
-            // after the list so the list above stays a prefix.
-            if (tid == 0) { S.cl[0] = K_MRG; }
-            SYNC();
-            luma_jobs8(S, L, 1, ql, true, false, nullptr);
-            // Skip pre-check: luma SSE of the merge prediction.
+            // Skip pre-check (src/encoder.c:1064-1142): luma SSE of the merge
+            // prediction, then fresh chroma SSE when the luma is exact.
             long long acc = 0;
             for (int p = tid; p < cu * cu; p += NT) {
                 const int y = p / cu, x = p - y * cu;
@@ -800,10 +909,40 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
     if (tid == 0) {
         const long long lam = P.lambda;
         long long best = (long long)1 << 60;
-        int b_intra = 0, b_skip = 0, b_merge = 0, b_dct = 1, b_ref = 0, b_mvdx = 0, b_mvdy = 0;
+        int b_intra = 0, b_skip = 0, b_merge = 0, b_dct = 1, b_ref = 0, b_bi = 0, b_mvdx = 0, b_mvdy = 0;
         int b_imode = 1, best_imode = 1;
-        if (is_p) {
-            const int base_x = mvpx + L.px * 4, base_y = mvpy + L.py * 4;
+        const int base_x = mvpx + L.px * 4, base_y = mvpy + L.py * 4;
+        if (is_b) {
+            for (int dir = 0; dir < 2; ++dir) {
+                if ((dir == 0 ? rf : rb) < 0) continue;
+                const int slot = K_B0 + dir;
+                const int dx = S.cand_mvx[slot] - base_x, dy = S.cand_mvy[slot] - base_y;
+                long long dl; int lb, dct = 1;
+                if (fast) {
+                    const long long sad = S.acc_sse[slot][0];
+                    dl = (sad * sad) / (long long)(cu * cu);
+                    lb = 3;
+                } else {
+                    dl = best_of(S, slot, use4, lam, lb, dct);
+                }
+                const long long cost = dl + lam * (6 + se_bits(dx) + se_bits(dy) + lb);
+                if (cost < best) { best = cost; b_dct = dct; b_mvdx = dx; b_mvdy = dy; b_ref = dir; b_bi = 0; }
+            }
+            if (medium && !fast) {
+                const int order[3] = {2, 3, 4};
+                for (int i = 0; i < 3; ++i) {
+                    const int k = order[i];
+                    const bool ok = k == 2 ? (rf >= 0 && rb >= 0) : (k == 3 ? rf >= 0 : rb >= 0);
+                    if (!ok) continue;
+                    const int slot = K_B0 + k;
+                    const long long cost = (long long)S.acc_sse[slot][0] + lam * (6 + S.acc_bits[slot][0]);
+                    if (cost < best) {
+                        best = cost; b_merge = 1; b_mvdx = 0; b_mvdy = 0; b_dct = 1;
+                        b_ref = k == 4 ? 1 : 0; b_bi = k == 2 ? 1 : 0;
+                    }
+                }
+            }
+        } else if (is_p) {
             // Explicit inter from the MVP centre.
             {
                 const int dx = S.cand_mvx[K_ME0] - base_x, dy = S.cand_mvy[K_ME0] - base_y;
@@ -851,7 +990,7 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
                     best = cost; b_merge = 1; b_dct = 1; b_ref = 0;
                     b_mvdx = S.cand_mvx[K_ME0] - base_x; b_mvdy = S.cand_mvy[K_ME0] - base_y;
                 }
-                if (!fast && P.ref_valid[0] && S.acc64[0] == 0 && S.acc64[1] == 0) {
+                if (P.ref_valid[0] && S.acc64[0] == 0 && S.acc64[1] == 0) {
                     const long long cost_skip = lam * 2;
                     if (cost_skip < best) {
                         best = cost_skip; b_skip = 1; b_merge = 0; b_dct = 1; b_mvdx = 0; b_mvdy = 0; b_ref = 0;
@@ -873,13 +1012,13 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
                 const long long cost = dl + lam * (8 + lb);
                 if (cost < best) {
                     best = cost; b_intra = 1; best_imode = m; b_dct = dct; b_skip = 0; b_merge = 0;
-                    b_mvdx = 0; b_mvdy = 0; b_ref = 0;
+                    b_mvdx = 0; b_mvdy = 0; b_ref = 0; b_bi = 0;
                 }
             }
             if (b_intra) b_imode = best_imode;
         }
         Node &nd = S.nodes[qt_index(L.depth, L.cx, L.cy)];
-        nd.intra = (uint8_t)b_intra; nd.skip = (uint8_t)b_skip; nd.merge = (uint8_t)b_merge; nd.bi = 0;
+        nd.intra = (uint8_t)b_intra; nd.skip = (uint8_t)b_skip; nd.merge = (uint8_t)b_merge; nd.bi = (uint8_t)b_bi;
         nd.intra_mode = (uint8_t)b_imode; nd.intra_cmode = 0; nd.ch_intra = 0;
         nd.ref_sel = (uint8_t)b_ref; nd.dct_size = (uint8_t)b_dct;
         nd.mvd_x = (int16_t)b_mvdx; nd.mvd_y = (int16_t)b_mvdy;
@@ -891,10 +1030,10 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
     // ---- intra chroma choice: MC vs CfL-blended DC (src/encoder.c:1194-1221)
     const Node nd0 = S.nodes[qt_index(L.depth, L.cx, L.cy)];
     if (nd0.intra && !fast && medium) {
-        if (tid == 0) S.cl[0] = K_INTRA + nd0.intra_mode;
+        if (tid == 0) S.cl2[0] = K_INTRA + nd0.intra_mode;
         SYNC();
-        if (nd0.dct_size) luma_jobs8(S, L, 1, ql, false, true, nullptr);
-        else luma_jobs4(S, L, 1, ql, false, true, nullptr);
+        if (nd0.dct_size) luma_jobs8(S, L, S.cl2, 1, ql, false, true, nullptr);
+        else luma_jobs4(S, L, S.cl2, 1, ql, false, true, nullptr);
         SYNC();
         if (P.ref_valid[0]) chroma_mc(S, P, L, 0, mvpx + L.px * 4, mvpy + L.py * 4, 0, false);
         else chroma_dc_pred(S, L, 0);
@@ -922,9 +1061,27 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
 // ====================================================================
 // Quadtree recursion (reference src/encoder.c:1292-1397).
 // ====================================================================
+// `cached`: this node was already evaluated as a leaf (in its parent's
+// split test) from exactly the state it sees now — every earlier sibling
+// kept the leaf decision it had then — so its decision (still in
+// S.nodes) and cost (S.node_cost) are reused and only the replay runs.
+template <int D>
+__device__ long long leaf_eval(Smem &S, const FrameParams &P, const Leaf &L, const QuantParams &ql,
+                               const QuantParams &qc, bool cached) {
+    const int idx = qt_index(L.depth, L.cx, L.cy);
+    if (cached) {
+        const long long c = S.node_cost[idx];
+        leaf_code(S, P, L, ql, qc, false, nullptr);
+        return c;
+    }
+    const long long c = leaf_decide(S, P, L, ql, qc);
+    if (threadIdx.x == 0) S.node_cost[idx] = c;
+    return c;
+}
+
 template <int D>
 __device__ void qt_decide(Smem &S, const FrameParams &P, int ctu_x, int ctu_y, int cx, int cy,
-                          const QuantParams &ql, const QuantParams &qc) {
+                          const QuantParams &ql, const QuantParams &qc, bool cached) {
     constexpr int cu = 64 >> D;
     const int px = ctu_x + cx * 8, py = ctu_y + cy * 8;
     const bool in_frame = px + cu <= P.W && py + cu <= P.H;
@@ -933,7 +1090,7 @@ __device__ void qt_decide(Smem &S, const FrameParams &P, int ctu_x, int ctu_y, i
         constexpr int h = 4 >> D;   // child offset in cells
         if (!in_frame) {
             for (int q = 0; q < 4; ++q)
-                qt_decide<D + 1>(S, P, ctu_x, ctu_y, cx + (q & 1) * h, cy + (q >> 1) * h, ql, qc);
+                qt_decide<D + 1>(S, P, ctu_x, ctu_y, cx + (q & 1) * h, cy + (q >> 1) * h, ql, qc, false);
             return;
         }
         const int fast_leaf_depth = P.preset == 0 ? 3 : 2;
@@ -941,24 +1098,30 @@ __device__ void qt_decide(Smem &S, const FrameParams &P, int ctu_x, int ctu_y, i
             if (threadIdx.x == 0) nd.split = 1;
             SYNC();
             for (int q = 0; q < 4; ++q)
-                qt_decide<D + 1>(S, P, ctu_x, ctu_y, cx + (q & 1) * h, cy + (q >> 1) * h, ql, qc);
+                qt_decide<D + 1>(S, P, ctu_x, ctu_y, cx + (q & 1) * h, cy + (q >> 1) * h, ql, qc, false);
             return;
         }
         const Leaf L(P, ctu_x, ctu_y, D, cx, cy);
         snap<D>(S, L, 0, true);
-        const long long parent = leaf_decide(S, P, L, ql, qc);
+        const long long parent = leaf_eval<D>(S, P, L, ql, qc, cached);
         snap<D>(S, L, 1, true);
         snap<D>(S, L, 0, false);
         long long child = 0;
         for (int q = 0; q < 4; ++q) {
             const Leaf C(P, ctu_x, ctu_y, D + 1, cx + (q & 1) * h, cy + (q >> 1) * h);
-            child += leaf_decide(S, P, C, ql, qc);
+            child += leaf_eval<D + 1>(S, P, C, ql, qc, false);
         }
         if (child <= parent) {
             if (threadIdx.x == 0) nd.split = 1;
             snap<D>(S, L, 0, false);
-            for (int q = 0; q < 4; ++q)
-                qt_decide<D + 1>(S, P, ctu_x, ctu_y, cx + (q & 1) * h, cy + (q >> 1) * h, ql, qc);
+            // Children keep their split-test evaluation until one of them
+            // splits (its region then differs from the split test's state).
+            bool same_state = true;
+            for (int q = 0; q < 4; ++q) {
+                const int qx = cx + (q & 1) * h, qy = cy + (q >> 1) * h;
+                qt_decide<D + 1>(S, P, ctu_x, ctu_y, qx, qy, ql, qc, same_state);
+                if (S.nodes[qt_index(D + 1, qx, qy)].split) same_state = false;
+            }
         } else {
             if (threadIdx.x == 0) nd.split = 0;
             snap<D>(S, L, 1, false);
@@ -966,7 +1129,7 @@ __device__ void qt_decide(Smem &S, const FrameParams &P, int ctu_x, int ctu_y, i
     } else {
         if (!in_frame) return;
         const Leaf L(P, ctu_x, ctu_y, D, cx, cy);
-        leaf_decide(S, P, L, ql, qc);
+        leaf_eval<D>(S, P, L, ql, qc, cached);
         if (threadIdx.x == 0) nd.split = 0;
         SYNC();
     }
@@ -1107,15 +1270,7 @@ __device__ void sao_tile(Smem &S, int w, int h, int lambda_sao) {
 // ====================================================================
 // The CTU kernel.  items[i] = (stream << 20) | (row << 10) | col.
 // ====================================================================
-__global__ void __launch_bounds__(NT, 1)
-ctu_kernel(const FrameParams *__restrict__ params, const int *__restrict__ items) {
-    extern __shared__ __align__(16) uint8_t smem_raw[];
-    Smem &S = *reinterpret_cast<Smem *>(smem_raw);
-    __shared__ FrameParams P;
-    const int item = items[blockIdx.x];
-    const int sid = item >> 20, row = (item >> 10) & 1023, col = item & 1023;
-    if (threadIdx.x == 0) P = params[sid];
-    SYNC();
+__device__ void encode_ctu(Smem &S, const FrameParams &P, int row, int col) {
     const int ctu_x = col * 64, ctu_y = row * 64;
     const int w = mini(64, P.W - ctu_x), h = mini(64, P.H - ctu_y);
     const int wc = w >> 1, hc = h >> 1;
@@ -1131,23 +1286,23 @@ ctu_kernel(const FrameParams *__restrict__ params, const int *__restrict__ items
     }
     if (ctu_y > 0) {
         for (int x = threadIdx.x - 2; x < w; x += NT)
-            if (ctu_x + x >= 0) RY(S, x, -1) = P.rec_y[(size_t)(ctu_y - 1) * P.stride_y + ctu_x + x];
+            if (ctu_x + x >= 0) RY(S, x, -1) = __ldcg(P.rec_y + (size_t)(ctu_y - 1) * P.stride_y + ctu_x + x);
         for (int i = threadIdx.x; i < 2 * 33; i += NT) {
             const int c = i / 33, x = i - c * 33 - 1;
             const uint8_t *src = c ? P.rec_cr : P.rec_cb;
             if (x < wc && ctu_x / 2 + x >= 0)
-                RC(S, c, x, -1) = src[(size_t)((ctu_y >> 1) - 1) * P.stride_c + (ctu_x >> 1) + x];
+                RC(S, c, x, -1) = __ldcg(src + (size_t)((ctu_y >> 1) - 1) * P.stride_c + (ctu_x >> 1) + x);
         }
     }
     if (ctu_x > 0) {
         for (int i = threadIdx.x; i < 2 * h; i += NT) {
             const int y = i >> 1, x = (i & 1) - 2;
-            RY(S, x, y) = P.rec_y[(size_t)(ctu_y + y) * P.stride_y + ctu_x + x];
+            RY(S, x, y) = __ldcg(P.rec_y + (size_t)(ctu_y + y) * P.stride_y + ctu_x + x);
         }
         for (int i = threadIdx.x; i < 2 * hc; i += NT) {
             const int c = i / hc, y = i - c * hc;
             const uint8_t *src = c ? P.rec_cr : P.rec_cb;
-            RC(S, c, -1, y) = src[(size_t)((ctu_y >> 1) + y) * P.stride_c + (ctu_x >> 1) - 1];
+            RC(S, c, -1, y) = __ldcg(src + (size_t)((ctu_y >> 1) + y) * P.stride_c + (ctu_x >> 1) - 1);
         }
     }
     for (int i = threadIdx.x; i < 64; i += NT) {
@@ -1157,7 +1312,7 @@ ctu_kernel(const FrameParams *__restrict__ params, const int *__restrict__ items
         Node z = {};
         S.nodes[i] = z;
     }
-    if (threadIdx.x == 0) S.ncoef = 0;
+    if (threadIdx.x == 0) { S.ncoef = 0; S.tu8mask = 0; }
     SYNC();
 
     QuantParams ql, qc;
@@ -1170,7 +1325,7 @@ ctu_kernel(const FrameParams *__restrict__ params, const int *__restrict__ items
     qc.lambda = P.lambda_c;
 
     // ---- decide, then write in syntax order ----------------------------
-    qt_decide<0>(S, P, ctu_x, ctu_y, 0, 0, ql, qc);
+    qt_decide<0>(S, P, ctu_x, ctu_y, 0, 0, ql, qc, false);
     for (int i = threadIdx.x; i < 64; i += NT) {
         S.grid[i].dx = 0; S.grid[i].dy = 0; S.grid[i].intra = 1;
     }
@@ -1199,17 +1354,92 @@ ctu_kernel(const FrameParams *__restrict__ params, const int *__restrict__ items
     for (int i = threadIdx.x; i < QT_NODES; i += NT) out->nodes[i] = S.nodes[i];
     if (threadIdx.x == 0) {
         out->ncoef = S.ncoef;
+        out->tu8mask = S.tu8mask;
         out->sao_has = (int16_t)S.sao[0];
         out->sao_band = (int16_t)S.sao[1];
         out->sao_offset = (int16_t)S.sao[2];
     }
 }
 
+// One CTA per CTU of one anti-diagonal (items[blockIdx.x]).
+__global__ void __launch_bounds__(NT, 1)
+ctu_kernel(const FrameParams *__restrict__ params, const int *__restrict__ items) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    Smem &S = *reinterpret_cast<Smem *>(smem_raw);
+    __shared__ FrameParams P;
+    const int item = items[blockIdx.x];
+    if (threadIdx.x == 0) P = params[item >> 20];
+    SYNC();
+    encode_ctu(S, P, (item >> 10) & 1023, item & 1023);
+}
+
+__device__ __forceinline__ int ld_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int *p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Persistent wavefront: a resident grid pulls CTUs from a queue laid out in
+// topological (anti-diagonal) order and starts each one as soon as its
+// left and above neighbours are published.  A CTU only ever waits for
+// items dequeued before it, by CTAs that are already running, so the queue
+// always drains.  Waits are bounded: on expiry the CTA records an error in
+// ctrl[1] and goes on, and the host reports TC_ERR_INTERNAL.
+__global__ void __launch_bounds__(NT, 1)
+ctu_persistent_kernel(const FrameParams *__restrict__ params, const int *__restrict__ items, int n_items,
+                      int *ctrl) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    Smem &S = *reinterpret_cast<Smem *>(smem_raw);
+    __shared__ FrameParams P;
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int i = atomicAdd(&ctrl[0], 1);
+            s_item = i < n_items ? items[i] : -1;
+        }
+        SYNC();
+        const int item = s_item;
+        if (item < 0) break;
+        const int row = (item >> 10) & 1023, col = item & 1023;
+        if (threadIdx.x == 0) {
+            P = params[item >> 20];
+            const int epoch = P.epoch;
+            const int *dl = col > 0 ? P.done + row * P.ctu_cols + col - 1 : nullptr;
+            const int *du = row > 0 ? P.done + (row - 1) * P.ctu_cols + col : nullptr;
+            unsigned ns = 32;
+            long long spins = 0;
+            while ((dl && ld_acquire(dl) != epoch) || (du && ld_acquire(du) != epoch)) {
+                __nanosleep(ns);
+                if (ns < 2048) ns <<= 1;
+                if (++spins > (1ll << 22)) { atomicExch(&ctrl[1], 1); break; }
+            }
+        }
+        SYNC();
+        encode_ctu(S, P, row, col);
+        __threadfence();
+        SYNC();
+        if (threadIdx.x == 0) st_release(P.done + row * P.ctu_cols + col, P.epoch);
+    }
+}
+
 cudaError_t init_engine_tables() {
     cudaError_t e = upload_dct_tables();
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(ctu_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(Smem));
+    if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(ctu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(Smem));
+}
+
+cudaError_t launch_ctu_persistent(const FrameParams *d_params, const int *d_items, int n, int *d_ctrl,
+                                  int grid, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    ctu_persistent_kernel<<<grid < n ? grid : n, NT, sizeof(Smem), st>>>(d_params, d_items, n, d_ctrl);
+    return cudaGetLastError();
 }
 
 size_t ctu_smem_bytes() { return sizeof(Smem); }
@@ -1218,6 +1448,301 @@ cudaError_t launch_ctu_items(const FrameParams *d_params, const int *d_items, in
                              cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     ctu_kernel<<<n, NT, sizeof(Smem), st>>>(d_params, d_items);
+    return cudaGetLastError();
+}
+
+}  // namespace tcb
+
+// ====================================================================
+// Decoder reconstruction (reference src/decoder.c:1521-1816): the same
+// wavefront of CTAs rebuilds each CTU from its parsed record — prediction
+// exactly as the encoder's write pass, residual from the transmitted
+// levels.  Levels come from an arbitrary bitstream, so the second inverse
+// pass accumulates in 64 bits.
+// ====================================================================
+namespace tcb {
+
+__device__ __forceinline__ int dq_eff(const QuantParams &qp, int pos, int n) {
+    return qp.eff[freq_band(pos, n)];
+}
+
+// 8x8 TU from levels on an octet; writes pred + residual into the tile.
+__device__ void dec_luma8(Smem &S, const Leaf &L, int slot, const int16_t *lv, const QuantParams &qp) {
+    const int cu = L.cu, ntu = cu >> 3, J = ntu * ntu;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, oct = lane >> 3, l8 = lane & 7;
+    int *scr = S.scratch[warp] + oct * 64;
+    const int dc = S.dc;
+    for (int base = 0; base < J; base += NW * 4) {
+        const int t = base + warp * 4 + oct;
+        const int t0 = t < J ? t : 0, ty0 = t0 / ntu, tx0 = t0 - ty0 * ntu;
+        const bool act = t < J && ((S.tu8mask >> ((L.cy + ty0) * 8 + L.cx + tx0)) & 1);
+        const int tt = act ? t : 0, ty = tt / ntu, tx = tt - ty * ntu;
+        int row[8];
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+            const int pos = l8 * 8 + n;
+            row[n] = (int16_t)dequant_coeff(act ? lv[tt * 64 + pos] : 0, dq_eff(qp, pos, 64));
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            int acc = 0;
+#pragma unroll
+            for (int n = 0; n < 8; ++n) acc += c_dct8[n][k] * row[n];
+            scr[l8 * 8 + k] = (acc + 8192) >> 14;
+        }
+        __syncwarp();
+        long long col[8];
+#pragma unroll
+        for (int n = 0; n < 8; ++n) col[n] = scr[n * 8 + l8];
+        __syncwarp();
+        const int x = tx * 8 + l8;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            long long acc = 0;
+#pragma unroll
+            for (int n = 0; n < 8; ++n) acc += (long long)c_dct8[n][k] * col[n];
+            const int r = (int16_t)(int)((acc + 8192) >> 14);
+            const int y = ty * 8 + k;
+            if (act) RY(S, L.lx + x, L.ly + y) = (uint8_t)clampi(lpred(S, cu, slot, dc, x, y) + r, 0, 255);
+        }
+    }
+}
+
+// 4x4 TUs from levels on quads.  Luma: per 8x8 TU four sub-blocks in
+// raster order; chroma (chroma_c >= 0): (cs/4)^2 TUs of that component.
+__device__ void dec_tu4(Smem &S, const Leaf &L, int slot, int chroma_c, const int16_t *lv,
+                        const QuantParams &qp) {
+    const int cu = L.cu;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, qd = lane >> 2, l4 = lane & 3;
+    int *scr = S.scratch[warp] + qd * 16;
+    const int dc = S.dc;
+    const int cs = cu >> 1;
+    const int J = chroma_c >= 0 ? (cs >> 2) * (cs >> 2) : (cu >> 3) * (cu >> 3) * 4;
+    for (int base = 0; base < J; base += NW * 8) {
+        const int j = base + warp * 8 + qd;
+        bool act = j < J;
+        if (act && chroma_c < 0) {
+            const int ntu = cu >> 3, t = j >> 2;
+            act = !((S.tu8mask >> ((L.cy + t / ntu) * 8 + L.cx + t % ntu)) & 1);
+        }
+        const int jj = act ? j : 0;
+        int sx, sy;
+        if (chroma_c >= 0) {
+            const int nt = cs >> 2, ty = jj / nt, tx = jj - ty * nt;
+            sx = tx * 4; sy = ty * 4;
+        } else {
+            const int ntu = cu >> 3, t = jj >> 2, q = jj & 3, ty = t / ntu, tx = t - ty * ntu;
+            sx = tx * 8 + (q & 1) * 4; sy = ty * 8 + (q & 2) * 2;
+        }
+        int row[4];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            const int pos = l4 * 4 + n;
+            row[n] = (int16_t)dequant_coeff(act ? lv[jj * 16 + pos] : 0, dq_eff(qp, pos, 16));
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            int acc = 0;
+#pragma unroll
+            for (int n = 0; n < 4; ++n) acc += c_dct4[n][k] * row[n];
+            scr[l4 * 4 + k] = (acc + 8192) >> 14;
+        }
+        __syncwarp();
+        long long col[4];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) col[n] = scr[n * 4 + l4];
+        __syncwarp();
+        const int x = sx + l4;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            long long acc = 0;
+#pragma unroll
+            for (int n = 0; n < 4; ++n) acc += (long long)c_dct4[n][k] * col[n];
+            const int r = (int16_t)(int)((acc + 8192) >> 14);
+            const int y = sy + k;
+            if (!act) continue;
+            if (chroma_c >= 0) {
+                const int v = clampi((int)S.cpred[chroma_c][y * cs + x] + r, 0, 255);
+                RC(S, chroma_c, (L.lx >> 1) + x, (L.ly >> 1) + y) = (uint8_t)v;
+            } else {
+                RY(S, L.lx + x, L.ly + y) = (uint8_t)clampi(lpred(S, cu, slot, dc, x, y) + r, 0, 255);
+            }
+        }
+    }
+}
+
+// Decoder prediction reference choice (reference src/decoder.c:1628-1664,
+// 1697-1750); `flat` = no reference (128 / chroma DC).
+__device__ void dec_leaf(Smem &S, const FrameParams &P, const Leaf &L, const int16_t *coef,
+                         const QuantParams &ql, const QuantParams &qc) {
+    const Node nd = S.nodes[qt_index(L.depth, L.cx, L.cy)];
+    int mvpx, mvpy;
+    mvp_at(S.grid, L.cx, L.cy, mvpx, mvpy);
+    const int cu = L.cu;
+    const int16_t *el = coef + S.ncoef, *ec = el + cu * cu;
+    const bool use_mvd = !(nd.skip || nd.merge || nd.intra);
+    const int mvx = (int16_t)(mvpx + L.px * 4 + (use_mvd ? nd.mvd_x : 0));
+    const int mvy = (int16_t)(mvpy + L.py * 4 + (use_mvd ? nd.mvd_y : 0));
+    const bool bidir = P.frame_type == 2;
+    int slot = 0;
+    if (nd.intra) {
+        build_refs(S, L);
+        slot = K_INTRA + nd.intra_mode;
+    } else {
+        int r1 = -1, r2 = -1;
+        if (bidir) {
+            const int rf = dpb_fwd(P), rb = dpb_bwd(P);
+            if ((nd.bi || nd.skip) && rf >= 0 && rb >= 0) { r1 = rf; r2 = rb; }
+            else {
+                int r = nd.bi ? rf : (nd.ref_sel ? rb : rf);
+                if (r < 0) r = rf >= 0 ? rf : rb;
+                r1 = r;
+            }
+        } else {
+            r1 = (nd.ref_sel < MAX_REFS && P.ref_valid[nd.ref_sel]) ? nd.ref_sel : -1;
+        }
+        if (threadIdx.x == 0) {
+            S.cand_mvx[0] = mvx; S.cand_mvy[0] = mvy; S.cand_ref[0] = r1 < 0 ? 0 : r1; S.cand_ref2[0] = r2;
+        }
+        SYNC();
+        if (r1 >= 0) {
+            const int slots[1] = {0};
+            luma_mc_slots(S, P, L, 1, slots);
+        } else {
+            for (int i = threadIdx.x; i < cu * cu; i += NT) S.pred[0][i] = 128;
+            SYNC();
+        }
+        slot = 0;
+    }
+    if (nd.skip) {
+        for (int i = threadIdx.x; i < cu * cu; i += NT) {
+            const int y = i / cu, x = i - y * cu;
+            RY(S, L.lx + x, L.ly + y) = S.pred[0][i];
+        }
+        SYNC();
+        if (P.fresh_skip && P.frame_type == 1 && P.ref_valid[0]) chroma_mc(S, P, L, 0, mvx, mvy, 0, true);
+        grid_update(S, L, nd, mvpx, mvpy);
+        return;
+    }
+    // Luma residual: each 8x8 region carries its own TU-size flag.
+    dec_luma8(S, L, slot, el, ql);
+    dec_tu4(S, L, slot, -1, el, ql);
+    SYNC();
+    // Chroma prediction.
+    if (nd.intra) {
+        if (nd.ch_intra) { chroma_dc_pred(S, L, 0); cfl_blend(S, L, 0); }
+        else if (P.ref_valid[0]) chroma_mc(S, P, L, 0, mvx, mvy, 0, false);
+        else chroma_dc_pred(S, L, 0);
+    } else if (bidir && nd.bi) {
+        const int cf = dpb_fwd(P), cbw = dpb_bwd(P);
+        if (cf >= 0 && cbw >= 0) chroma_mc_bi(S, P, L, cf, cbw, mvx, mvy);
+        else if (cf >= 0 || cbw >= 0) chroma_mc_bi(S, P, L, cf >= 0 ? cf : cbw, -1, mvx, mvy);
+        else chroma_dc_pred(S, L, 0);
+    } else {
+        int r = (nd.ref_sel < MAX_REFS && P.ref_valid[nd.ref_sel]) ? nd.ref_sel : -1;
+        if (bidir) r = nd.ref_sel ? dpb_bwd(P) : dpb_fwd(P);
+        if (r >= 0) chroma_mc_bi(S, P, L, r, -1, mvx, mvy);
+        else chroma_dc_pred(S, L, 0);
+    }
+    dec_tu4(S, L, 0, 0, ec, qc);
+    dec_tu4(S, L, 0, 1, ec + (cu >> 1) * (cu >> 1), qc);
+    SYNC();
+    if (threadIdx.x == 0) S.ncoef += cu * cu + (cu * cu >> 1);
+    grid_update(S, L, nd, mvpx, mvpy);
+}
+
+template <int D>
+__device__ void qt_dec(Smem &S, const FrameParams &P, int ctu_x, int ctu_y, int cx, int cy,
+                       const int16_t *coef, const QuantParams &ql, const QuantParams &qc) {
+    constexpr int cu = 64 >> D;
+    const int px = ctu_x + cx * 8, py = ctu_y + cy * 8;
+    const bool in_frame = px + cu <= P.W && py + cu <= P.H;
+    if constexpr (D < 3) {
+        constexpr int h = 4 >> D;
+        if (!in_frame || S.nodes[qt_index(D, cx, cy)].split) {
+            for (int q = 0; q < 4; ++q)
+                qt_dec<D + 1>(S, P, ctu_x, ctu_y, cx + (q & 1) * h, cy + (q >> 1) * h, coef, ql, qc);
+            return;
+        }
+    } else {
+        if (!in_frame) return;
+    }
+    const Leaf L(P, ctu_x, ctu_y, D, cx, cy);
+    dec_leaf(S, P, L, coef, ql, qc);
+}
+
+__global__ void __launch_bounds__(NT, 1)
+decode_kernel(const FrameParams *__restrict__ params, const int *__restrict__ items) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    Smem &S = *reinterpret_cast<Smem *>(smem_raw);
+    __shared__ FrameParams P;
+    const int item = items[blockIdx.x];
+    const int sid = item >> 20, row = (item >> 10) & 1023, col = item & 1023;
+    if (threadIdx.x == 0) P = params[sid];
+    SYNC();
+    const int ctu_x = col * 64, ctu_y = row * 64;
+    const int w = mini(64, P.W - ctu_x), h = mini(64, P.H - ctu_y);
+    const int wc = w >> 1, hc = h >> 1;
+    const CtuOut *rec = P.out + row * P.ctu_cols + col;
+    // Border from the frame being rebuilt; interior starts from the
+    // persistent reconstruction buffer (stale samples are only ever read
+    // by streams that skip with stale chroma, as in the reference).
+    for (int i = threadIdx.x; i < 65 * 66; i += NT) {
+        const int y = i / 66 - 1, x = i % 66 - 2;
+        if (ctu_y + y >= 0 && ctu_x + x >= 0 && y < h && x < w)
+            RY(S, x, y) = P.rec_y[(size_t)(ctu_y + y) * P.stride_y + ctu_x + x];
+    }
+    for (int i = threadIdx.x; i < 2 * 33 * 33; i += NT) {
+        const int c = i / (33 * 33), p = i - c * 33 * 33, y = p / 33 - 1, x = p % 33 - 1;
+        const uint8_t *src = c ? P.rec_cr : P.rec_cb;
+        if ((ctu_y >> 1) + y >= 0 && (ctu_x >> 1) + x >= 0 && y < hc && x < wc)
+            RC(S, c, x, y) = src[(size_t)((ctu_y >> 1) + y) * P.stride_c + (ctu_x >> 1) + x];
+    }
+    for (int i = threadIdx.x; i < 64; i += NT) {
+        S.grid[i].dx = 0; S.grid[i].dy = 0; S.grid[i].intra = 1; S.grid[i].pad = 0;
+    }
+    for (int i = threadIdx.x; i < QT_NODES; i += NT) S.nodes[i] = rec->nodes[i];
+    if (threadIdx.x == 0) { S.ncoef = 0; S.tu8mask = rec->tu8mask; }
+    SYNC();
+    QuantParams ql, qc;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        ql.eff[b] = P.eff_l[b]; ql.rcp[b] = P.rcp_l[b];
+        qc.eff[b] = P.eff_c[b]; qc.rcp[b] = P.rcp_c[b];
+    }
+    ql.lambda = 0; qc.lambda = 0;
+    qt_dec<0>(S, P, ctu_x, ctu_y, 0, 0, rec->coef, ql, qc);
+    SYNC();
+    if (w == 64 && h == 64) deblock_tile(S, P.qp);
+    if (rec->sao_has) {
+        const int band = clampi(rec->sao_band, 0, 31), off = clampi(rec->sao_offset, -7, 7);
+        for (int i = threadIdx.x; i < w * h; i += NT) {
+            const int y = i / w, x = i - y * w;
+            uint8_t &p = RY(S, x, y);
+            if ((p >> 3) == band) p = (uint8_t)clampi(p + off, 0, 255);
+        }
+        SYNC();
+    }
+    for (int i = threadIdx.x; i < w * h; i += NT) {
+        const int y = i / w, x = i - y * w;
+        P.rec_y[(size_t)(ctu_y + y) * P.stride_y + ctu_x + x] = RY(S, x, y);
+    }
+    for (int i = threadIdx.x; i < 2 * wc * hc; i += NT) {
+        const int c = i / (wc * hc), p = i - c * wc * hc, y = p / wc, x = p - y * wc;
+        uint8_t *dst = c ? P.rec_cr : P.rec_cb;
+        dst[(size_t)((ctu_y >> 1) + y) * P.stride_c + (ctu_x >> 1) + x] = RC(S, c, x, y);
+    }
+}
+
+cudaError_t init_decode_tables() {
+    return cudaFuncSetAttribute(decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(Smem));
+}
+
+cudaError_t launch_decode_items(const FrameParams *d_params, const int *d_items, int n,
+                                cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    decode_kernel<<<n, NT, sizeof(Smem), st>>>(d_params, d_items);
     return cudaGetLastError();
 }
 

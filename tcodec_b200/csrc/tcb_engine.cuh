@@ -47,6 +47,7 @@ struct Smem {
     MvCell snap_g[3][2][64];
     MvCell grid[64];
     Node nodes[QT_NODES];
+    long long node_cost[QT_NODES];
     uint8_t pred[NPRED][64 * 64];
     uint8_t cpred[4][32 * 32];
     uint8_t ra[2 * 64 + 4], rl[2 * 64 + 4];     // index i+1 holds ref[i], i in -1..2N
@@ -56,12 +57,14 @@ struct Smem {
     int acc_bits[NCAND][2];
     long long acc64[4];
     int cl[NCAND];             // candidate list for job loops
-    int cand_mvx[NPRED], cand_mvy[NPRED], cand_ref[NPRED];
+    int cl2[8];                // 8x8-only candidates (merges)
+    int cand_mvx[NPRED], cand_mvy[NPRED], cand_ref[NPRED], cand_ref2[NPRED];
     int ncl, dc, flag;
     long long best_cost;
     int sao[3];
     int band_sum[32], band_cnt[32], band_sq[32], band_new[32];
     int ncoef;
+    unsigned long long tu8mask;
 };
 
 }  // namespace tcb

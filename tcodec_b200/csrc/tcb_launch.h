@@ -11,6 +11,10 @@ cudaError_t init_device_tables();
 cudaError_t init_engine_tables();
 cudaError_t init_unit_tables();
 size_t ctu_smem_bytes();
+cudaError_t init_decode_tables();
+cudaError_t launch_decode_items(const FrameParams *d_params, const int *d_items, int n, cudaStream_t st);
+cudaError_t launch_ctu_persistent(const FrameParams *d_params, const int *d_items, int n, int *d_ctrl,
+                                  int grid, cudaStream_t st);
 cudaError_t launch_ctu_items(const FrameParams *d_params, const int *d_items, int n, cudaStream_t st);
 cudaError_t launch_glob_mv(const uint8_t *cur, const uint8_t *ref, int W, int H, int s,
                            FrameParams *d_params, cudaStream_t st);

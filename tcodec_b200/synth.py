@@ -13,6 +13,8 @@ distributions the benchmark configurations describe:
 * ``moving_rects_clip`` — the sinusoid background plus 16 axis-aligned
   rectangles (32..160 px sides) of uniform 0..255 noise texture, each with
   its own velocity drawn from [-6, 6]^2 px/frame.
+* ``with_lines`` — static 1-px high-contrast lines over 5% of the area
+  (screen-content-like detail that exercises the intra modes).
 
 Everything is deterministic in the seeds.
 """
@@ -25,9 +27,12 @@ import numpy as np
 Frame = Tuple[np.ndarray, np.ndarray, np.ndarray]
 
 
-def _texture(h: int, w: int, seed: int, n_waves: int = 8) -> np.ndarray:
+def _texture(h: int, w: int, seed: int, origin: int = 0, n_waves: int = 8) -> np.ndarray:
+    """Sinusoid field on an h x w canvas whose sample (origin, origin) is
+    texture coordinate (0, 0), so the visible window does not depend on the
+    canvas margin (and therefore not on the clip length)."""
     rng = np.random.default_rng(seed)
-    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64) - origin
     out = np.full((h, w), 128.0)
     for _ in range(n_waves):
         period = rng.uniform(8.0, 64.0)
@@ -92,9 +97,9 @@ def _render(width, height, frames, motion, sigma, seed_l, seed_c, seed_n, rects)
     vx, vy = motion
     span = int(np.ceil(max(abs(vx), abs(vy)) * frames)) + 4
     m = span
-    base_y = _texture(height + 2 * m, width + 2 * m, seed_l)
+    base_y = _texture(height + 2 * m, width + 2 * m, seed_l, origin=m)
     mc = span // 2 + 4
-    base_c = [_texture(height // 2 + 2 * mc, width // 2 + 2 * mc, seed_c * 1000 + k) for k in range(2)]
+    base_c = [_texture(height // 2 + 2 * mc, width // 2 + 2 * mc, seed_c * 1000 + k, origin=mc) for k in range(2)]
     noise = np.random.default_rng(seed_n)
     out: List[Frame] = []
     for t in range(frames):
@@ -118,6 +123,33 @@ def _render(width, height, frames, motion, sigma, seed_l, seed_c, seed_n, rects)
     return out
 
 
+def with_lines(frames: List[Frame], area_frac: float = 0.05, seed: int = 21) -> List[Frame]:
+    """Overlay static 1-px high-contrast horizontal / vertical lines covering
+    `area_frac` of the luma area (screen-content-like detail)."""
+    h, w = frames[0][0].shape
+    rng = np.random.default_rng(seed)
+    mask = np.zeros((h, w), bool)
+    val = np.zeros((h, w), np.uint8)
+    target = int(area_frac * h * w)
+    while mask.sum() < target:
+        length = int(rng.integers(16, max(17, min(w, h) // 2)))
+        v = 255 if rng.integers(0, 2) else 0
+        if rng.integers(0, 2):
+            y, x = int(rng.integers(0, h)), int(rng.integers(0, w - length))
+            mask[y, x:x + length] = True
+            val[y, x:x + length] = v
+        else:
+            y, x = int(rng.integers(0, h - length)), int(rng.integers(0, w))
+            mask[y:y + length, x] = True
+            val[y:y + length, x] = v
+    out = []
+    for (y, cb, cr) in frames:
+        y2 = y.copy()
+        y2[mask] = val[mask]
+        out.append((y2, cb, cr))
+    return out
+
+
 def workload(name: str, frames: int = None, width: int = None, height: int = None) -> List[Frame]:
     """Named workloads: 'cfg0' (320x240 sinusoid, motion (+1.25, -0.5),
     sigma 2) and 'cfg1' (1280x720 sinusoid + rectangles, motion
@@ -126,4 +158,7 @@ def workload(name: str, frames: int = None, width: int = None, height: int = Non
         return sinusoid_clip(width or 320, height or 240, frames or 30)
     if name == "cfg1":
         return moving_rects_clip(width or 1280, height or 720, frames or 60)
+    if name == "cfg2":
+        return with_lines(moving_rects_clip(width or 1920, height or 1080, frames or 120, motion=(2.5, 0.75),
+                                            noise_sigma=3.0))
     raise ValueError(name)
