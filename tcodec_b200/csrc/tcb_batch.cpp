@@ -124,7 +124,7 @@ tc_error_t run_step(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkt
         float ms = 0.f;
         cudaEventElapsedTime(&ms, b->ev0, b->ev1);
         b->ctu_ms += ms;
-        b->ctu_launches += b->max_diag;
+        b->ctu_launches += persistent ? 1 : b->max_diag;
         b->steps++;
         b->ctu_count += (long long)b->h_items.size();
     }

@@ -36,6 +36,18 @@ __constant__ int8_t c_qpel[9][2] = {{0, 0}, {1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1
 
 #define SYNC() __syncthreads()
 
+// Optional per-phase cycle counters (build with -DTCB_PHASE_PROFILE); thread
+// 0 of each CTA accumulates clock64() deltas into tcb_phase_cycles[].
+#ifdef TCB_PHASE_PROFILE
+__device__ unsigned long long tcb_phase_cycles[16];
+#define PHASE_T0() long long _ph_t = clock64()
+#define PHASE(k) do { if (threadIdx.x == 0) { const long long _n = clock64(); \
+    atomicAdd(&tcb_phase_cycles[k], (unsigned long long)(_n - _ph_t)); _ph_t = _n; } } while (0)
+#else
+#define PHASE_T0() do {} while (0)
+#define PHASE(k) do {} while (0)
+#endif
+
 __device__ __forceinline__ void group_bar(int g) {
     asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(GT) : "memory");
 }
@@ -748,10 +760,12 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
     const bool key = P.frame_type == 0;
     const bool is_p = P.frame_type == 1;
     const bool is_b = P.frame_type == 2;
+    PHASE_T0();
     int mvpx, mvpy;
     mvp_at(S.grid, L.cx, L.cy, mvpx, mvpy);
     build_refs(S, L);
     zero_acc(S);
+    PHASE(0);
 
     // ---- candidate set -------------------------------------------------
     bool has_glb = false, has_tmp = false, has_me1 = false;
@@ -784,6 +798,7 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
             me_run(S, 3, gt, P.ref_y[0], P.stride_y, P.W, P.H, L.lx, L.ly, cu,
                    (L.px * 4 + tdx) >> 2, (L.py * 4 + tdy) >> 2, sr);
         SYNC();
+        PHASE(1);
         if (has_glb && S.me[2].mvx == S.me[0].mvx && S.me[2].mvy == S.me[0].mvy) has_glb = false;
         if (has_tmp && S.me[3].mvx == S.me[0].mvx && S.me[3].mvy == S.me[0].mvy) has_tmp = false;
         int slots[5], ns = 0;
@@ -804,6 +819,7 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
         if (medium) n8only = 1;
         SYNC();
         luma_mc_slots(S, P, L, ns, slots);
+        PHASE(2);
     } else if (is_b) {
         // Forward / backward searches (reference src/encoder.c:795-852).
         const int sr = fast ? 16 : 32;
@@ -812,6 +828,7 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
         else if (g == 1 && rb >= 0)
             me_run(S, 1, gt, P.ref_y[rb], P.stride_y, P.W, P.H, L.lx, L.ly, cu, cx0, cy0, sr);
         SYNC();
+        PHASE(1);
         int slots[5], ns = 0;
         if (rf >= 0) slots[ns++] = K_B0 + 0;
         if (rb >= 0) slots[ns++] = K_B0 + 1;
@@ -836,6 +853,7 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
         n8only = (mrg && rf >= 0 && rb >= 0) + (mrg && rf >= 0) + (mrg && rb >= 0);
         SYNC();
         luma_mc_slots(S, P, L, ns, slots);
+        PHASE(2);
     }
 
     // ---- residual coding / SAD proxies for every candidate --------------
@@ -873,6 +891,7 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
         if (use4) luma_jobs4(S, L, S.cl, ncl, ql, true, false, nullptr);
         if (n8only) luma_jobs8(S, L, S.cl2, n8only, ql, true, false, nullptr);
         SYNC();
+        PHASE(3);
         if (is_p && medium) {
             // Skip pre-check (src/encoder.c:1064-1142): luma SSE of the merge
             // prediction, then fresh chroma SSE when the luma is exact.
@@ -905,6 +924,7 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
         }
     }
 
+    PHASE(4);
     // ---- in-order candidate scan (strict <, first minimum wins) ---------
     if (tid == 0) {
         const long long lam = P.lambda;
@@ -1027,6 +1047,7 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
     }
     SYNC();
 
+    PHASE(5);
     // ---- intra chroma choice: MC vs CfL-blended DC (src/encoder.c:1194-1221)
     const Node nd0 = S.nodes[qt_index(L.depth, L.cx, L.cy)];
     if (nd0.intra && !fast && medium) {
@@ -1053,8 +1074,10 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
         SYNC();
     }
     const long long best = S.best_cost;
+    PHASE(6);
     // ---- replay of the winner ------------------------------------------
     leaf_code(S, P, L, ql, qc, false, nullptr);
+    PHASE(7);
     return best;
 }
 
@@ -1325,7 +1348,9 @@ __device__ void encode_ctu(Smem &S, const FrameParams &P, int row, int col) {
     qc.lambda = P.lambda_c;
 
     // ---- decide, then write in syntax order ----------------------------
+    PHASE_T0();
     qt_decide<0>(S, P, ctu_x, ctu_y, 0, 0, ql, qc, false);
+    PHASE(8);
     for (int i = threadIdx.x; i < 64; i += NT) {
         S.grid[i].dx = 0; S.grid[i].dy = 0; S.grid[i].intra = 1;
     }
@@ -1333,9 +1358,11 @@ __device__ void encode_ctu(Smem &S, const FrameParams &P, int row, int col) {
     CtuOut *out = P.out + row * P.ctu_cols + col;
     qt_write<0>(S, P, ctu_x, ctu_y, 0, 0, ql, qc, out);
     SYNC();
+    PHASE(9);
     // ---- in-loop filters ------------------------------------------------
     if (w == 64 && h == 64) deblock_tile(S, P.qp);
     sao_tile(S, w, h, P.lambda_sao);
+    PHASE(10);
     // ---- exports --------------------------------------------------------
     for (int i = threadIdx.x; i < w * h; i += NT) {
         const int y = i / w, x = i - y * w;
@@ -1747,3 +1774,13 @@ cudaError_t launch_decode_items(const FrameParams *d_params, const int *d_items,
 }
 
 }  // namespace tcb
+
+#ifdef TCB_PHASE_PROFILE
+// Profiling builds only: read and reset the phase cycle counters.
+extern "C" __attribute__((visibility("default"))) int tcb_debug_phase_cycles(unsigned long long *out16) {
+    cudaDeviceSynchronize();
+    if (cudaMemcpyFromSymbol(out16, tcb::tcb_phase_cycles, 16 * sizeof(unsigned long long)) != cudaSuccess) return -1;
+    unsigned long long z[16] = {0};
+    return cudaMemcpyToSymbol(tcb::tcb_phase_cycles, z, sizeof(z)) == cudaSuccess ? 0 : -1;
+}
+#endif
