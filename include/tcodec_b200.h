@@ -79,6 +79,45 @@ void tcb_batch_set_timing(tcb_batch_t *batch, int enabled);
 void tcb_batch_get_timing(tcb_batch_t *batch, double *ctu_ms, int64_t *ctu_launches, int64_t *ctu_count,
                           int64_t *steps, int64_t *kernel_launches);
 
+/* ---------------------------------------------------------------------
+ * Part 2: standalone kernels.
+ * ------------------------------------------------------------------- */
+
+/* One frame for the CTU engine.  Every pointer is a device pointer; all
+ * planes share stride_y / stride_c.  ref_*[i] == NULL marks an empty DPB
+ * slot.  prev_mv_grid / cur_mv_grid hold ceil(W/8)*ceil(H/8) cells of
+ * tcb_mv_cell_bytes() each (prev may be NULL); ctu_records holds
+ * ceil(W/64)*ceil(H/64) records of tcb_ctu_record_bytes() each: the
+ * decision tree, quantised coefficients in syntax order and SAO
+ * parameters of every CTU, ready for the v2 syntax writer. */
+typedef struct tcb_frame_desc {
+    int width, height, stride_y, stride_c;
+    const tc_pixel_t *src_y, *src_cb, *src_cr;
+    tc_pixel_t *rec_y, *rec_cb, *rec_cr;
+    const tc_pixel_t *ref_y[TC_REF_FRAMES], *ref_cb[TC_REF_FRAMES], *ref_cr[TC_REF_FRAMES];
+    int ref_poc[TC_REF_FRAMES];
+    const void *prev_mv_grid;
+    void *cur_mv_grid;
+    void *ctu_records;
+    int frame_type;        /* 0 key, 1 P, 2 B */
+    int poc, qp, preset, profile;
+    int global_mv_valid, global_mv_x, global_mv_y;   /* encoder-only hint, quarter-pel */
+} tcb_frame_desc_t;
+
+size_t tcb_ctu_record_bytes(void);
+size_t tcb_mv_cell_bytes(void);
+/* Device scratch tcb_ctu_encode_frame needs for a width x height frame. */
+size_t tcb_ctu_scratch_bytes(int width, int height);
+
+/* Encode every CTU of one frame (decide, write pass, deblocking, SAO) as a
+ * persistent wavefront kernel: replaces the per-CTU loop of the reference
+ * frame encoder, src/encoder.c:2939-2946 calling encode_ctu_v2
+ * (src/encoder.c:1399-1522).  `scratch` is device memory of at least
+ * tcb_ctu_scratch_bytes(width, height) bytes (queue, publish flags,
+ * frame parameters); it may be reused once the call's work has finished. */
+tc_error_t tcb_ctu_encode_frame(const tcb_frame_desc_t *desc, void *scratch, size_t scratch_bytes,
+                                void *stream);
+
 #ifdef __cplusplus
 }
 #endif

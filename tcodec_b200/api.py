@@ -269,6 +269,25 @@ class Decoder:
         return self.lib.tc_decoder_crc_valid(self.h)
 
 
+REF_FRAMES = 4
+
+
+class FrameDesc(ctypes.Structure):
+    """tcb_frame_desc_t: one frame for the CTU engine (device pointers)."""
+    _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int),
+                ("stride_y", ctypes.c_int), ("stride_c", ctypes.c_int),
+                ("src_y", ctypes.c_void_p), ("src_cb", ctypes.c_void_p), ("src_cr", ctypes.c_void_p),
+                ("rec_y", ctypes.c_void_p), ("rec_cb", ctypes.c_void_p), ("rec_cr", ctypes.c_void_p),
+                ("ref_y", ctypes.c_void_p * REF_FRAMES), ("ref_cb", ctypes.c_void_p * REF_FRAMES),
+                ("ref_cr", ctypes.c_void_p * REF_FRAMES), ("ref_poc", ctypes.c_int * REF_FRAMES),
+                ("prev_mv_grid", ctypes.c_void_p), ("cur_mv_grid", ctypes.c_void_p),
+                ("ctu_records", ctypes.c_void_p),
+                ("frame_type", ctypes.c_int), ("poc", ctypes.c_int), ("qp", ctypes.c_int),
+                ("preset", ctypes.c_int), ("profile", ctypes.c_int),
+                ("global_mv_valid", ctypes.c_int), ("global_mv_x", ctypes.c_int),
+                ("global_mv_y", ctypes.c_int)]
+
+
 def bind_b200(lib: ctypes.CDLL) -> ctypes.CDLL:
     """Attach argtypes of the include/tcodec_b200.h encoder extensions."""
     vp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)
@@ -293,6 +312,12 @@ def bind_b200(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.tcb_batch_flush.restype = ctypes.c_int
     lib.tcb_batch_set_timing.argtypes = [vp, ctypes.c_int]
     lib.tcb_batch_get_timing.argtypes = [vp] + [vp] * 5
+    lib.tcb_ctu_record_bytes.restype = ctypes.c_size_t
+    lib.tcb_mv_cell_bytes.restype = ctypes.c_size_t
+    lib.tcb_ctu_scratch_bytes.argtypes = [ctypes.c_int, ctypes.c_int]
+    lib.tcb_ctu_scratch_bytes.restype = ctypes.c_size_t
+    lib.tcb_ctu_encode_frame.argtypes = [ctypes.POINTER(FrameDesc), vp, ctypes.c_size_t, vp]
+    lib.tcb_ctu_encode_frame.restype = ctypes.c_int
     return lib
 
 

@@ -15,13 +15,14 @@
 #include <cuda_runtime.h>
 
 #include "../../include/tcodec_b200.h"
+#include "tcb_batch.h"
 #include "tcb_encoder.h"
 #include "tcb_launch.h"
 
 using namespace tcb;
 
 struct tcb_batch {
-    std::vector<tc_encoder_t *> encs;
+    std::vector<tc_encoder_t *> encs;        // slot -> stream (NULL: free slot)
     cudaStream_t st = nullptr;
     FrameParams *d_params = nullptr;         // [n] contiguous for the kernel
     int *d_items = nullptr;
@@ -44,7 +45,7 @@ void release(tcb_batch *b) {
     if (b->st) cudaStreamSynchronize(b->st);
     for (tc_encoder_t *e : b->encs) {
         if (e && e->impl) e->impl->st = e->impl->own_st;
-        tc_encoder_destroy(e);
+        if (e) tc_encoder_destroy(e);
     }
     cudaFree(b->d_params);
     cudaFree(b->d_items);
@@ -146,34 +147,81 @@ tc_error_t run_step(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkt
 
 }  // namespace
 
-extern "C" {
-
-tcb_batch_t *tcb_batch_create(const tc_config_t *configs, int n) {
-    if (!configs || n <= 0 || n > MAX_STREAMS) return nullptr;
+tcb_batch *tcb::batch_new(int cap) {
+    if (cap <= 0 || cap > MAX_STREAMS) return nullptr;
     tcb_batch *b = new (std::nothrow) tcb_batch();
     if (!b) return nullptr;
     if (cudaGetDevice(&b->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
-        cudaMalloc(&b->d_params, sizeof(FrameParams) * n) != cudaSuccess ||
+        cudaMalloc(&b->d_params, sizeof(FrameParams) * cap) != cudaSuccess ||
         cudaMalloc(&b->d_ctrl, 2 * sizeof(int)) != cudaSuccess ||
         cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess) {
         release(b);
         return nullptr;
     }
+    b->encs.assign(cap, nullptr);
+    b->stream_diag.assign(cap, {});
+    return b;
+}
+
+int tcb::batch_attach(tcb_batch *b, tc_encoder_t *e) {
+    int s = 0;
+    while (s < (int)b->encs.size() && b->encs[s]) ++s;
+    if (s == (int)b->encs.size()) return -1;
+    b->encs[s] = e;
+    EncImpl &im = *e->impl;
+    im.st = b->st;                          // all device work on the batch stream
+    std::vector<std::vector<int>> diags(im.diag_off.size());
+    for (int d = 0; d < (int)im.diag_off.size(); ++d)
+        for (int r = 0; r < im.ctu_rows; ++r) {
+            const int c = d - r;
+            if (c >= 0 && c < im.ctu_cols) diags[d].push_back((s << 20) | (r << 10) | c);
+        }
+    b->stream_diag[s] = std::move(diags);
+    b->max_diag = 0;
+    for (auto &sd : b->stream_diag) b->max_diag = std::max(b->max_diag, (int)sd.size());
+    return s;
+}
+
+void tcb::batch_detach(tcb_batch *b, int s) {
+    if (s < 0 || s >= (int)b->encs.size() || !b->encs[s]) return;
+    cudaStreamSynchronize(b->st);
+    tc_encoder_t *e = b->encs[s];
+    e->impl->st = e->impl->own_st;
+    tc_encoder_destroy(e);
+    b->encs[s] = nullptr;
+    b->stream_diag[s].clear();
+    b->max_diag = 0;
+    for (auto &sd : b->stream_diag) b->max_diag = std::max(b->max_diag, (int)sd.size());
+}
+
+tc_encoder_t *tcb::batch_slot(tcb_batch *b, int s) {
+    return (s >= 0 && s < (int)b->encs.size()) ? b->encs[s] : nullptr;
+}
+
+cudaStream_t tcb::batch_stream(tcb_batch *b) { return b->st; }
+
+tc_error_t tcb::batch_run(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkts, int *status) {
+    if (part.empty()) return TC_OK;
+    if (cudaSetDevice(b->device) != cudaSuccess) return TC_ERR_INTERNAL;
+    return run_step(b, part, pkts, status);
+}
+
+void tcb::batch_free(tcb_batch *b) { if (b) release(b); }
+
+extern "C" {
+
+tcb_batch_t *tcb_batch_create(const tc_config_t *configs, int n) {
+    if (!configs || n <= 0 || n > MAX_STREAMS) return nullptr;
+    tcb_batch *b = batch_new(n);
+    if (!b) return nullptr;
     for (int s = 0; s < n; ++s) {
         tc_encoder_t *e = tc_encoder_create(&configs[s]);
-        if (!e) { release(b); return nullptr; }
-        b->encs.push_back(e);
-        EncImpl &im = *e->impl;
-        im.st = b->st;                      // all device work on the batch stream
-        std::vector<std::vector<int>> diags(im.diag_off.size());
-        for (int d = 0; d < (int)im.diag_off.size(); ++d)
-            for (int r = 0; r < im.ctu_rows; ++r) {
-                const int c = d - r;
-                if (c >= 0 && c < im.ctu_cols) diags[d].push_back((s << 20) | (r << 10) | c);
-            }
-        b->max_diag = std::max(b->max_diag, (int)diags.size());
-        b->stream_diag.push_back(std::move(diags));
+        if (!e || batch_attach(b, e) != s) {
+            if (e) tc_encoder_destroy(e);
+            release(b);
+            return nullptr;
+        }
     }
     return b;
 }

@@ -90,6 +90,22 @@ void EncImpl::rc_frame_end(long long bits) {
 
 #define CK(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { last_cuda_error = _e; return false; } } while (0)
 
+size_t EncImpl::device_footprint(const tc_config_t &c) {
+    const int W = c.width, H = c.height;
+    const size_t sy = ((W + 63) / 64) * 64, sc = ((W / 2 + 63) / 64) * 64;
+    const size_t nctu = (size_t)((W + 63) / 64) * ((H + 63) / 64);
+    const size_t cells = (size_t)((W + 7) / 8) * ((H + 7) / 8);
+    auto R = DeviceArena::round_up;
+    const size_t frame = R(sy * H + 64) + 2 * R(sc * (H / 2) + 64);
+    size_t n = (NPOOL + 1) * frame;                       // DPB pool + input
+    n += 2 * R(sizeof(MvCell) * cells);                   // MV grids
+    n += R(sizeof(CtuOut) * nctu);                        // decision records
+    n += R(sizeof(FrameParams)) + R(16 * sizeof(int)) + R(sizeof(unsigned long long)) + R(sizeof(int));
+    n += R(sizeof(int) * nctu) + R(2 * sizeof(int)) + R(sizeof(int) * nctu);   // flags, ctrl, queue
+    if (c.enable_b_frames) n += BF_MAX * frame;           // reorder buffers at their cap
+    return n;
+}
+
 bool EncImpl::init(const tc_config_t &c) {
     cfg = c;
     W = c.width; H = c.height;
@@ -109,38 +125,38 @@ bool EncImpl::init(const tc_config_t &c) {
     CK(cudaEventCreate(&ev1));
     const size_t ybytes = (size_t)sy * H + 64, cbytes = (size_t)sc * (H / 2) + 64;
     for (int i = 0; i < NPOOL; ++i) {
-        CK(cudaMalloc(&pool[i].y, ybytes));
-        CK(cudaMalloc(&pool[i].cb, cbytes));
-        CK(cudaMalloc(&pool[i].cr, cbytes));
+        CK(dmalloc(&pool[i].y, ybytes));
+        CK(dmalloc(&pool[i].cb, cbytes));
+        CK(dmalloc(&pool[i].cr, cbytes));
         CK(cudaMemset(pool[i].y, 0, ybytes));
         CK(cudaMemset(pool[i].cb, 0, cbytes));
         CK(cudaMemset(pool[i].cr, 0, cbytes));
     }
-    CK(cudaMalloc(&cur.y, ybytes));
-    CK(cudaMalloc(&cur.cb, cbytes));
-    CK(cudaMalloc(&cur.cr, cbytes));
+    CK(dmalloc(&cur.y, ybytes));
+    CK(dmalloc(&cur.cb, cbytes));
+    CK(dmalloc(&cur.cr, cbytes));
     CK(cudaMemset(cur.y, 0, ybytes));
     CK(cudaMemset(cur.cb, 0, cbytes));
     CK(cudaMemset(cur.cr, 0, cbytes));
     for (int i = 0; i < 2; ++i) {
-        CK(cudaMalloc(&grid[i], sizeof(MvCell) * grid_w * grid_h));
+        CK(dmalloc(&grid[i], sizeof(MvCell) * grid_w * grid_h));
         std::vector<MvCell> init(grid_w * grid_h);
         for (auto &g : init) { g.dx = 0; g.dy = 0; g.intra = 1; g.pad = 0; }
         CK(cudaMemcpy(grid[i], init.data(), sizeof(MvCell) * init.size(), cudaMemcpyHostToDevice));
     }
     const int nctu = ctu_cols * ctu_rows;
-    CK(cudaMalloc(&d_out, sizeof(CtuOut) * nctu));
+    CK(dmalloc(&d_out, sizeof(CtuOut) * nctu));
     CK(cudaMallocHost(&h_out, sizeof(CtuOut) * nctu));
-    CK(cudaMalloc(&d_params, sizeof(FrameParams)));
-    CK(cudaMalloc(&d_hist, 16 * sizeof(int)));
+    CK(dmalloc(&d_params, sizeof(FrameParams)));
+    CK(dmalloc(&d_hist, 16 * sizeof(int)));
     CK(cudaMallocHost(&h_hist, 16 * sizeof(int)));
-    CK(cudaMalloc(&d_sse, sizeof(unsigned long long)));
+    CK(dmalloc(&d_sse, sizeof(unsigned long long)));
     CK(cudaMallocHost(&h_sse, sizeof(unsigned long long)));
-    CK(cudaMalloc(&d_err, sizeof(int)));
+    CK(dmalloc(&d_err, sizeof(int)));
     CK(cudaMemset(d_err, 0, sizeof(int)));
-    CK(cudaMalloc(&d_done, sizeof(int) * ctu_cols * ctu_rows));
+    CK(dmalloc(&d_done, sizeof(int) * ctu_cols * ctu_rows));
     CK(cudaMemset(d_done, 0, sizeof(int) * ctu_cols * ctu_rows));
-    CK(cudaMalloc(&d_ctrl, 2 * sizeof(int)));
+    CK(dmalloc(&d_ctrl, 2 * sizeof(int)));
     CK(cudaMallocHost(&h_ctrl, 2 * sizeof(int)));
     CK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
     {
@@ -157,7 +173,7 @@ bool EncImpl::init(const tc_config_t &c) {
         }
         diag_cnt.push_back((int)items.size() - diag_off.back());
     }
-    CK(cudaMalloc(&d_items, sizeof(int) * items.size()));
+    CK(dmalloc(&d_items, sizeof(int) * items.size()));
     CK(cudaMemcpy(d_items, items.data(), sizeof(int) * items.size(), cudaMemcpyHostToDevice));
     for (int i = 0; i < TC_REF_FRAMES; ++i) { dpb_slot[i] = -1; dpb_poc[i] = -1; }
     out_buf_size = (size_t)W * H * 3;
@@ -171,14 +187,14 @@ bool EncImpl::init(const tc_config_t &c) {
 void EncImpl::release() {
     if (st) cudaStreamSynchronize(st);
     if (own_st) cudaStreamSynchronize(own_st);
-    for (int i = 0; i < NPOOL; ++i) { cudaFree(pool[i].y); cudaFree(pool[i].cb); cudaFree(pool[i].cr); }
-    cudaFree(cur.y); cudaFree(cur.cb); cudaFree(cur.cr);
-    cudaFree(grid[0]); cudaFree(grid[1]);
-    cudaFree(d_out); cudaFreeHost(h_out);
-    cudaFree(d_params); cudaFree(d_hist); cudaFreeHost(h_hist);
-    cudaFree(d_sse); cudaFreeHost(h_sse); cudaFree(d_err); cudaFree(d_items);
-    cudaFree(d_done); cudaFree(d_ctrl); cudaFreeHost(h_ctrl);
-    for (auto &f : bf_frames) { cudaFree(f.y); cudaFree(f.cb); cudaFree(f.cr); }
+    for (int i = 0; i < NPOOL; ++i) { dfree(pool[i].y); dfree(pool[i].cb); dfree(pool[i].cr); }
+    dfree(cur.y); dfree(cur.cb); dfree(cur.cr);
+    dfree(grid[0]); dfree(grid[1]);
+    dfree(d_out); cudaFreeHost(h_out);
+    dfree(d_params); dfree(d_hist); cudaFreeHost(h_hist);
+    dfree(d_sse); cudaFreeHost(h_sse); dfree(d_err); dfree(d_items);
+    dfree(d_done); dfree(d_ctrl); cudaFreeHost(h_ctrl);
+    for (auto &f : bf_frames) { dfree(f.y); dfree(f.cb); dfree(f.cr); }
     bf_frames.clear();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -496,7 +512,7 @@ tc_error_t EncImpl::stage_d(tc_packet_t *pkt) {
     prev_mv_valid = 1;
     if (pend.bf_idx >= 0) {
         DevFrame &f = bf_frames[pend.bf_idx];
-        cudaFree(f.y); cudaFree(f.cb); cudaFree(f.cr);
+        dfree(f.y); dfree(f.cb); dfree(f.cr);
         bf_frames.erase(bf_frames.begin() + pend.bf_idx);
         bf_pocs.erase(bf_pocs.begin() + pend.bf_idx);
         pend.bf_idx = -1;
@@ -521,6 +537,56 @@ tc_error_t EncImpl::encode_planned(tc_packet_t *pkt) {
         frames_timed++;
     }
     return stage_d(pkt);
+}
+
+// Frame parameters of the CTU engine from the public frame descriptor
+// (same derivations as stage_b: multiref / fresh-skip tool conditions,
+// keyframe lambda scaling, per-band quant steps).
+bool tcb::frame_params_from_desc(const tcb_frame_desc_t &d, FrameParams &P) {
+    if (d.width <= 0 || d.height <= 0 || (d.width & 1) || (d.height & 1) || d.width > TC_MAX_WIDTH ||
+        d.height > TC_MAX_HEIGHT || d.stride_y < d.width || d.stride_c < d.width / 2 || !d.src_y || !d.src_cb ||
+        !d.src_cr || !d.rec_y || !d.rec_cb || !d.rec_cr || !d.cur_mv_grid || !d.ctu_records ||
+        d.frame_type < 0 || d.frame_type > 2 || d.qp < 0 || d.qp > 63 || d.preset < 0 || d.preset > 3)
+        return false;
+    memset(&P, 0, sizeof(P));
+    P.W = d.width; P.H = d.height; P.stride_y = d.stride_y; P.stride_c = d.stride_c;
+    P.ctu_cols = (d.width + 63) / 64; P.ctu_rows = (d.height + 63) / 64;
+    P.grid_w = (d.width + 7) / 8; P.grid_h = (d.height + 7) / 8;
+    P.cur_y = d.src_y; P.cur_cb = d.src_cb; P.cur_cr = d.src_cr;
+    P.rec_y = d.rec_y; P.rec_cb = d.rec_cb; P.rec_cr = d.rec_cr;
+    for (int i = 0; i < MAX_REFS; ++i) {
+        const bool ok = d.ref_y[i] && d.ref_cb[i] && d.ref_cr[i];
+        P.ref_valid[i] = ok;
+        P.ref_poc[i] = ok ? d.ref_poc[i] : -1;
+        P.ref_y[i] = ok ? d.ref_y[i] : d.src_y;
+        P.ref_cb[i] = ok ? d.ref_cb[i] : d.src_cb;
+        P.ref_cr[i] = ok ? d.ref_cr[i] : d.src_cr;
+    }
+    P.prev_valid = d.prev_mv_grid != nullptr;
+    P.prev_grid = (const MvCell *)(d.prev_mv_grid ? d.prev_mv_grid : d.cur_mv_grid);
+    P.cur_grid = (MvCell *)d.cur_mv_grid;
+    P.out = (CtuOut *)d.ctu_records;
+    P.frame_type = d.frame_type;
+    P.poc = d.poc;
+    P.qp = d.qp;
+    P.qp_c = clampi(d.qp + 1, 0, 63);
+    P.preset = d.preset;
+    const int profile = d.profile > TC_PROFILE_MAX ? TC_PROFILE_BASELINE_MOBILE : d.profile;
+    P.multiref = d.preset >= TC_PRESET_MEDIUM && profile >= TC_PROFILE_STREAMING_MAIN && d.frame_type == 1;
+    P.fresh_skip = d.preset >= TC_PRESET_MEDIUM;
+    P.glob_valid = d.global_mv_valid ? 1 : 0;
+    P.glob_x = d.global_mv_x;
+    P.glob_y = d.global_mv_y;
+    long long lam = tc_lambda_host(d.qp);
+    if (d.frame_type == 0) lam = (lam * 3) / 4;
+    P.lambda = lam;
+    P.lambda_c = tc_lambda_host(P.qp_c);
+    P.lambda_sao = tc_lambda_host(d.qp);
+    for (int b = 0; b < 4; ++b) {
+        P.eff_l[b] = eff_scale(d.qp, b); P.rcp_l[b] = quant_rcp(P.eff_l[b]);
+        P.eff_c[b] = eff_scale(P.qp_c, b); P.rcp_c[b] = quant_rcp(P.eff_c[b]);
+    }
+    return true;
 }
 
 long long tcb::tc_lambda_host(int qp) {
@@ -565,11 +631,11 @@ bool EncImpl::bf_can_emit() const {
     return bf_emit_pos > bf_anchor_slot(p);
 }
 tc_error_t EncImpl::bf_push_current() {
-    if (bf_pocs.size() >= 8) return TC_OK;
+    if (bf_pocs.size() >= BF_MAX) return TC_OK;
     DevFrame f;
     const size_t ybytes = (size_t)sy * H + 64, cbytes = (size_t)sc * (H / 2) + 64;
-    if (cudaMalloc(&f.y, ybytes) != cudaSuccess || cudaMalloc(&f.cb, cbytes) != cudaSuccess ||
-        cudaMalloc(&f.cr, cbytes) != cudaSuccess)
+    if (dmalloc(&f.y, ybytes) != cudaSuccess || dmalloc(&f.cb, cbytes) != cudaSuccess ||
+        dmalloc(&f.cr, cbytes) != cudaSuccess)
         return TC_ERR_MEMORY;
     if (!dcopy(f, cur)) return TC_ERR_INTERNAL;
     bf_frames.push_back(f);
@@ -635,9 +701,7 @@ tc_error_t EncImpl::encode_input(tc_packet_t *out) {
 // ---------------------------------------------------------------------------
 // Public API
 // ---------------------------------------------------------------------------
-extern "C" {
-
-tc_encoder_t *tc_encoder_create(const tc_config_t *config) {
+tc_encoder_t *tcb::encoder_create(const tc_config_t *config, DeviceArena *arena) {
     if (!config) return nullptr;
     if (!config->use_v2) return nullptr;   // this library implements the v2 bitstream
     if (config->width <= 0 || config->height <= 0 || (config->width & 1) || (config->height & 1) ||
@@ -647,6 +711,7 @@ tc_encoder_t *tc_encoder_create(const tc_config_t *config) {
     if (!enc) return nullptr;
     enc->cfg = *config;
     enc->impl = new (std::nothrow) EncImpl();
+    if (enc->impl) enc->impl->arena = arena;
     if (!enc->impl || !enc->impl->init(*config)) {
         tc_encoder_destroy(enc);
         return nullptr;
@@ -657,6 +722,10 @@ tc_encoder_t *tc_encoder_create(const tc_config_t *config) {
     enc->impl->recon_host = enc->recon;
     return enc;
 }
+
+extern "C" {
+
+tc_encoder_t *tc_encoder_create(const tc_config_t *config) { return tcb::encoder_create(config, nullptr); }
 
 void tc_encoder_destroy(tc_encoder_t *enc) {
     if (!enc) return;

@@ -9,8 +9,12 @@
 #include <cuda_runtime.h>
 
 #include "../../include/tcodec.h"
+#include "../../include/tcodec_b200.h"
+#include "tcb_arena.h"
 #include "tcb_common.cuh"
 #include "tcb_entropy.h"
+
+struct tc_encoder;
 
 namespace tcb {
 
@@ -19,9 +23,11 @@ struct DevFrame {
 };
 
 long long tc_lambda_host(int qp);
+bool frame_params_from_desc(const tcb_frame_desc_t &d, FrameParams &P);
 
 struct EncImpl {
     static constexpr int NPOOL = 6;   // 4 DPB slots + the frame being built + spare
+    static constexpr size_t BF_MAX = 8;   // B-frame reorder buffers held at most
     tc_config_t cfg{};
     int W = 0, H = 0, sy = 0, sc = 0, ctu_cols = 0, ctu_rows = 0, grid_w = 0, grid_h = 0;
     int device = 0;
@@ -72,6 +78,22 @@ struct EncImpl {
     std::vector<DevFrame> bf_frames;
     std::vector<int> bf_pocs;
 
+    // Device memory comes from `arena` when set (served sessions), else
+    // from cudaMalloc.
+    DeviceArena *arena = nullptr;
+    template <typename T> cudaError_t dmalloc(T **p, size_t n) {
+        if (!arena) return cudaMalloc((void **)p, n);
+        *p = (T *)arena->alloc(n);
+        return *p ? cudaSuccess : cudaErrorMemoryAllocation;
+    }
+    void dfree(void *p) {
+        if (!p) return;
+        if (arena && arena->owns(p)) arena->release(p);
+        else cudaFree(p);
+    }
+    // Device bytes a stream of configuration c holds at most (arena
+    // granules; B-frame reorder buffers at their cap included).
+    static size_t device_footprint(const tc_config_t &c);
     bool init(const tc_config_t &c);
     void release();
     int free_pool_slot() const;
@@ -102,6 +124,10 @@ struct EncImpl {
     bool bf_can_emit() const;
     tc_error_t bf_push_current();
 };
+
+// tc_encoder_create with the device memory taken from `arena` (NULL:
+// cudaMalloc).
+tc_encoder_t *encoder_create(const tc_config_t *config, DeviceArena *arena);
 
 }  // namespace tcb
 

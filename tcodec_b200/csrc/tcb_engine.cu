@@ -22,9 +22,12 @@
 // CTUs of one frame run as an anti-diagonal wavefront: CTU (r, c) reads the
 // filtered reconstruction of (r, c-1), (r-1, c) and (r-1, c-1) only, so all
 // CTUs with the same r + c are independent and go in one launch.
+#include <mutex>
+
 #include "tcb_engine.cuh"
 #include "tcb_pixel.cuh"
 #include "tcb_launch.h"
+#include "tcb_encoder.h"
 
 namespace tcb {
 
@@ -52,11 +55,15 @@ __device__ __forceinline__ void group_bar(int g) {
     asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(GT) : "memory");
 }
 
+// Four bytes from any address.  Reads only the aligned words that hold
+// p[0..3], so a plane whose last row ends exactly at the end of its
+// allocation (no padding) is never read past.
 __device__ __forceinline__ uint32_t ld4u(const uint8_t *p) {
     const uintptr_t a = (uintptr_t)p;
     const uint32_t *w = (const uint32_t *)(a & ~(uintptr_t)3);
-    const uint32_t lo = __ldg(w), hi = __ldg(w + 1);
-    return __funnelshift_r(lo, hi, (uint32_t)(a & 3) * 8);
+    const uint32_t lo = __ldg(w);
+    if ((a & 3) == 0) return lo;
+    return __funnelshift_r(lo, __ldg(w + 1), (uint32_t)(a & 3) * 8);
 }
 
 __device__ __forceinline__ uint8_t &RY(Smem &S, int x, int y) {
@@ -1462,6 +1469,70 @@ cudaError_t init_engine_tables() {
                                 (int)sizeof(Smem));
 }
 
+// Layout of the CTU-engine scratch used by tcb_ctu_encode_frame: frame
+// parameters, queue counter + error word, per-CTU publish flags, queue.
+constexpr size_t SCR_PARAMS = 0, SCR_CTRL = 1024, SCR_DONE = 1280;
+constexpr int MAX_DEVICES = 64;
+inline size_t scratch_bytes_for(int nctu) { return SCR_DONE + 8 * (size_t)nctu; }
+
+static_assert(sizeof(FrameParams) <= SCR_CTRL, "frame parameters overflow their scratch slot");
+
+// Writes the frame parameters into the scratch, clears the queue counter,
+// error word and publish flags, and lays out the queue in wavefront order:
+// anti-diagonal d = r + c ascending, rows ascending within a diagonal, so
+// every CTU's left / above / above-right neighbours are dequeued before it.
+__global__ void frame_setup_kernel(FrameParams P, uint8_t *__restrict__ scratch) {
+    const int nctu = P.ctu_cols * P.ctu_rows;
+    int *ctrl = (int *)(scratch + SCR_CTRL), *done = (int *)(scratch + SCR_DONE), *items = done + nctu;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0) {
+        *(FrameParams *)(scratch + SCR_PARAMS) = P;
+        ctrl[0] = 0;
+        ctrl[1] = 0;
+    }
+    if (t >= nctu) return;
+    done[t] = 0;
+    const int r = t / P.ctu_cols, c = t - r * P.ctu_cols, d = r + c;
+    int pos = 0;
+    for (int dd = 0; dd < d; ++dd) pos += min(dd, P.ctu_rows - 1) - max(0, dd - (P.ctu_cols - 1)) + 1;
+    items[pos + r - max(0, d - (P.ctu_cols - 1))] = (r << 10) | c;
+}
+
+// Shared host half of the frame entry points: one set-up launch fills
+// `scratch`, one persistent launch drains its queue.  Nothing is allocated
+// and nothing is copied from host memory.
+cudaError_t encode_frame_with_scratch(const FrameParams &P0, uint8_t *scratch, cudaStream_t st) {
+    FrameParams P = P0;
+    const int nctu = P.ctu_cols * P.ctu_rows;
+    int *ctrl = (int *)(scratch + SCR_CTRL), *done = (int *)(scratch + SCR_DONE), *items = done + nctu;
+    P.done = done;
+    P.epoch = 1;
+    P.err = ctrl + 1;
+    frame_setup_kernel<<<(nctu + 255) / 256, 256, 0, st>>>(P, scratch);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    return launch_ctu_persistent((const FrameParams *)(scratch + SCR_PARAMS), items, nctu, ctrl, sms, st);
+}
+
+// Constant tables and kernel attributes, once per device.
+cudaError_t ensure_device_tables() {
+    static std::mutex mu;
+    static bool ready[MAX_DEVICES] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!ready[dev]) {
+        if ((e = init_device_tables()) != cudaSuccess) return e;
+        ready[dev] = true;
+    }
+    return cudaSuccess;
+}
+
 cudaError_t launch_ctu_persistent(const FrameParams *d_params, const int *d_items, int n, int *d_ctrl,
                                   int grid, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
@@ -1479,6 +1550,26 @@ cudaError_t launch_ctu_items(const FrameParams *d_params, const int *d_items, in
 }
 
 }  // namespace tcb
+
+extern "C" {
+
+size_t tcb_ctu_record_bytes(void) { return sizeof(tcb::CtuOut); }
+size_t tcb_mv_cell_bytes(void) { return sizeof(tcb::MvCell); }
+size_t tcb_ctu_scratch_bytes(int width, int height) {
+    if (width <= 0 || height <= 0) return 0;
+    return tcb::scratch_bytes_for(((width + 63) / 64) * ((height + 63) / 64));
+}
+
+tc_error_t tcb_ctu_encode_frame(const tcb_frame_desc_t *desc, void *scratch, size_t scratch_bytes, void *stream) {
+    tcb::FrameParams P;
+    if (!desc || !scratch || !tcb::frame_params_from_desc(*desc, P)) return TC_ERR_PARAM;
+    if (scratch_bytes < tcb::scratch_bytes_for(P.ctu_cols * P.ctu_rows)) return TC_ERR_PARAM;
+    if (tcb::ensure_device_tables() != cudaSuccess) return TC_ERR_INTERNAL;
+    return tcb::encode_frame_with_scratch(P, (uint8_t *)scratch, (cudaStream_t)stream) == cudaSuccess
+               ? TC_OK : TC_ERR_INTERNAL;
+}
+
+}  // extern "C"
 
 // ====================================================================
 // Decoder reconstruction (reference src/decoder.c:1521-1816): the same

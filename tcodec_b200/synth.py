@@ -162,3 +162,51 @@ def workload(name: str, frames: int = None, width: int = None, height: int = Non
         return with_lines(moving_rects_clip(width or 1920, height or 1080, frames or 120, motion=(2.5, 0.75),
                                             noise_sigma=3.0))
     raise ValueError(name)
+
+
+# ---------------------------------------------------------------------------
+# Mixed-resolution stream sets (the batched and served workloads)
+# ---------------------------------------------------------------------------
+MIX_RESOLUTIONS = ((320, 240), (640, 360), (1280, 720), (1920, 1080))
+MIX_QPS = (22, 27, 32, 37)
+
+
+def mixed_streams(n: int = 64, frames: int = 32, seed: int = 7, stream_seed0: int = 1000):
+    """Specs of `n` independent streams: resolution and QP drawn uniformly
+    from MIX_RESOLUTIONS / MIX_QPS with `seed`; stream i renders the
+    moving-rectangles generator from its own seed stream_seed0 + i.
+    Returns a list of dicts {w, h, qp, seed, frames}."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        w, h = MIX_RESOLUTIONS[int(rng.integers(0, len(MIX_RESOLUTIONS)))]
+        qp = MIX_QPS[int(rng.integers(0, len(MIX_QPS)))]
+        out.append(dict(w=w, h=h, qp=qp, seed=stream_seed0 + i, frames=frames))
+    return out
+
+
+def stream_clip(spec, frames: int = None) -> List[Frame]:
+    """Frames of one mixed-workload stream (moving rectangles over the
+    sinusoid background, motion (+2.5, +0.75), sigma 3), all four seeds
+    derived from the stream's own seed."""
+    s = int(spec["seed"])
+    return moving_rects_clip(spec["w"], spec["h"], frames or spec["frames"], seed_luma=4 * s,
+                             seed_chroma=4 * s + 1, seed_noise=4 * s + 2, seed_rects=4 * s + 3)
+
+
+def served_sessions(n: int = 2000, rate_per_s: float = 200.0, seed: int = 9, session_seed0: int = 5000):
+    """Encode sessions arriving as a Poisson process of `rate_per_s`:
+    exponential inter-arrival gaps, 8..64 frames (uniform), resolution and
+    QP uniform over MIX_RESOLUTIONS / MIX_QPS, all from `seed`; session j
+    renders from its own seed session_seed0 + j.  Returns a list of dicts
+    {arrival_s, w, h, qp, seed, frames}."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for j in range(n):
+        t += float(rng.exponential(1.0 / rate_per_s))
+        w, h = MIX_RESOLUTIONS[int(rng.integers(0, len(MIX_RESOLUTIONS)))]
+        qp = MIX_QPS[int(rng.integers(0, len(MIX_QPS)))]
+        nf = int(rng.integers(8, 65))
+        out.append(dict(arrival_s=t, w=w, h=h, qp=qp, seed=session_seed0 + j, frames=nf))
+    return out
