@@ -118,6 +118,34 @@ size_t tcb_ctu_scratch_bytes(int width, int height);
 tc_error_t tcb_ctu_encode_frame(const tcb_frame_desc_t *desc, void *scratch, size_t scratch_bytes,
                                 void *stream);
 
+/* tcb_ctu_encode_frame without any device allocation (no counterpart in
+ * the reference).  For callers that cannot allocate device memory: an
+ * application whose own pool allocator owns all of the GPU's memory, a
+ * plugin host that only lends out the frame buffers it manages, or a
+ * real-time loop in which cudaMalloc / cudaFree and the synchronisation
+ * cudaFree implies are not allowed.  The caller still passes every input
+ * and output buffer in `desc`; the scratch is a fixed device array inside
+ * the library, sized for TCB_CTU_STATIC_MAX_CTUS CTUs (17,664 bytes),
+ * which every GPU that loads the library holds until the process exits.
+ *
+ *  - Frames of more than TCB_CTU_STATIC_MAX_CTUS CTUs (ceil(W/64) *
+ *    ceil(H/64); 3840x2160 is 2,040) return TC_ERR_MEMORY; use
+ *    tcb_ctu_encode_frame for them.  Invalid descriptors return
+ *    TC_ERR_PARAM.
+ *  - The first call on a device, made with that device current, looks up
+ *    the array's device address and uploads the constant tables; make
+ *    that first call before any stream capture.
+ *  - Every call on a device shares the one array, which keeps the last
+ *    call's contents; each call resets what must start at zero on
+ *    `stream` before its encode kernel runs.  Calls whose work overlaps
+ *    on the GPU (different streams, or different host threads, without
+ *    ordering between them) race on the array and give wrong results:
+ *    order them on one stream or serialise them.
+ *  - Calls nothing that allocates (no cudaMalloc, cudaFree, pinned host
+ *    memory or library allocator); launches are asynchronous on `stream`. */
+#define TCB_CTU_STATIC_MAX_CTUS 2048
+tc_error_t tcb_ctu_encode_frame_static(const tcb_frame_desc_t *desc, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

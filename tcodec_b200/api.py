@@ -318,6 +318,8 @@ def bind_b200(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.tcb_ctu_scratch_bytes.restype = ctypes.c_size_t
     lib.tcb_ctu_encode_frame.argtypes = [ctypes.POINTER(FrameDesc), vp, ctypes.c_size_t, vp]
     lib.tcb_ctu_encode_frame.restype = ctypes.c_int
+    lib.tcb_ctu_encode_frame_static.argtypes = [ctypes.POINTER(FrameDesc), vp]
+    lib.tcb_ctu_encode_frame_static.restype = ctypes.c_int
     return lib
 
 

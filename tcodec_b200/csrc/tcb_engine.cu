@@ -1551,6 +1551,47 @@ cudaError_t launch_ctu_items(const FrameParams *d_params, const int *d_items, in
 
 }  // namespace tcb
 
+// --------------------------------------------------------------------
+// Frame entry point that allocates nothing (tcb_ctu_encode_frame_static).
+//
+// Some callers cannot allocate device memory: an application whose own
+// pool allocator reserves the GPU's memory up front and owns every byte of
+// it, a plugin host that only lends out the frame buffers it manages, or a
+// real-time loop in which cudaMalloc / cudaFree (and the device-wide
+// synchronisation cudaFree implies) are not allowed.  For them the
+// scratch that tcb_ctu_encode_frame takes from its caller -- frame
+// parameters, queue counter and error word, per-CTU publish flags, work
+// queue -- lives in this fixed device array instead.  Every GPU that loads
+// the library holds it (17,664 bytes) until the process exits.  In host
+// code the name below only identifies the symbol; its device address comes
+// from cudaGetSymbolAddress.
+// --------------------------------------------------------------------
+static __device__ __align__(256) uint8_t g_ctu_static_scratch[tcb::SCR_DONE + 8 * TCB_CTU_STATIC_MAX_CTUS];
+
+namespace tcb {
+
+// Device address of g_ctu_static_scratch on the current device, looked up
+// on the first call made with that device current and kept afterwards.
+cudaError_t static_scratch_address(uint8_t **out) {
+    static std::mutex mu;
+    static uint8_t *addr[MAX_DEVICES] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_ctu_static_scratch);
+        if (e != cudaSuccess) return e;
+        addr[dev] = (uint8_t *)p;
+    }
+    *out = addr[dev];
+    return cudaSuccess;
+}
+
+}  // namespace tcb
+
 extern "C" {
 
 size_t tcb_ctu_record_bytes(void) { return sizeof(tcb::CtuOut); }
@@ -1567,6 +1608,17 @@ tc_error_t tcb_ctu_encode_frame(const tcb_frame_desc_t *desc, void *scratch, siz
     if (tcb::ensure_device_tables() != cudaSuccess) return TC_ERR_INTERNAL;
     return tcb::encode_frame_with_scratch(P, (uint8_t *)scratch, (cudaStream_t)stream) == cudaSuccess
                ? TC_OK : TC_ERR_INTERNAL;
+}
+
+tc_error_t tcb_ctu_encode_frame_static(const tcb_frame_desc_t *desc, void *stream) {
+    tcb::FrameParams P;
+    if (!desc || !tcb::frame_params_from_desc(*desc, P)) return TC_ERR_PARAM;
+    if (P.ctu_cols * P.ctu_rows > TCB_CTU_STATIC_MAX_CTUS) return TC_ERR_MEMORY;
+    if (tcb::ensure_device_tables() != cudaSuccess) return TC_ERR_INTERNAL;
+    uint8_t *scratch = nullptr;
+    if (tcb::static_scratch_address(&scratch) != cudaSuccess) return TC_ERR_INTERNAL;
+    return tcb::encode_frame_with_scratch(P, scratch, (cudaStream_t)stream) == cudaSuccess ? TC_OK
+                                                                                           : TC_ERR_INTERNAL;
 }
 
 }  // extern "C"
