@@ -1,12 +1,12 @@
 #!/usr/bin/env python
 """Benchmark of the B200 v2 encoder on the headline workload.
 
-Workload (the 1080p configuration the metric is quoted
-on): 1920x1080 4:2:0, GOP4 hierarchical B-frames, CQP QP 32, preset MEDIUM,
+Headline workload (the 1080p configuration the metric is quoted on):
+1920x1080 4:2:0, GOP4 hierarchical B-frames, CQP QP 32, preset MEDIUM,
 profile 1 (two searched references: the reference encoder's reachable form
 of "4 references"), deblocking + SAO.  Source: seeded synthetic sinusoid
 texture + 16 moving noise rectangles + 1-px high-contrast lines over 5% of
-the area (tcodec_b200.synth 'cfg2').
+the area (tcodec_b200.synth 'rects_lines').
 
 Batched form (the headline): --streams independent 1080p streams per GPU
 (default 16; stream s encodes clip frames s, s+1, ...) advance together and
@@ -19,6 +19,20 @@ frames of a device-resident clip.
   e2e        the same through host (pinned) buffers: host->device copies and
              packet / reconstruction read-back inside the timed region
   plain_gpu  one stream alone through the same kernels
+
+Two more forms run at N=1 (section "forms" of the JSON line):
+
+  mixed_batch  64 independent P-only streams, resolutions uniform over
+               {320x240, 640x360, 1280x720, 1920x1080}, QP uniform over
+               {22, 27, 32, 37}, 32 frames each, all in one batch; against
+               the plain one-stream-at-a-time GPU path on the same mix
+               (per-resolution seconds/frame measured on a sample).
+  served       Poisson arrivals (200 sessions/s) of 8..64-frame P-only
+               sessions of the same mix, admitted under an HBM budget
+               (tcb_server); per-frame latency p50/p99 and aggregate
+               frames/s.
+  Both check every stream / session against the reference encoder's
+  digests (tests/golden/mixed_streams.json).
 
 --impl reference times the reference C encoder (oracle/_ref, built from the
 reference sources) on all host cores: one encoder process per core, each
@@ -51,11 +65,13 @@ METRIC = "1080p v2 encode frames/s (bit-exact), batched/served vs plain GPU; p50
 UNIT = "frames/s"
 GOLDEN = os.path.join(ROOT, "tests", "golden", "bench_1080p_gop4b.json")
 TRAFFIC = os.path.join(ROOT, "profiles", "ctu_engine_traffic.json")
+MIXED_GOLDEN = os.path.join(ROOT, "tests", "golden", "mixed_streams.json")
+SERVED_BUDGET = 150 * 10**9          # HBM budget of the served form (bytes)
 
 
 def make_clip(n):
     from tcodec_b200 import synth
-    return synth.workload("cfg2", frames=n)
+    return synth.workload("rects_lines", frames=n)
 
 
 def make_cfg(lib):
@@ -192,6 +208,148 @@ def cpu_baseline(procs):
                       f"C encoder (oracle/_ref, -O3 scalar); {per_proc:.1f} s encode, {wall:.1f} s wall"}
 
 
+# ---------------------------------------------------------------- mixed workloads
+def _render_stream(spec):
+    from tcodec_b200 import synth
+    return synth.stream_clip(spec)
+
+
+def render_streams(specs, procs):
+    """Frames of every stream spec, rendered on `procs` spawned processes
+    (before any CUDA work in this process)."""
+    with mp.get_context("spawn").Pool(procs) as pool:
+        return pool.map(_render_stream, specs, chunksize=1)
+
+
+def stream_digest(packets):
+    h = hashlib.sha256()
+    for p in packets:
+        h.update(len(p).to_bytes(4, "little") + p)
+    return h.hexdigest()
+
+
+def run_mixed_batch(lib, specs, clips):
+    """All streams in one batch, host (pinned) inputs; returns device time,
+    frames and every stream's packets."""
+    import torch
+    from tcodec_b200 import api
+    cfgs = [api.make_config(lib, s["w"], s["h"], qp=s["qp"], preset=PRESET, profile=PROFILE,
+                            keyframe_interval=1000) for s in specs]
+    pinned = [[tuple(torch.from_numpy(np.ascontiguousarray(p)).pin_memory().numpy() for p in f) for f in c]
+              for c in clips]
+    batch = api.BatchEncoder(lib, cfgs)
+    lib.tcb_batch_set_timing(batch.h, 1)
+    n = len(specs)
+    nf = max(len(c) for c in clips)
+    got = [[] for _ in range(n)]
+    stream = torch.cuda.ExternalStream(lib.tcb_batch_stream(batch.h))
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    for t in range(nf):
+        pk = batch.encode([pinned[i][t] if t < len(pinned[i]) else None for i in range(n)], on_device=False)
+        for i, p in enumerate(pk):
+            if p is not None:
+                got[i].append(p)
+    tail = batch.flush()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    st = (ctypes.c_double(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64())
+    lib.tcb_batch_get_timing(batch.h, *[ctypes.byref(x) for x in st])
+    batch.close()
+    for i in range(n):
+        got[i].extend(tail[i])
+    return dict(ms=ev0.elapsed_time(ev1), wall=wall, frames=sum(len(g) for g in got), packets=got,
+                ctu_ms=st[0].value, launches=st[4].value)
+
+
+def plain_seconds_per_frame(lib, w, h, qp, frames):
+    """One stream alone (device inputs, tcb_encoder_encode_device): seconds
+    per frame over `frames` after 2 warm-up frames."""
+    import torch
+    from tcodec_b200 import api
+    enc = api.Encoder(lib, api.make_config(lib, w, h, qp=qp, preset=PRESET, profile=PROFILE,
+                                           keyframe_interval=1000))
+    lib.tcb_encoder_set_recon_readback(enc.h, 0)
+    dev = [tuple(torch.from_numpy(np.ascontiguousarray(p)).cuda() for p in f) for f in frames]
+    stream = torch.cuda.ExternalStream(lib.tcb_encoder_stream(enc.h))
+
+    def one(f):
+        pkt = api.Packet()
+        r = lib.tcb_encoder_encode_device(enc.h, f[0].data_ptr(), w, f[1].data_ptr(), w // 2, f[2].data_ptr(),
+                                          w // 2, ctypes.byref(pkt))
+        if r != api.TC_OK:
+            raise RuntimeError(f"plain encode -> {r}")
+
+    for f in dev[:2]:
+        one(f)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for f in dev[2:]:
+        one(f)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    enc.close()
+    return ev0.elapsed_time(ev1) / 1000.0 / max(1, len(dev) - 2)
+
+
+def run_forms(lib, mixed_specs, mixed_clips, served_specs, served_clips):
+    from tcodec_b200 import serving, synth
+    golden = json.load(open(MIXED_GOLDEN)) if os.path.exists(MIXED_GOLDEN) else None
+    out = {}
+    # ---- batched, 64-stream mix ------------------------------------------
+    mb = run_mixed_batch(lib, mixed_specs, mixed_clips)
+    exact = None
+    if golden:
+        exact = all(stream_digest(mb["packets"][i]) == golden["batch"][i]["digest"]
+                    for i in range(len(mixed_specs)))
+    # plain path on the same mix: seconds/frame per resolution (QP 32
+    # sample, 4 timed frames), summed over the mix's frames
+    spf = {}
+    for (w, h) in synth.MIX_RESOLUTIONS:
+        spec = next((s for s in mixed_specs if (s["w"], s["h"]) == (w, h)), None)
+        if spec is not None:
+            spf[(w, h)] = plain_seconds_per_frame(lib, w, h, 32, synth.stream_clip(dict(spec, frames=6)))
+    plain_s = sum(len(c) * spf[(s["w"], s["h"])] for s, c in zip(mixed_specs, mixed_clips))
+    mixed_frames = sum(len(c) for c in mixed_clips)
+    batched_fps = mb["frames"] / (mb["ms"] / 1000.0)
+    plain_fps = mixed_frames / plain_s
+    pix = sum(s["w"] * s["h"] * len(c) for s, c in zip(mixed_specs, mixed_clips))
+    out["mixed_batch"] = {
+        "streams": len(mixed_specs), "frames": mb["frames"], "value": batched_fps, "unit": UNIT,
+        "pixels_per_s": pix / (mb["ms"] / 1000.0), "plain_gpu_fps": plain_fps,
+        "batched_over_plain": batched_fps / plain_fps, "bit_exact_all_streams": exact,
+        "plain_s_per_frame": {f"{w}x{h}": v for (w, h), v in spf.items()},
+        "what": "64 P-only streams (mixed resolution and QP, 32 frames) in one tcb_batch, host inputs and packets "
+                "inside the timed region; plain = the same frames encoded one stream at a time "
+                "(per-resolution s/frame measured on a 4-frame sample)"}
+    # ---- served -------------------------------------------------------------
+    import torch
+    free, total = torch.cuda.mem_get_info()
+    budget = min(SERVED_BUDGET, int(free * 0.9))
+    sv = serving.serve(lib, served_specs, served_clips, budget, max_active=256, preset=PRESET, profile=PROFILE)
+    exact_s = None
+    if golden and len(golden.get("served", [])) >= len(served_specs):
+        exact_s = all(stream_digest(sv["packets"][j]) == golden["served"][j]["digest"]
+                      for j in range(len(served_specs)))
+    lat = sorted(sv["latencies"])
+    pix_s = sum(s["w"] * s["h"] * s["frames"] for s in served_specs)
+    out["served"] = {
+        "sessions": len(served_specs), "frames": sv["frames"], "value": sv["frames"] / sv["makespan"],
+        "unit": UNIT, "pixels_per_s": pix_s / sv["makespan"],
+        "latency_ms": {"p50": 1000 * lat[len(lat) // 2], "p99": 1000 * lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                       "what": "per frame: push to the server until its packet returns"},
+        "hbm_budget_bytes": sv["budget"], "peak_bytes_in_use": sv["peak_bytes"],
+        "peak_active_sessions": sv["peak_active"], "steps": sv["steps"], "bit_exact_all_sessions": exact_s,
+        "what": f"first {len(served_specs)} sessions of the Poisson schedule (200 sessions/s, 8..64 frames, "
+                "P-only, mixed resolution/QP), replayed in real time through tcb_server; makespan from the "
+                "first arrival to the last packet"}
+    return out
+
+
 # ---------------------------------------------------------------- B200 arm
 def run_b200(args, rank, world):
     """Batched pass (device-resident and host inputs) and a plain
@@ -285,6 +443,11 @@ def run_b200(args, rank, world):
     return dev_run, e2e_run, plain, clocks.summary()
 
 
+def api_lib():
+    from tcodec_b200 import api
+    return api.bind_b200(api.load_library())
+
+
 def max_over_ranks(x, world):
     if world <= 1:
         return x
@@ -312,13 +475,15 @@ def main():
     ap.add_argument("--streams", type=int, default=16, help="1080p streams per GPU in the batched form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the mixed-batch and served forms")
+    ap.add_argument("--served-sessions", type=int, default=64)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
     config = {"workload": "1920x1080 4:2:0, GOP4 hierarchical B, CQP QP32, preset medium, profile 1 (2 searched "
-                          "refs), deblock+SAO, synthetic cfg2 source (sinusoids + 16 moving noise rectangles + "
+                          "refs), deblock+SAO, synthetic source (sinusoids + 16 moving noise rectangles + "
                           "1-px lines over 5% area)",
               "streams_per_gpu": args.streams, "frames_per_step": f"one per stream ({args.streams})",
               "l2": "fresh input frames every step from a device-resident clip (no reuse across steps)",
@@ -344,6 +509,14 @@ def main():
         print(json.dumps(line))
         return
 
+    forms = not args.no_forms and world == 1
+    if forms:
+        from tcodec_b200 import synth
+        procs = max(1, min(32, os.cpu_count() or 1))
+        mixed_specs = synth.mixed_streams()
+        served_specs = synth.served_sessions()[:args.served_sessions]
+        rendered = render_streams(mixed_specs + served_specs, procs)
+        mixed_clips, served_clips = rendered[:len(mixed_specs)], rendered[len(mixed_specs):]
     import torch
     if world > 1:
         torch.cuda.set_device(local)
@@ -365,7 +538,7 @@ def main():
     # Bit-exactness of this run's stream against the reference's committed
     # answers for the same workload (first packets in coding order).
     bit_exact = None
-    if os.path.exists(GOLDEN):
+    if os.path.exists(GOLDEN) and json.load(open(GOLDEN))["inputs"] <= args.warmup + args.steps:
         want = json.load(open(GOLDEN))["packets"]
         got = [hashlib.sha256(p).hexdigest() for p in dev_run["packets"][:len(want)]]
         bit_exact = got == want[:len(got)] and len(got) == len(want)
@@ -382,7 +555,7 @@ def main():
         peak, peak_src = 6650.0, "fallback"
     steps = max(1, dev_run["steps"])
     launches = max(1, dev_run["ctu_launches"])
-    per_launch_s = dev_run["ctu_ms"] / 1000.0 / launches
+    per_launch_s = max(1e-9, dev_run["ctu_ms"] / 1000.0 / launches)
     # frames the timed launches encoded (all CTUs of every stream per step)
     nctu_frame = ((W + 63) // 64) * ((H + 63) // 64)
     frames_in_launches = dev_run["ctu_count"] / nctu_frame
@@ -407,14 +580,14 @@ def main():
         "latency_ms": {"p50": p50, "p99": p99, "what": "per-step batch call latency (one frame of every stream), "
                        "device-resident input"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "kernel": "ctu_kernel (CTU RDO engine)",
+                     "frac": achieved / peak, "traffic": traffic, "kernel": "ctu_persistent_kernel (CTU RDO engine)",
                      "peak_source": peak_src,
-                     "note": "algorithmic bytes 10*W*H per frame (MC 3WH + deblock 3WH + SAO 4WH) spread over "
-                             "the frame's wavefront launches; the engine is latency / integer-pipe bound"},
+                     "note": "algorithmic bytes 10*W*H per frame (MC 3WH + deblock 3WH + SAO 4WH) over the "
+                             "step's persistent launch; the engine is latency / integer-pipe bound, not HBM bound"},
         "ctu_engine": {"ms_per_step": dev_run["ctu_ms"] / steps, "launches_per_step": launches / steps,
                        "ctus_per_launch": dev_run["ctu_count"] / launches},
-        "batch": {"streams_per_gpu": args.streams, "form": "batched: every stream's CTUs on anti-diagonal d share "
-                  "one launch (tcb_batch_encode)"},
+        "batch": {"streams_per_gpu": args.streams, "form": "batched: every stream's CTUs in one persistent "
+                  "wavefront launch per step (tcb_batch_encode)"},
         "plain_gpu": (None if plain is None else {"value": plain["frames"] / (plain["ms"] / 1000.0), "unit": UNIT,
                       "what": "one stream alone through the same kernels (tcb_encoder_encode_device)"}),
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(import_rec),
@@ -422,6 +595,8 @@ def main():
         "gpu_launches": int(dev_run["launches"]),
         "clocks": clocks,
     }
+    if forms:
+        line["forms"] = run_forms(api_lib(), mixed_specs, mixed_clips, served_specs, served_clips)
     if not args.no_cpu_baseline:
         try:
             from oracle import tcref

@@ -80,6 +80,56 @@ void tcb_batch_get_timing(tcb_batch_t *batch, double *ctu_ms, int64_t *ctu_launc
                           int64_t *steps, int64_t *kernel_launches);
 
 /* ---------------------------------------------------------------------
+ * Served form (no reference counterpart): encode sessions that arrive and
+ * leave at any time, admitted under a device-memory budget and advanced
+ * together (continuous batching).  Each admitted session keeps its
+ * reference frames, MV grids and QP state on the device; every step
+ * encodes one frame of every admitted session that has input, in shared
+ * CTU-engine launches.  A session's packets are bit-identical to encoding
+ * it alone with tc_encoder_*.
+ * ------------------------------------------------------------------- */
+typedef struct tcb_server tcb_server_t;
+
+typedef struct tcb_server_packet {
+    int session;            /* id returned by tcb_server_open */
+    int status;             /* TC_OK: packet filled; TC_ERR_NEED_MORE: frame
+                               buffered for B reordering; else an error
+                               (the session is retired) */
+    tc_packet_t packet;     /* data valid until the next tcb_server_step */
+} tcb_server_packet_t;
+
+/* Frames a session may have queued on the host before the server takes
+ * them (tcb_server_push returns TC_ERR_NEED_MORE beyond this). */
+#define TCB_SERVER_QUEUE 2
+
+/* One device allocation of hbm_budget_bytes holds every admitted session;
+ * at most max_active sessions (<= 256) are admitted at once. */
+tcb_server_t *tcb_server_create(size_t hbm_budget_bytes, int max_active);
+void tcb_server_destroy(tcb_server_t *server);
+/* Device bytes a session of this configuration occupies while admitted
+ * (0 for an invalid configuration). */
+size_t tcb_server_session_bytes(const tc_config_t *config);
+/* Queue a session (FIFO).  Returns its id (>= 0), TC_ERR_PARAM for an
+ * invalid configuration, TC_ERR_MEMORY if it can never fit the budget. */
+int tcb_server_open(tcb_server_t *server, const tc_config_t *config);
+/* Queue the session's next frame (host planes, copied before returning). */
+tc_error_t tcb_server_push(tcb_server_t *server, int session,
+                           const tc_pixel_t *y, int stride_y,
+                           const tc_pixel_t *cb, int stride_cb,
+                           const tc_pixel_t *cr, int stride_cr);
+/* No more input: the session drains its B-frame tail, then is retired
+ * and its device memory returns to the budget. */
+tc_error_t tcb_server_finish(tcb_server_t *server, int session);
+/* 0 waiting for admission, 1 admitted, 2 retired. */
+int tcb_server_session_state(tcb_server_t *server, int session);
+/* Admit waiting sessions that fit, then encode one frame of every admitted
+ * session with input.  Writes one entry per session that ran (cap must be
+ * >= max_active) and returns their number, or a negative tc_error_t. */
+int tcb_server_step(tcb_server_t *server, tcb_server_packet_t *out, int cap);
+void tcb_server_stats(tcb_server_t *server, int *waiting, int *active, int *retired,
+                      size_t *bytes_in_use, size_t *bytes_budget);
+
+/* ---------------------------------------------------------------------
  * Part 2: standalone kernels.
  * ------------------------------------------------------------------- */
 
@@ -145,6 +195,30 @@ tc_error_t tcb_ctu_encode_frame(const tcb_frame_desc_t *desc, void *scratch, siz
  *    memory or library allocator); launches are asynchronous on `stream`. */
 #define TCB_CTU_STATIC_MAX_CTUS 2048
 tc_error_t tcb_ctu_encode_frame_static(const tcb_frame_desc_t *desc, void *stream);
+
+/* One frame for the standalone in-loop filters.  Device pointers; the
+ * reconstruction planes are filtered in place. */
+typedef struct tcb_filter_frame {
+    int width, height, stride_y, stride_c;
+    tc_pixel_t *y, *cb, *cr;          /* reconstruction (in place) */
+    const tc_pixel_t *src_y;          /* source luma: SAO decision only */
+    int stride_src;
+    int qp;                           /* frame QP */
+    int16_t *sao_params;              /* SAO out, may be NULL: 3 int16 per CTU
+                                         (present, band, offset), raster order */
+} tcb_filter_frame_t;
+
+/* Deblocking of the internal 4-pixel edges of every full 64x64 CTU of n
+ * frames (partial CTUs at the right / bottom border are left alone, as in
+ * the reference): replaces tc_deblock_ctu (reference src/filter.c:23-237)
+ * as called per CTU at src/encoder.c:1457-1458.  One launch per 32 frames. */
+tc_error_t tcb_deblock_frames(const tcb_filter_frame_t *frames, int n, void *stream);
+
+/* Luma SAO band offset of every CTU of n frames: choose
+ * (tc_sao_choose_bo, reference src/filter.c:269-319), rate gate
+ * (src/encoder.c:1463-1493, lambda = tc_lambda(qp) * 6) and apply
+ * (tc_sao_ctu_luma, src/filter.c:251-266) against src_y. */
+tc_error_t tcb_sao_frames(const tcb_filter_frame_t *frames, int n, void *stream);
 
 #ifdef __cplusplus
 }

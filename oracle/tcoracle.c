@@ -550,6 +550,30 @@ void or_sao_apply(uint8_t *Y, int s, int x, int y0, int w, int h, int band, int 
         }
 }
 
+/* SAO decision of one CTU as the v2 encoder makes it (src/encoder.c:
+ * 1463-1493): tc_sao_choose_bo, then keep the offset only if its SSE plus
+ * 6 * tc_lambda(qp) is below the unfiltered SSE.  Returns present. */
+int or_sao_decide(const uint8_t *org, int os, const uint8_t *rec, int rs, int x, int y, int w, int h,
+                  int qp, int *band, int *offset) {
+    int b = 0, o = 0;
+    int has = or_sao_choose(org, os, rec, rs, x, y, w, h, &b, &o);
+    if (has) {
+        int x1 = x + 64 < w ? x + 64 : w, y1 = y + 64 < h ? y + 64 : h;
+        long long base = 0, cost = 0;
+        for (int r = y; r < y1; r++)
+            for (int c = x; c < x1; c++) {
+                int ov = org[r * os + c], rv = rec[r * rs + c];
+                int r1 = (rv >> 3) == b ? clipi(rv + o, 0, 255) : rv;
+                base += (long long)(ov - rv) * (ov - rv);
+                cost += (long long)(ov - r1) * (ov - r1);
+            }
+        if (cost + (long long)or_lambda(qp) * 6 >= base) has = 0;
+    }
+    *band = has ? b : 0;
+    *offset = has ? o : 0;
+    return has;
+}
+
 /* Two-pass greedy walk over a 4x-decimated SAD, committing each
  * improvement in scan order (src/encoder.c:171-202). */
 void or_global_mv(const uint8_t *cur, const uint8_t *ref, int w, int h, int s, int *gx, int *gy) {

@@ -66,6 +66,8 @@ void or_deblock_ctu(uint8_t *y, int sy, uint8_t *cb, int scb, uint8_t *cr, int s
 int  or_sao_choose(const uint8_t *org, int os, const uint8_t *rec, int rs, int x, int y,
                    int w, int h, int *band, int *offset);
 void or_sao_apply(uint8_t *y, int s, int x, int y0, int w, int h, int band, int offset);
+int  or_sao_decide(const uint8_t *org, int os, const uint8_t *rec, int rs, int x, int y,
+                   int w, int h, int qp, int *band, int *offset);
 
 /* Encoder-only global motion hint (reference src/encoder.c:171-202). */
 void or_global_mv(const uint8_t *cur, const uint8_t *ref, int w, int h, int s, int *gx, int *gy);

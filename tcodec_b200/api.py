@@ -424,3 +424,103 @@ def encode_sequence(lib: ctypes.CDLL, cfg: Config, frames, with_recon: bool = Fa
     finally:
         enc.close()
     return (pkts, recons) if with_recon else pkts
+
+
+class ServerPacket(ctypes.Structure):
+    _fields_ = [("session", ctypes.c_int), ("status", ctypes.c_int), ("packet", Packet)]
+
+
+SESSION_WAITING, SESSION_ACTIVE, SESSION_DONE = 0, 1, 2
+SERVER_QUEUE = 2
+
+
+def bind_server(lib: ctypes.CDLL) -> ctypes.CDLL:
+    """Attach argtypes of the include/tcodec_b200.h served-form entry points."""
+    vp = ctypes.c_void_p
+    lib.tcb_server_create.argtypes = [ctypes.c_size_t, ctypes.c_int]
+    lib.tcb_server_create.restype = vp
+    lib.tcb_server_destroy.argtypes = [vp]
+    lib.tcb_server_session_bytes.argtypes = [ctypes.POINTER(Config)]
+    lib.tcb_server_session_bytes.restype = ctypes.c_size_t
+    lib.tcb_server_open.argtypes = [vp, ctypes.POINTER(Config)]
+    lib.tcb_server_open.restype = ctypes.c_int
+    lib.tcb_server_push.argtypes = [vp, ctypes.c_int] + [vp, ctypes.c_int] * 3
+    lib.tcb_server_push.restype = ctypes.c_int
+    lib.tcb_server_finish.argtypes = [vp, ctypes.c_int]
+    lib.tcb_server_finish.restype = ctypes.c_int
+    lib.tcb_server_session_state.argtypes = [vp, ctypes.c_int]
+    lib.tcb_server_session_state.restype = ctypes.c_int
+    lib.tcb_server_step.argtypes = [vp, ctypes.POINTER(ServerPacket), ctypes.c_int]
+    lib.tcb_server_step.restype = ctypes.c_int
+    lib.tcb_server_stats.argtypes = [vp] + [vp] * 5
+    return lib
+
+
+class Server:
+    """Served form (tcb_server_*): sessions opened at any time, admitted
+    under an HBM budget, advanced together one frame per step."""
+
+    def __init__(self, lib: ctypes.CDLL, hbm_budget_bytes: int, max_active: int = 64):
+        self.lib = bind_server(lib)
+        self.h = lib.tcb_server_create(int(hbm_budget_bytes), int(max_active))
+        if not self.h:
+            raise RuntimeError("tcb_server_create failed")
+        self.max_active = max_active
+        self._out = (ServerPacket * max_active)()
+
+    def close(self):
+        if self.h:
+            self.lib.tcb_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def session_bytes(self, cfg: Config) -> int:
+        return self.lib.tcb_server_session_bytes(ctypes.byref(cfg))
+
+    def open(self, cfg: Config) -> int:
+        sid = self.lib.tcb_server_open(self.h, ctypes.byref(cfg))
+        if sid < 0:
+            raise RuntimeError(f"tcb_server_open -> {sid}")
+        return sid
+
+    def push(self, sid: int, frame) -> bool:
+        """Queue one (y, cb, cr) frame; False when the session's queue is full."""
+        y, cb, cr = (np.ascontiguousarray(p, dtype=np.uint8) for p in frame)
+        r = self.lib.tcb_server_push(self.h, sid, y.ctypes.data, y.shape[1], cb.ctypes.data, cb.shape[1],
+                                     cr.ctypes.data, cr.shape[1])
+        if r == TC_ERR_NEED_MORE:
+            return False
+        if r != TC_OK:
+            raise RuntimeError(f"tcb_server_push -> {r}")
+        return True
+
+    def finish(self, sid: int) -> None:
+        self.lib.tcb_server_finish(self.h, sid)
+
+    def state(self, sid: int) -> int:
+        return self.lib.tcb_server_session_state(self.h, sid)
+
+    def step(self):
+        """One step; returns [(session, status, packet bytes or None)]."""
+        n = self.lib.tcb_server_step(self.h, self._out, self.max_active)
+        if n < 0:
+            raise RuntimeError(f"tcb_server_step -> {n}")
+        res = []
+        for i in range(n):
+            e = self._out[i]
+            data = ctypes.string_at(e.packet.data, e.packet.size) if e.status == TC_OK else None
+            res.append((e.session, e.status, data))
+        return res
+
+    def stats(self):
+        w, a, d = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        used, cap = ctypes.c_size_t(), ctypes.c_size_t()
+        self.lib.tcb_server_stats(self.h, ctypes.byref(w), ctypes.byref(a), ctypes.byref(d), ctypes.byref(used),
+                                  ctypes.byref(cap))
+        return dict(waiting=w.value, active=a.value, retired=d.value, bytes_in_use=used.value,
+                    bytes_budget=cap.value)

@@ -71,10 +71,20 @@ tc_error_t run_step(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkt
         EncImpl &e = *b->encs[s]->impl;
         const tc_error_t r = e.stage_b();
         if (r != TC_OK) return r;
-        b->kernel_launches += 0;
         if (cudaMemcpyAsync(b->d_params + s, e.d_params, sizeof(FrameParams), cudaMemcpyDeviceToDevice, b->st) !=
             cudaSuccess)
             return TC_ERR_INTERNAL;
+    }
+    // Global-motion walks of all P streams, one CTA each, written into the
+    // batch's parameter copies.
+    std::vector<GlobJob> jobs;
+    for (int s : part) {
+        EncImpl &e = *b->encs[s]->impl;
+        if (e.pend.glob) jobs.push_back({e.cur.y, e.pend.glob_ref, e.W, e.H, e.sy, b->d_params + s});
+    }
+    if (!jobs.empty()) {
+        if (launch_glob_mv_multi(jobs.data(), (int)jobs.size(), b->st) != cudaSuccess) return TC_ERR_INTERNAL;
+        b->kernel_launches += ((int)jobs.size() + GlobJobs::MAX - 1) / GlobJobs::MAX;
     }
     // Merged anti-diagonal item lists of the participating streams.
     std::vector<int> off(b->max_diag), cnt(b->max_diag);
@@ -171,6 +181,7 @@ int tcb::batch_attach(tcb_batch *b, tc_encoder_t *e) {
     b->encs[s] = e;
     EncImpl &im = *e->impl;
     im.st = b->st;                          // all device work on the batch stream
+    im.defer_glob = true;
     std::vector<std::vector<int>> diags(im.diag_off.size());
     for (int d = 0; d < (int)im.diag_off.size(); ++d)
         for (int r = 0; r < im.ctu_rows; ++r) {

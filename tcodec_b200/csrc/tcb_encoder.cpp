@@ -366,7 +366,9 @@ tc_error_t EncImpl::stage_b() {
     P.epoch = ++epoch;
     if (cudaMemcpyAsync(d_params, &P, sizeof(P), cudaMemcpyHostToDevice, st) != cudaSuccess)
         return TC_ERR_INTERNAL;
-    if (frame_type == 1 && P.ref_valid[0]) {
+    pend.glob = frame_type == 1 && P.ref_valid[0];
+    pend.glob_ref = P.ref_y[0];
+    if (pend.glob && !defer_glob) {
         if (launch_glob_mv(cur.y, P.ref_y[0], W, H, sy, d_params, st) != cudaSuccess) return TC_ERR_INTERNAL;
         ++kernel_launches;
     }

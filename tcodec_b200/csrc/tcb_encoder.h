@@ -104,8 +104,12 @@ struct EncImpl {
     // staged frame driver
     struct Pending {
         int poc = 0, qp_off = 0, need_hist = 0, is_key = 0, frame_type = 0, qp = 0, use_ep = 0,
-            rs = -1, multiref = 0, bf_idx = -1;
+            rs = -1, multiref = 0, bf_idx = -1, glob = 0;
+        const uint8_t *glob_ref = nullptr;
     } pend;
+    // Batched streams leave the global-motion walk to the batch, which runs
+    // every stream's walk in one launch on the batch's parameter copies.
+    bool defer_glob = false;
     BitWriter fbw;
     std::vector<uint8_t> row_buf;
     tc_error_t plan_input();

@@ -1396,7 +1396,7 @@ __device__ void encode_ctu(Smem &S, const FrameParams &P, int row, int col) {
 }
 
 // One CTA per CTU of one anti-diagonal (items[blockIdx.x]).
-__global__ void __launch_bounds__(NT, 1)
+__global__ void __launch_bounds__(NT, CTAS_PER_SM)
 ctu_kernel(const FrameParams *__restrict__ params, const int *__restrict__ items) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     Smem &S = *reinterpret_cast<Smem *>(smem_raw);
@@ -1422,7 +1422,7 @@ __device__ __forceinline__ void st_release(int *p, int v) {
 // items dequeued before it, by CTAs that are already running, so the queue
 // always drains.  Waits are bounded: on expiry the CTA records an error in
 // ctrl[1] and goes on, and the host reports TC_ERR_INTERNAL.
-__global__ void __launch_bounds__(NT, 1)
+__global__ void __launch_bounds__(NT, CTAS_PER_SM)
 ctu_persistent_kernel(const FrameParams *__restrict__ params, const int *__restrict__ items, int n_items,
                       int *ctrl) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
@@ -1465,6 +1465,11 @@ cudaError_t init_engine_tables() {
     e = cudaFuncSetAttribute(ctu_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(Smem));
     if (e != cudaSuccess) return e;
+    if (CTAS_PER_SM > 1) {   // room for CTAS_PER_SM CTUs' shared memory per SM
+        e = cudaFuncSetAttribute(ctu_persistent_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
+    }
     return cudaFuncSetAttribute(ctu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(Smem));
 }
@@ -1536,6 +1541,7 @@ cudaError_t ensure_device_tables() {
 cudaError_t launch_ctu_persistent(const FrameParams *d_params, const int *d_items, int n, int *d_ctrl,
                                   int grid, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
+    grid *= CTAS_PER_SM;
     ctu_persistent_kernel<<<grid < n ? grid : n, NT, sizeof(Smem), st>>>(d_params, d_items, n, d_ctrl);
     return cudaGetLastError();
 }
@@ -1841,7 +1847,7 @@ __device__ void qt_dec(Smem &S, const FrameParams &P, int ctu_x, int ctu_y, int 
     dec_leaf(S, P, L, coef, ql, qc);
 }
 
-__global__ void __launch_bounds__(NT, 1)
+__global__ void __launch_bounds__(NT, CTAS_PER_SM)
 decode_kernel(const FrameParams *__restrict__ params, const int *__restrict__ items) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     Smem &S = *reinterpret_cast<Smem *>(smem_raw);

@@ -6,7 +6,11 @@
 
 namespace tcb {
 
-constexpr int NT = 512;             // threads per CTA
+#ifndef TCB_NT
+#define TCB_NT 512
+#endif
+constexpr int NT = TCB_NT;          // threads per CTA (one CTU)
+constexpr int CTAS_PER_SM = 512 / NT;   // CTUs resident per SM
 constexpr int NW = NT / 32;         // warps per CTA
 constexpr int NGROUP = 4;           // motion-search warp groups
 constexpr int GT = NT / NGROUP;     // threads per motion-search group

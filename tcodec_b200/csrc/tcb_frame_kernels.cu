@@ -5,6 +5,8 @@
 //                    over a downsampled SAD grid (reference
 //                    src/encoder.c:171-202 estimate_global_mv); each warp
 //                    scores one candidate, candidates commit in order.
+//                    glob_mv_multi_kernel runs the walks of all streams of
+//                    a batch step in one launch, one CTA per stream.
 //   hist16_kernel    16-bin luma histogram for scene-cut detection (the
 //                    chi-square test itself stays on the host in double,
 //                    reference src/encoder.c:2655-2678).
@@ -17,9 +19,8 @@
 
 namespace tcb {
 
-__global__ void __launch_bounds__(1024, 1)
-glob_mv_kernel(const uint8_t *__restrict__ cur, const uint8_t *__restrict__ ref, int W, int H,
-               int s, FrameParams *fp) {
+__device__ void glob_mv_walk(const uint8_t *__restrict__ cur, const uint8_t *__restrict__ ref, int W, int H,
+                             int s, FrameParams *fp) {
     const int cw = W / 4, ch = H / 4;
     const int nx = (cw + 1) / 2, ny = (ch + 1) / 2, ns = nx * ny;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -77,6 +78,18 @@ glob_mv_kernel(const uint8_t *__restrict__ cur, const uint8_t *__restrict__ ref,
     }
 }
 
+__global__ void __launch_bounds__(1024, 1)
+glob_mv_kernel(const uint8_t *__restrict__ cur, const uint8_t *__restrict__ ref, int W, int H,
+               int s, FrameParams *fp) {
+    glob_mv_walk(cur, ref, W, H, s, fp);
+}
+
+// Every stream of a batch step in one launch: CTA j walks job j.
+__global__ void __launch_bounds__(1024, 1) glob_mv_multi_kernel(GlobJobs jobs) {
+    const GlobJob &j = jobs.job[blockIdx.x];
+    glob_mv_walk(j.cur, j.ref, j.W, j.H, j.s, j.fp);
+}
+
 __global__ void hist16_kernel(const uint8_t *__restrict__ y, int W, int H, int s, int *hist) {
     __shared__ int h[16];
     if (threadIdx.x < 16) h[threadIdx.x] = 0;
@@ -111,6 +124,18 @@ cudaError_t launch_glob_mv(const uint8_t *cur, const uint8_t *ref, int W, int H,
                            FrameParams *d_params, cudaStream_t st) {
     glob_mv_kernel<<<1, 1024, 0, st>>>(cur, ref, W, H, s, d_params);
     return cudaGetLastError();
+}
+
+cudaError_t launch_glob_mv_multi(const GlobJob *jobs, int n, cudaStream_t st) {
+    for (int i = 0; i < n; i += GlobJobs::MAX) {
+        GlobJobs g;
+        g.n = n - i < GlobJobs::MAX ? n - i : GlobJobs::MAX;
+        for (int k = 0; k < g.n; ++k) g.job[k] = jobs[i + k];
+        glob_mv_multi_kernel<<<g.n, 1024, 0, st>>>(g);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_hist16(const uint8_t *y, int W, int H, int s, int *d_hist, cudaStream_t st) {

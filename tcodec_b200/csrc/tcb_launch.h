@@ -16,6 +16,17 @@ cudaError_t launch_decode_items(const FrameParams *d_params, const int *d_items,
 cudaError_t launch_ctu_persistent(const FrameParams *d_params, const int *d_items, int n, int *d_ctrl,
                                   int grid, cudaStream_t st);
 cudaError_t launch_ctu_items(const FrameParams *d_params, const int *d_items, int n, cudaStream_t st);
+struct GlobJob {
+    const uint8_t *cur, *ref;
+    int W, H, s;
+    FrameParams *fp;
+};
+struct GlobJobs {                  // passed by value as the kernel parameter
+    static constexpr int MAX = 64;
+    int n;
+    GlobJob job[MAX];
+};
+cudaError_t launch_glob_mv_multi(const GlobJob *jobs, int n, cudaStream_t st);
 cudaError_t launch_glob_mv(const uint8_t *cur, const uint8_t *ref, int W, int H, int s,
                            FrameParams *d_params, cudaStream_t st);
 cudaError_t launch_hist16(const uint8_t *y, int W, int H, int s, int *d_hist, cudaStream_t st);

@@ -151,14 +151,14 @@ def with_lines(frames: List[Frame], area_frac: float = 0.05, seed: int = 21) -> 
 
 
 def workload(name: str, frames: int = None, width: int = None, height: int = None) -> List[Frame]:
-    """Named workloads: 'cfg0' (320x240 sinusoid, motion (+1.25, -0.5),
-    sigma 2) and 'cfg1' (1280x720 sinusoid + rectangles, motion
-    (+2.5, +0.75), sigma 3)."""
-    if name == "cfg0":
+    """Named workloads: 'sinusoid' (320x240 sinusoid, motion (+1.25, -0.5),
+    sigma 2), 'rects' (1280x720 sinusoid + rectangles, motion (+2.5, +0.75),
+    sigma 3) and 'rects_lines' (1920x1080 rectangles + 1-px lines)."""
+    if name == "sinusoid":
         return sinusoid_clip(width or 320, height or 240, frames or 30)
-    if name == "cfg1":
+    if name == "rects":
         return moving_rects_clip(width or 1280, height or 720, frames or 60)
-    if name == "cfg2":
+    if name == "rects_lines":
         return with_lines(moving_rects_clip(width or 1920, height or 1080, frames or 120, motion=(2.5, 0.75),
                                             noise_sigma=3.0))
     raise ValueError(name)

@@ -1,6 +1,6 @@
 """Generates tests/golden/bench_1080p_gop4b.json: SHA-256 of the first
 packets (coding order) the reference encoder emits for bench.py's
-workload (1920x1080 GOP4 B, QP32, medium, profile 1, synthetic 'cfg2'
+workload (1920x1080 GOP4 B, QP32, medium, profile 1, synthetic 'rects_lines'
 source).  bench.py compares its own stream against these to report
 bit-exactness.  Run from the repository root (needs oracle/_ref):
     python tests/golden/make_bench_golden.py
