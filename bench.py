@@ -64,7 +64,7 @@ W, H, QP, PRESET, PROFILE = 1920, 1080, 32, 2, 1
 METRIC = "1080p v2 encode frames/s (bit-exact), batched/served vs plain GPU; p50/p99 latency"
 UNIT = "frames/s"
 GOLDEN = os.path.join(ROOT, "tests", "golden", "bench_1080p_gop4b.json")
-TRAFFIC = os.path.join(ROOT, "profiles", "ctu_engine_traffic.json")
+TRAFFIC = os.path.join(ROOT, "profiles", "ctu_engine_traffic.txt")   # JSON body
 MIXED_GOLDEN = os.path.join(ROOT, "tests", "golden", "mixed_streams.json")
 SERVED_BUDGET = 150 * 10**9          # HBM budget of the served form (bytes)
 
