@@ -408,14 +408,20 @@ def run_b200(args, rank, world):
             return len(got), sum(len(p) for p in got)
 
         st = (ctypes.c_double(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64())
-        reset = lambda: lib.tcb_batch_get_timing(batch.h, *[ctypes.byref(x) for x in st])
+        hs = (ctypes.c_double(), ctypes.c_double(), ctypes.c_double())
+
+        def reset():
+            lib.tcb_batch_get_timing(batch.h, *[ctypes.byref(x) for x in st])
+            lib.tcb_batch_get_host_timing(batch.h, *[ctypes.byref(x) for x in hs])
+
         res = timed(lib.tcb_batch_stream(batch.h), step, reset)
         reset()
         tail = batch.flush()
         batch.close()
         ms, frames, nbytes, lat = res
         return dict(ms=ms, frames=frames, bytes=nbytes, lat=lat, packets=first + tail[0], ctu_ms=st[0].value,
-                    ctu_launches=st[1].value, ctu_count=st[2].value, steps=st[3].value, launches=st[4].value)
+                    ctu_launches=st[1].value, ctu_count=st[2].value, steps=st[3].value, launches=st[4].value,
+                    host=[x.value for x in hs])
 
     def plain_pass():
         enc = api.Encoder(lib, make_cfg(lib))
@@ -586,6 +592,8 @@ def main():
                              "step's persistent launch; the engine is latency / integer-pipe bound, not HBM bound"},
         "ctu_engine": {"ms_per_step": dev_run["ctu_ms"] / steps, "launches_per_step": launches / steps,
                        "ctus_per_launch": dev_run["ctu_count"] / launches},
+        "host_ms_per_step": {k: v / steps for k, v in zip(("plan_launch", "wait_device", "entropy"),
+                                                          dev_run["host"])},
         "batch": {"streams_per_gpu": args.streams, "form": "batched: every stream's CTUs in one persistent "
                   "wavefront launch per step (tcb_batch_encode)"},
         "plain_gpu": (None if plain is None else {"value": plain["frames"] / (plain["ms"] / 1000.0), "unit": UNIT,

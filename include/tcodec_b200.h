@@ -78,6 +78,9 @@ tc_error_t tcb_batch_flush(tcb_batch_t *batch, tc_packet_t *packets, int *status
 void tcb_batch_set_timing(tcb_batch_t *batch, int enabled);
 void tcb_batch_get_timing(tcb_batch_t *batch, double *ctu_ms, int64_t *ctu_launches, int64_t *ctu_count,
                           int64_t *steps, int64_t *kernel_launches);
+/* Host wall-clock split of the timed steps (timing enabled): planning and
+ * launch, waiting for the device, entropy coding.  Reading resets. */
+void tcb_batch_get_host_timing(tcb_batch_t *batch, double *plan_ms, double *wait_ms, double *entropy_ms);
 
 /* ---------------------------------------------------------------------
  * Served form (no reference counterpart): encode sessions that arrive and

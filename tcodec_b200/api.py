@@ -312,6 +312,7 @@ def bind_b200(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.tcb_batch_flush.restype = ctypes.c_int
     lib.tcb_batch_set_timing.argtypes = [vp, ctypes.c_int]
     lib.tcb_batch_get_timing.argtypes = [vp] + [vp] * 5
+    lib.tcb_batch_get_host_timing.argtypes = [vp] + [vp] * 3
     lib.tcb_ctu_record_bytes.restype = ctypes.c_size_t
     lib.tcb_mv_cell_bytes.restype = ctypes.c_size_t
     lib.tcb_ctu_scratch_bytes.argtypes = [ctypes.c_int, ctypes.c_int]

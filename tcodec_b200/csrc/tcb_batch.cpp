@@ -9,6 +9,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <thread>
 #include <vector>
 
@@ -36,6 +37,7 @@ struct tcb_batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double ctu_ms = 0.0;
     long long ctu_launches = 0, ctu_count = 0, steps = 0, kernel_launches = 0;
+    double host_plan_ms = 0.0, host_wait_ms = 0.0, host_entropy_ms = 0.0;   // wall-clock split of steps
     int device = 0;
 };
 
@@ -57,8 +59,13 @@ void release(tcb_batch *b) {
 }
 
 // Run stage_a..stage_d for the streams whose plan produced a frame.
+double ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
 tc_error_t run_step(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkts, int *status) {
     const int n = (int)b->encs.size();
+    auto t0 = std::chrono::steady_clock::now();
     for (int s : part) {
         EncImpl &e = *b->encs[s]->impl;
         const tc_error_t r = e.stage_a(e.pend.poc, e.pend.qp_off);
@@ -130,7 +137,9 @@ tc_error_t run_step(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkt
                                           cudaMemcpyDeviceToHost, b->st) != cudaSuccess)
             return TC_ERR_INTERNAL;
     }
+    if (b->timing) { b->host_plan_ms += ms_since(t0); t0 = std::chrono::steady_clock::now(); }
     if (cudaStreamSynchronize(b->st) != cudaSuccess) return TC_ERR_INTERNAL;
+    if (b->timing) { b->host_wait_ms += ms_since(t0); t0 = std::chrono::steady_clock::now(); }
     if (b->timing) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, b->ev0, b->ev1);
@@ -145,6 +154,7 @@ tc_error_t run_step(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkt
     for (int s : part)
         th.emplace_back([&, s]() { rs[s] = b->encs[s]->impl->stage_d(&pkts[s]); });
     for (auto &t : th) t.join();
+    if (b->timing) b->host_entropy_ms += ms_since(t0);
     tc_error_t worst = TC_OK;
     for (int s : part) {
         status[s] = rs[s];
@@ -290,6 +300,14 @@ tc_error_t tcb_batch_flush(tcb_batch_t *b, tc_packet_t *packets, int *status) {
 
 void tcb_batch_set_timing(tcb_batch_t *b, int enabled) {
     if (b) b->timing = enabled != 0;
+}
+
+void tcb_batch_get_host_timing(tcb_batch_t *b, double *plan_ms, double *wait_ms, double *entropy_ms) {
+    if (!b) return;
+    if (plan_ms) *plan_ms = b->host_plan_ms;
+    if (wait_ms) *wait_ms = b->host_wait_ms;
+    if (entropy_ms) *entropy_ms = b->host_entropy_ms;
+    b->host_plan_ms = b->host_wait_ms = b->host_entropy_ms = 0.0;
 }
 
 void tcb_batch_get_timing(tcb_batch_t *b, double *ctu_ms, int64_t *ctu_launches, int64_t *ctu_count,

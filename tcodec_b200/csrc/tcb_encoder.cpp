@@ -181,6 +181,16 @@ bool EncImpl::init(const tc_config_t &c) {
     if (!out_buf) return false;
     rc_init(c);
     bf_b_mode = c.enable_b_frames ? 1 : 0;
+    // B-frame reorder buffers, allocated once: the reorder path then makes
+    // no device allocation (and no implicit device synchronisation) per frame.
+    if (bf_b_mode)
+        for (size_t i = 0; i < BF_MAX; ++i) {
+            DevFrame f;
+            CK(dmalloc(&f.y, ybytes));
+            CK(dmalloc(&f.cb, cbytes));
+            CK(dmalloc(&f.cr, cbytes));
+            bf_free.push_back(f);
+        }
     return true;
 }
 
@@ -195,7 +205,9 @@ void EncImpl::release() {
     dfree(d_sse); cudaFreeHost(h_sse); dfree(d_err); dfree(d_items);
     dfree(d_done); dfree(d_ctrl); cudaFreeHost(h_ctrl);
     for (auto &f : bf_frames) { dfree(f.y); dfree(f.cb); dfree(f.cr); }
+    for (auto &f : bf_free) { dfree(f.y); dfree(f.cb); dfree(f.cr); }
     bf_frames.clear();
+    bf_free.clear();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (own_st) cudaStreamDestroy(own_st);
@@ -513,8 +525,7 @@ tc_error_t EncImpl::stage_d(tc_packet_t *pkt) {
     grid_cur = 1 - grid_cur;   // this frame's grid becomes the temporal predictor
     prev_mv_valid = 1;
     if (pend.bf_idx >= 0) {
-        DevFrame &f = bf_frames[pend.bf_idx];
-        dfree(f.y); dfree(f.cb); dfree(f.cr);
+        bf_free.push_back(bf_frames[pend.bf_idx]);   // back to the reorder pool
         bf_frames.erase(bf_frames.begin() + pend.bf_idx);
         bf_pocs.erase(bf_pocs.begin() + pend.bf_idx);
         pend.bf_idx = -1;
@@ -633,12 +644,9 @@ bool EncImpl::bf_can_emit() const {
     return bf_emit_pos > bf_anchor_slot(p);
 }
 tc_error_t EncImpl::bf_push_current() {
-    if (bf_pocs.size() >= BF_MAX) return TC_OK;
-    DevFrame f;
-    const size_t ybytes = (size_t)sy * H + 64, cbytes = (size_t)sc * (H / 2) + 64;
-    if (dmalloc(&f.y, ybytes) != cudaSuccess || dmalloc(&f.cb, cbytes) != cudaSuccess ||
-        dmalloc(&f.cr, cbytes) != cudaSuccess)
-        return TC_ERR_MEMORY;
+    if (bf_pocs.size() >= BF_MAX || bf_free.empty()) return TC_OK;
+    DevFrame f = bf_free.back();
+    bf_free.pop_back();
     if (!dcopy(f, cur)) return TC_ERR_INTERNAL;
     bf_frames.push_back(f);
     bf_pocs.push_back(bf_next_input);

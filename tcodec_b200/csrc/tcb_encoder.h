@@ -75,7 +75,8 @@ struct EncImpl {
     double rc_buffer_size = 0.0, rc_buffer_level = 0.5;
     // B-frame reorder
     int bf_b_mode = 0, bf_emit_pos = 0, bf_next_input = 0;
-    std::vector<DevFrame> bf_frames;
+    std::vector<DevFrame> bf_frames;   // occupied reorder buffers (with bf_pocs)
+    std::vector<DevFrame> bf_free;     // unoccupied reorder buffers
     std::vector<int> bf_pocs;
 
     // Device memory comes from `arena` when set (served sessions), else

@@ -46,9 +46,16 @@ __device__ unsigned long long tcb_phase_cycles[16];
 #define PHASE_T0() long long _ph_t = clock64()
 #define PHASE(k) do { if (threadIdx.x == 0) { const long long _n = clock64(); \
     atomicAdd(&tcb_phase_cycles[k], (unsigned long long)(_n - _ph_t)); _ph_t = _n; } } while (0)
+// Inside a motion search, thread 0 of group 0 splits its time into the
+// integer stages (slot 11) and the quarter-pel refinement (slot 12).
+#define ME_T0() long long _me_t = clock64()
+#define ME_MARK(k) do { if (g == 0 && gt == 0) { const long long _n = clock64(); \
+    atomicAdd(&tcb_phase_cycles[k], (unsigned long long)(_n - _me_t)); _me_t = _n; } } while (0)
 #else
 #define PHASE_T0() do {} while (0)
 #define PHASE(k) do {} while (0)
+#define ME_T0() do {} while (0)
+#define ME_MARK(k) do {} while (0)
 #endif
 
 __device__ __forceinline__ void group_bar(int g) {
@@ -182,21 +189,16 @@ __device__ void int_stage(Smem &S, int g, int gt, const uint8_t *ref, int s, int
     }
 }
 
-// Sub-pel SADs of the quarter-pel pattern points first..8 around (cx, cy)
-// (quarter-pel), all in one pass: six-tap diagonal interpolation where the
+// Sub-pel SAD of one candidate: six-tap diagonal interpolation where the
 // margins allow, else the bilinear sub-pel SAD (reference
-// src/motion.c:308-341 and 450-481).  Points whose integer footprint leaves
-// the frame get 0x7FFFFFFF and are skipped by the caller.
-__device__ void group_subpel_sads(Smem &S, int g, int gt, const uint8_t *ref, int s, int W, int H,
-                                  const uint8_t *cur, int blk, int cx, int cy, int first) {
-    const int K = 9 - first, npx = blk * blk, total = K * npx;
-    int acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+// src/motion.c:308-341 and 450-481).
+__device__ int group_subpel_sad(Smem &S, int g, int gt, const uint8_t *ref, int s,
+                                const uint8_t *cur, int blk, int qx, int qy, bool six) {
+    const int fx = qx >> 2, fy = qy >> 2, dx = qx & 3, dy = qy & 3;
+    int acc = 0;
+    const int total = blk * blk;
     for (int i = gt; i < total; i += GT) {
-        const int k = i / npx, pix = i - k * npx, yy = pix / blk, xx = pix - yy * blk;
-        const int qx = cx + c_qpel[first + k][0], qy = cy + c_qpel[first + k][1];
-        const int fx = qx >> 2, fy = qy >> 2, dx = qx & 3, dy = qy & 3;
-        if (fx < 0 || fy < 0 || fx + blk + 1 > W || fy + blk + 1 > H) continue;
-        const bool six = fx >= 2 && fy >= 2 && fx + blk + 2 < W && fy + blk + 2 < H;
+        const int yy = i / blk, xx = i - yy * blk;
         int p;
         if (six) {
             p = luma_hv(ref, s, fx + xx, fy + yy, dx, dy);
@@ -206,32 +208,21 @@ __device__ void group_subpel_sads(Smem &S, int g, int gt, const uint8_t *ref, in
             const int bot = interp_qpel(q[s], q[s + 1], dx);
             p = interp_qpel(top, bot, dy);
         }
-        const int v = absi((int)cur[yy * 64 + xx] - p);
-#pragma unroll
-        for (int kk = 0; kk < 8; ++kk) acc[kk] += (kk == k) ? v : 0;
+        acc += absi((int)cur[yy * 64 + xx] - p);
     }
-    const int wig = gt >> 5, lane = gt & 31;
-#pragma unroll
-    for (int kk = 0; kk < 8; ++kk) {
-        if (kk < K) {
-            const int v = __reduce_add_sync(0xffffffffu, acc[kk]);
-            if (lane == 0) S.me[g].part[wig][kk] = v;
-        }
-    }
+    acc = __reduce_add_sync(0xffffffffu, acc);
+    if ((gt & 31) == 0) S.me[g].part[gt >> 5][0] = acc;
     group_bar(g);
-    if (gt < K) {
-        const int qx = cx + c_qpel[first + gt][0], qy = cy + c_qpel[first + gt][1];
-        const int fx = qx >> 2, fy = qy >> 2;
-        int sum = 0;
+    int sum = 0;
 #pragma unroll
-        for (int w = 0; w < GT / 32; ++w) sum += S.me[g].part[w][gt];
-        S.me[g].sad[gt] = (fx < 0 || fy < 0 || fx + blk + 1 > W || fy + blk + 1 > H) ? 0x7FFFFFFF : sum;
-    }
+    for (int w = 0; w < GT / 32; ++w) sum += S.me[g].part[w][0];
     group_bar(g);
+    return sum;
 }
 
 __device__ void me_run(Smem &S, int g, int gt, const uint8_t *ref, int s, int W, int H,
                        int lx, int ly, int blk, int center_x, int center_y, int sr) {
+    ME_T0();
     const uint8_t *cur = S.cur_y + ly * 64 + lx;
     int bx = clampi(center_x, 0, W - blk), by = clampi(center_y, 0, H - blk);
     group_int_sads(S, g, gt, ref, s, W, H, cur, blk, 3, 0, 1, bx, by, 1);
@@ -241,25 +232,19 @@ __device__ void me_run(Smem &S, int g, int gt, const uint8_t *ref, int s, int W,
     int_stage(S, g, gt, ref, s, W, H, cur, blk, 0, 6, 2, scale, bx, by, bsad);
     int_stage(S, g, gt, ref, s, W, H, cur, blk, 1, 6, 3, 1, bx, by, bsad);
     int_stage(S, g, gt, ref, s, W, H, cur, blk, 2, 4, 4, 1, bx, by, bsad);
-    // Quarter-pel refinement: points are taken relative to the running best
-    // and the first improvement commits, so after a commit the remaining
-    // points are scored again around the new best.
+    ME_MARK(11);
+    // Quarter-pel refinement around the running best, first improvement
+    // commits (reference src/motion.c:450-481).
     int mx = bx * 4, my = by * 4;
-    int first = 1;
-    while (first <= 8) {
-        group_subpel_sads(S, g, gt, ref, s, W, H, cur, blk, mx, my, first);
-        int found = -1;
-        for (int k = 0; k < 9 - first; ++k)
-            if (S.me[g].sad[k] < bsad) { found = k; break; }
-        const int fs = found >= 0 ? S.me[g].sad[found] : 0;
-        group_bar(g);
-        if (found < 0) break;
-        const int p = first + found;
-        mx += c_qpel[p][0];
-        my += c_qpel[p][1];
-        bsad = fs;
-        first = p + 1;
+    for (int p = 1; p < 9; ++p) {
+        const int qx = mx + c_qpel[p][0], qy = my + c_qpel[p][1];
+        const int fx = qx >> 2, fy = qy >> 2;
+        if (fx < 0 || fy < 0 || fx + blk + 1 > W || fy + blk + 1 > H) continue;
+        const bool six = fx >= 2 && fy >= 2 && fx + blk + 2 < W && fy + blk + 2 < H;
+        const int sad = group_subpel_sad(S, g, gt, ref, s, cur, blk, qx, qy, six);
+        if (sad < bsad) { bsad = sad; mx = qx; my = qy; }
     }
+    ME_MARK(12);
     if (gt == 0) { S.me[g].mvx = mx; S.me[g].mvy = my; S.me[g].best = bsad; }
 }
 

@@ -32,7 +32,17 @@ namespace tcb {
 
 namespace {
 
-constexpr int FT = 256;   // threads per CTA (one CTU)
+// Threads per CTA (one CTU each).  Small CTAs let many CTUs' loads be in
+// flight per SM while other CTUs of the same SM filter.
+#ifndef TCB_DEBLOCK_FT
+#define TCB_DEBLOCK_FT 128
+#endif
+#ifndef TCB_SAO_FT
+#define TCB_SAO_FT 64
+#endif
+constexpr int DFT = TCB_DEBLOCK_FT, SFT = TCB_SAO_FT;
+static_assert(384 % DFT == 0 && DFT >= 32, "deblock CTA: 384 16-byte pieces per CTU");
+static_assert(256 % SFT == 0 && SFT >= 32 && SFT <= 256, "SAO CTA: 256 16-pixel segments per CTU");
 
 __device__ __forceinline__ int find_frame(const int *off, int n, int g) {
     int k = 0;
@@ -46,7 +56,7 @@ __device__ __forceinline__ bool aligned16(const void *p, int stride) {
 
 // ---------------------------------------------------------------- deblock
 
-__global__ void __launch_bounds__(FT) deblock_frames_kernel(DeblockJobs J) {
+__global__ void __launch_bounds__(DFT) deblock_frames_kernel(DeblockJobs J) {
     __shared__ __align__(16) uint8_t ty[64 * 64];
     __shared__ __align__(16) uint8_t tc[2][32 * 32];
     const int k = find_frame(J.ctu_off, J.n, blockIdx.x);
@@ -57,16 +67,32 @@ __global__ void __launch_bounds__(FT) deblock_frames_kernel(DeblockJobs J) {
     uint8_t *gy = F.y + (size_t)y0 * F.sy + x0;
     uint8_t *gc[2] = {F.cb + (size_t)(y0 >> 1) * F.sc + (x0 >> 1), F.cr + (size_t)(y0 >> 1) * F.sc + (x0 >> 1)};
     const bool vec = aligned16(F.y, F.sy) && aligned16(F.cb, F.sc) && aligned16(F.cr, F.sc);
-    // ---- load: luma row t>>2, 16-byte segment t&3; chroma rows on t < 128
+    // ---- load: 16-byte pieces 0..255 luma (row p>>2, segment p&3),
+    // 256..383 chroma (plane, row, segment); all issued before any use
     if (vec) {
-        *(uint4 *)&ty[t * 16] = __ldcs((const uint4 *)(gy + (size_t)(t >> 2) * F.sy + (t & 3) * 16));
-        if (t < 128) {
-            const int c = t >> 6, r = (t >> 1) & 31, s = t & 1;
-            *(uint4 *)&tc[c][r * 32 + s * 16] = __ldcs((const uint4 *)(gc[c] + (size_t)r * F.sc + s * 16));
+        uint4 v[384 / DFT];
+#pragma unroll
+        for (int j = 0; j < 384 / DFT; ++j) {
+            const int p = t + j * DFT;
+            if (p < 256) {
+                v[j] = __ldcs((const uint4 *)(gy + (size_t)(p >> 2) * F.sy + (p & 3) * 16));
+            } else {
+                const int q = p - 256, c = q >> 6, r = (q >> 1) & 31, sg = q & 1;
+                v[j] = __ldcs((const uint4 *)(gc[c] + (size_t)r * F.sc + sg * 16));
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 384 / DFT; ++j) {
+            const int p = t + j * DFT;
+            if (p < 256) *(uint4 *)&ty[p * 16] = v[j];
+            else {
+                const int q = p - 256, c = q >> 6, r = (q >> 1) & 31, sg = q & 1;
+                *(uint4 *)&tc[c][r * 32 + sg * 16] = v[j];
+            }
         }
     } else {
-        for (int i = t; i < 64 * 64; i += FT) ty[i] = gy[(size_t)(i >> 6) * F.sy + (i & 63)];
-        for (int i = t; i < 2 * 32 * 32; i += FT) {
+        for (int i = t; i < 64 * 64; i += DFT) ty[i] = gy[(size_t)(i >> 6) * F.sy + (i & 63)];
+        for (int i = t; i < 2 * 32 * 32; i += DFT) {
             const int c = i >> 10, p = i & 1023;
             tc[c][p] = gc[c][(size_t)(p >> 5) * F.sc + (p & 31)];
         }
@@ -75,7 +101,7 @@ __global__ void __launch_bounds__(FT) deblock_frames_kernel(DeblockJobs J) {
     const int qp = F.qp, ltc = clampi(qp / 3, 1, 10);
     const int cqp = clampi(qp - 1, 0, 63), ctc = clampi(cqp / 4, 1, 6);
     // ---- vertical edges: luma x = 4..60 (rows 0..63), Cb x = 4..28
-    for (int i = t; i < 15 * 64 + 7 * 32; i += FT) {
+    for (int i = t; i < 15 * 64 + 7 * 32; i += DFT) {
         if (i < 15 * 64) {
             const int r = i / 15, x = (i - r * 15 + 1) * 4;
             uint8_t *p = &ty[r * 64 + x];
@@ -98,7 +124,7 @@ __global__ void __launch_bounds__(FT) deblock_frames_kernel(DeblockJobs J) {
     __syncthreads();
     // ---- horizontal edges: luma y = 4..60; chroma rows (4e, 4e+1),
     // e = 1..7, with the Cr strength deciding for both planes
-    for (int i = t; i < 15 * 64 + 7 * 32; i += FT) {
+    for (int i = t; i < 15 * 64 + 7 * 32; i += DFT) {
         if (i < 15 * 64) {
             const int y = (i / 64 + 1) * 4, c = i & 63;
             uint8_t *p = &ty[y * 64 + c];
@@ -124,14 +150,19 @@ __global__ void __launch_bounds__(FT) deblock_frames_kernel(DeblockJobs J) {
     __syncthreads();
     // ---- store
     if (vec) {
-        __stcs((uint4 *)(gy + (size_t)(t >> 2) * F.sy + (t & 3) * 16), *(const uint4 *)&ty[t * 16]);
-        if (t < 128) {
-            const int c = t >> 6, r = (t >> 1) & 31, s = t & 1;
-            __stcs((uint4 *)(gc[c] + (size_t)r * F.sc + s * 16), *(const uint4 *)&tc[c][r * 32 + s * 16]);
+#pragma unroll
+        for (int j = 0; j < 384 / DFT; ++j) {
+            const int p = t + j * DFT;
+            if (p < 256) {
+                __stcs((uint4 *)(gy + (size_t)(p >> 2) * F.sy + (p & 3) * 16), *(const uint4 *)&ty[p * 16]);
+            } else {
+                const int q = p - 256, c = q >> 6, r = (q >> 1) & 31, sg = q & 1;
+                __stcs((uint4 *)(gc[c] + (size_t)r * F.sc + sg * 16), *(const uint4 *)&tc[c][r * 32 + sg * 16]);
+            }
         }
     } else {
-        for (int i = t; i < 64 * 64; i += FT) gy[(size_t)(i >> 6) * F.sy + (i & 63)] = ty[i];
-        for (int i = t; i < 2 * 32 * 32; i += FT) {
+        for (int i = t; i < 64 * 64; i += DFT) gy[(size_t)(i >> 6) * F.sy + (i & 63)] = ty[i];
+        for (int i = t; i < 2 * 32 * 32; i += DFT) {
             const int c = i >> 10, p = i & 1023;
             gc[c][(size_t)(p >> 5) * F.sc + (p & 31)] = tc[c][p];
         }
@@ -145,36 +176,51 @@ __device__ __forceinline__ uint8_t byte_of(const uint4 &v, int k) {
     return (uint8_t)(w >> ((k & 3) * 8));
 }
 
-__global__ void __launch_bounds__(FT) sao_frames_kernel(SaoJobs J) {
-    __shared__ int hist[32][FT];              // count * 65536 + sum, per thread
+// Packs bytes b[0..15] into a uint4 (little endian within each word).
+__device__ __forceinline__ uint4 pack16(const uint8_t *b) {
+    uint4 v;
+    v.x = b[0] | b[1] << 8 | b[2] << 16 | (uint32_t)b[3] << 24;
+    v.y = b[4] | b[5] << 8 | b[6] << 16 | (uint32_t)b[7] << 24;
+    v.z = b[8] | b[9] << 8 | b[10] << 16 | (uint32_t)b[11] << 24;
+    v.w = b[12] | b[13] << 8 | b[14] << 16 | (uint32_t)b[15] << 24;
+    return v;
+}
+
+__global__ void __launch_bounds__(SFT) sao_frames_kernel(SaoJobs J) {
+    constexpr int NSEG = 256 / SFT;           // 16-pixel segments per thread
+    constexpr int TPB = SFT / 32;             // threads summing one band
+    __shared__ int hist[32][SFT];             // count * 65536 + sum, per thread
     __shared__ int band_cnt[32], band_sum[32], corr[32];
-    __shared__ long long red[FT / 32];
+    __shared__ long long red[SFT / 32];
     __shared__ int dec[3];
     const int k = find_frame(J.ctu_off, J.n, blockIdx.x);
     const SaoFrame &F = J.f[k];
     const int local = blockIdx.x - J.ctu_off[k], cols = (F.W + 63) >> 6;
     const int x0 = (local % cols) << 6, y0 = (local / cols) << 6;
     const int w = min(64, F.W - x0), h = min(64, F.H - y0);
-    const int t = threadIdx.x, row = t >> 2, c0 = (t & 3) * 16;
-    const int nvalid = row < h ? max(0, min(16, w - c0)) : 0;
-    uint8_t *gr = F.rec + (size_t)(y0 + row) * F.sr + x0 + c0;
-    const uint8_t *go = F.org + (size_t)(y0 + row) * F.so + x0 + c0;
-    uint4 rv = make_uint4(0, 0, 0, 0), ov = make_uint4(0, 0, 0, 0);
-    const bool vec = nvalid == 16 && aligned16(gr, F.sr) && aligned16(go, F.so);
-    if (vec) {
-        rv = __ldcs((const uint4 *)gr);
-        ov = __ldcs((const uint4 *)go);
-    } else if (nvalid > 0) {
-        uint8_t rb[16] = {0}, ob[16] = {0};
-        for (int i = 0; i < nvalid; ++i) { rb[i] = gr[i]; ob[i] = go[i]; }
-        rv.x = rb[0] | rb[1] << 8 | rb[2] << 16 | (uint32_t)rb[3] << 24;
-        rv.y = rb[4] | rb[5] << 8 | rb[6] << 16 | (uint32_t)rb[7] << 24;
-        rv.z = rb[8] | rb[9] << 8 | rb[10] << 16 | (uint32_t)rb[11] << 24;
-        rv.w = rb[12] | rb[13] << 8 | rb[14] << 16 | (uint32_t)rb[15] << 24;
-        ov.x = ob[0] | ob[1] << 8 | ob[2] << 16 | (uint32_t)ob[3] << 24;
-        ov.y = ob[4] | ob[5] << 8 | ob[6] << 16 | (uint32_t)ob[7] << 24;
-        ov.z = ob[8] | ob[9] << 8 | ob[10] << 16 | (uint32_t)ob[11] << 24;
-        ov.w = ob[12] | ob[13] << 8 | ob[14] << 16 | (uint32_t)ob[15] << 24;
+    const int t = threadIdx.x;
+    // segment j of this thread: row (t + j*SFT) >> 2, columns 16 * ((t + j*SFT) & 3)
+    uint4 rv[NSEG], ov[NSEG];
+    int nvalid[NSEG];
+    bool vec[NSEG];
+#pragma unroll
+    for (int j = 0; j < NSEG; ++j) {
+        const int sg = t + j * SFT, row = sg >> 2, c0 = (sg & 3) * 16;
+        nvalid[j] = row < h ? max(0, min(16, w - c0)) : 0;
+        const uint8_t *gr = F.rec + (size_t)(y0 + row) * F.sr + x0 + c0;
+        const uint8_t *go = F.org + (size_t)(y0 + row) * F.so + x0 + c0;
+        vec[j] = nvalid[j] == 16 && aligned16(gr, F.sr) && aligned16(go, F.so);
+        rv[j] = make_uint4(0, 0, 0, 0);
+        ov[j] = make_uint4(0, 0, 0, 0);
+        if (vec[j]) {
+            rv[j] = __ldcs((const uint4 *)gr);
+            ov[j] = __ldcs((const uint4 *)go);
+        } else if (nvalid[j] > 0) {
+            uint8_t rb[16] = {0}, ob[16] = {0};
+            for (int i = 0; i < nvalid[j]; ++i) { rb[i] = gr[i]; ob[i] = go[i]; }
+            rv[j] = pack16(rb);
+            ov[j] = pack16(ob);
+        }
     }
 #pragma unroll
     for (int b = 0; b < 32; ++b) hist[b][t] = 0;
@@ -182,28 +228,30 @@ __global__ void __launch_bounds__(FT) sao_frames_kernel(SaoJobs J) {
     // ---- pass 1: per-band (count, sum) and the unfiltered SSE
     int base = 0;
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-        if (i < nvalid) {
-            const int r = byte_of(rv, i), d = (int)byte_of(ov, i) - r;
-            base += d * d;
-            hist[r >> 3][t] += 65536 + d;
+    for (int j = 0; j < NSEG; ++j)
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            if (i < nvalid[j]) {
+                const int r = byte_of(rv[j], i), d = (int)byte_of(ov[j], i) - r;
+                base += d * d;
+                hist[r >> 3][t] += 65536 + d;
+            }
         }
-    }
     long long bsum = base;
     for (int o = 16; o > 0; o >>= 1) bsum += __shfl_xor_sync(0xffffffffu, bsum, o);
     if ((t & 31) == 0) red[t >> 5] = bsum;
     __syncthreads();
-    // ---- per-band totals: 8 threads per band, 32 columns each
+    // ---- per-band totals: TPB threads per band, SFT / TPB columns each
     {
-        const int b = t >> 3, part = t & 7;
+        const int b = t / TPB, part = t - b * TPB;
         int cnt = 0, sum = 0;
-        for (int j = part; j < FT; j += 8) {
+        for (int j = part; j < SFT; j += TPB) {
             const int v = hist[b][j];
-            const int s = (int)(int16_t)(v & 0xffff);
-            sum += s;
-            cnt += (v - s) >> 16;
+            const int sv = (int)(int16_t)(v & 0xffff);
+            sum += sv;
+            cnt += (v - sv) >> 16;
         }
-        for (int o = 1; o < 8; o <<= 1) {
+        for (int o = 1; o < TPB; o <<= 1) {
             cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
             sum += __shfl_xor_sync(0xffffffffu, sum, o);
         }
@@ -220,18 +268,20 @@ __global__ void __launch_bounds__(FT) sao_frames_kernel(SaoJobs J) {
         const int c_lo = cand_of(0), c_hi = cand_of(31);
         int lo = 0, hi = 0;
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            if (i < nvalid) {
-                const int r = byte_of(rv, i), o = byte_of(ov, i), d = o - r;
-                const int cand = r < 8 ? c_lo : (r >= 248 ? c_hi : 0);
-                const int v = r + cand;
-                if (cand && (v < 0 || v > 255)) {
-                    const int e = o - clampi(v, 0, 255);
-                    const int fix = (e * e - d * d) - (cand * cand - 2 * d * cand);
-                    if (r < 8) lo += fix; else hi += fix;
+        for (int j = 0; j < NSEG; ++j)
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                if (i < nvalid[j]) {
+                    const int r = byte_of(rv[j], i), o = byte_of(ov[j], i), d = o - r;
+                    const int cand = r < 8 ? c_lo : (r >= 248 ? c_hi : 0);
+                    const int v = r + cand;
+                    if (cand && (v < 0 || v > 255)) {
+                        const int e = o - clampi(v, 0, 255);
+                        const int fix = (e * e - d * d) - (cand * cand - 2 * d * cand);
+                        if (r < 8) lo += fix; else hi += fix;
+                    }
                 }
             }
-        }
         if (lo) atomicAdd(&corr[0], lo);
         if (hi) atomicAdd(&corr[31], hi);
     }
@@ -239,10 +289,10 @@ __global__ void __launch_bounds__(FT) sao_frames_kernel(SaoJobs J) {
     // ---- decision (warp 0): first band with the smallest SSE, rate gate
     if (t < 32) {
         long long b0 = 0;
-        for (int i = 0; i < FT / 32; ++i) b0 += red[i];
+        for (int i = 0; i < SFT / 32; ++i) b0 += red[i];
         const int cand = cand_of(t);
         long long sse = b0;
-        bool ok = band_cnt[t] > 0 && cand != 0;
+        const bool ok = band_cnt[t] > 0 && cand != 0;
         if (ok) sse = b0 - 2LL * cand * band_sum[t] + (long long)band_cnt[t] * cand * cand + corr[t];
         long long best = ok ? sse : b0;
         int bb = ok ? t : 32;
@@ -264,29 +314,26 @@ __global__ void __launch_bounds__(FT) sao_frames_kernel(SaoJobs J) {
         }
     }
     __syncthreads();
-    // ---- apply
-    if (dec[0] && nvalid > 0) {
+    // ---- apply (only segments holding pixels of the chosen band are written)
+    if (dec[0]) {
         const int band = dec[1], off = dec[2];
-        uint8_t nb[16];
-        bool any = false;
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            const int r = byte_of(rv, i);
-            const bool hit = i < nvalid && (r >> 3) == band;
-            nb[i] = hit ? (uint8_t)clampi(r + off, 0, 255) : (uint8_t)r;
-            any |= hit;
-        }
-        if (any) {
-            if (vec) {
-                uint4 o;
-                o.x = nb[0] | nb[1] << 8 | nb[2] << 16 | (uint32_t)nb[3] << 24;
-                o.y = nb[4] | nb[5] << 8 | nb[6] << 16 | (uint32_t)nb[7] << 24;
-                o.z = nb[8] | nb[9] << 8 | nb[10] << 16 | (uint32_t)nb[11] << 24;
-                o.w = nb[12] | nb[13] << 8 | nb[14] << 16 | (uint32_t)nb[15] << 24;
-                __stcs((uint4 *)gr, o);
-            } else {
-                for (int i = 0; i < nvalid; ++i) gr[i] = nb[i];
+        for (int j = 0; j < NSEG; ++j) {
+            if (nvalid[j] <= 0) continue;
+            const int sg = t + j * SFT, row = sg >> 2, c0 = (sg & 3) * 16;
+            uint8_t *gr = F.rec + (size_t)(y0 + row) * F.sr + x0 + c0;
+            uint8_t nb[16];
+            bool any = false;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int r = byte_of(rv[j], i);
+                const bool hit = i < nvalid[j] && (r >> 3) == band;
+                nb[i] = hit ? (uint8_t)clampi(r + off, 0, 255) : (uint8_t)r;
+                any |= hit;
             }
+            if (!any) continue;
+            if (vec[j]) __stcs((uint4 *)gr, pack16(nb));
+            else for (int i = 0; i < nvalid[j]; ++i) gr[i] = nb[i];
         }
     }
 }
@@ -307,7 +354,7 @@ cudaError_t launch_deblock_frames(const DeblockFrame *frames, int n, cudaStream_
         }
         J.ctu_off[J.n] = total;
         if (total > 0) {
-            deblock_frames_kernel<<<total, FT, 0, st>>>(J);
+            deblock_frames_kernel<<<total, DFT, 0, st>>>(J);
             const cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) return e;
         }
@@ -329,7 +376,7 @@ cudaError_t launch_sao_frames(const SaoFrame *frames, int n, cudaStream_t st) {
         }
         J.ctu_off[J.n] = total;
         if (total > 0) {
-            sao_frames_kernel<<<total, FT, 0, st>>>(J);
+            sao_frames_kernel<<<total, SFT, 0, st>>>(J);
             const cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) return e;
         }
