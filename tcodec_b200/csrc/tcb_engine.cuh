@@ -39,6 +39,17 @@ struct MeGroup {
     int mvx, mvy, best;
 };
 
+// Quarter-pel refinement window of one motion search (blocks up to 32x32):
+// source samples and the three half-sample planes the nine-anchor
+// interpolation combines, around the integer best (bx, by).
+constexpr int WIN_RAW = 40, WIN_PL = 35;   // raw: (blk+8)^2, planes: (blk+3)^2, blk <= 32
+struct MeWindow {
+    uint8_t raw[WIN_RAW * WIN_RAW];        // rows by-3.., cols bx-3..
+    int16_t hb[WIN_RAW * WIN_PL];          // horizontal half-pel, rows by-3.., cols bx-1..
+    int16_t cv[WIN_PL * WIN_PL];           // vertical half-pel, rows by-1.., cols bx-1..
+    int16_t dd[WIN_PL * WIN_PL];           // centre half-pel (h then v)
+};
+
 struct Smem {
     uint8_t cur_y[64 * 64];
     uint8_t cur_c[2][32 * 32];
@@ -55,8 +66,11 @@ struct Smem {
     uint8_t pred[NPRED][64 * 64];
     uint8_t cpred[4][32 * 32];
     uint8_t ra[2 * 64 + 4], rl[2 * 64 + 4];     // index i+1 holds ref[i], i in -1..2N
+    uint8_t ipred[18][32 * 32];                  // intra predictions of the current leaf (<= 32x32)
+    uint32_t ipred_ok;                           // modes held in ipred
     int scratch[NW][256];
     MeGroup me[NGROUP];
+    MeWindow win[NGROUP];
     int acc_sse[NCAND][2];
     int acc_bits[NCAND][2];
     long long acc64[4];
