@@ -95,6 +95,16 @@ void tc_config_defaults(tc_config_t *cfg, int32_t width, int32_t height);
 double tc_psnr(const tc_pixel_t *a, int stride_a,
                const tc_pixel_t *b, int stride_b, int width, int height);
 
+/* Packed RGB (3 bytes per pixel) to planar YCbCr 4:2:0 and back, BT.601
+ * full-range in 14-bit fixed point, chroma as the 2x2 box average
+ * (reference include/tcodec.h:130-142, src/color.c).  Host memory. */
+tc_error_t tc_rgb_to_ycbcr(const uint8_t *rgb, int rgb_stride,
+                           tc_pixel_t *y, int stride_y, tc_pixel_t *cb, int stride_cb,
+                           tc_pixel_t *cr, int stride_cr, int width, int height);
+tc_error_t tc_ycbcr_to_rgb(const tc_pixel_t *y, int stride_y, const tc_pixel_t *cb, int stride_cb,
+                           const tc_pixel_t *cr, int stride_cr, uint8_t *rgb, int rgb_stride,
+                           int width, int height);
+
 #ifdef __cplusplus
 }
 #endif

@@ -199,6 +199,23 @@ tc_error_t tcb_ctu_encode_frame(const tcb_frame_desc_t *desc, void *scratch, siz
 #define TCB_CTU_STATIC_MAX_CTUS 2048
 tc_error_t tcb_ctu_encode_frame_static(const tcb_frame_desc_t *desc, void *stream);
 
+/* One frame for standalone motion compensation.  Device pointers; the
+ * reference and prediction planes share stride_y / stride_c. */
+typedef struct tcb_mc_frame {
+    int width, height, stride_y, stride_c;
+    const tc_pixel_t *ref_y, *ref_cb, *ref_cr;
+    tc_pixel_t *pred_y, *pred_cb, *pred_cr;
+    const int16_t *mv;     /* ceil(W/8) * ceil(H/8) (dx, dy) pairs in quarter
+                              luma samples, raster order of the 8x8 blocks */
+} tcb_mc_frame_t;
+
+/* Motion-compensated prediction of n frames: every 8x8 luma block and its
+ * 4x4 chroma blocks predicted from the reference at the block's vector,
+ * exactly as tc_inter_predict / tc_inter_predict_chroma (reference
+ * src/motion.c:493-632) with an 8x8 block; samples beyond the frame are not
+ * written.  One launch per 32 frames. */
+tc_error_t tcb_mc_frames(const tcb_mc_frame_t *frames, int n, void *stream);
+
 /* One frame for the standalone in-loop filters.  Device pointers; the
  * reconstruction planes are filtered in place. */
 typedef struct tcb_filter_frame {

@@ -79,6 +79,7 @@ void tc_config_defaults(tc_config_t *cfg, int32_t width, int32_t height) {
 
 double tc_psnr(const tc_pixel_t *a, int stride_a, const tc_pixel_t *b, int stride_b, int width,
                int height) {
+    if (!a || !b || width <= 0 || height <= 0) return 0.0;
     int64_t sse = 0;
     for (int y = 0; y < height; ++y)
         for (int x = 0; x < width; ++x) {
@@ -88,6 +89,58 @@ double tc_psnr(const tc_pixel_t *a, int stride_a, const tc_pixel_t *b, int strid
     if (sse == 0) return 100.0;
     const double mse = (double)sse / ((double)width * (double)height);
     return 10.0 * log10(255.0 * 255.0 / mse);
+}
+
+// Colour conversion, BT.601 full range with 14-bit constants: the
+// format's colour matrix (reference src/color.c:20-40).
+namespace {
+inline uint8_t clip8(int v) { return (uint8_t)(v < 0 ? 0 : (v > 255 ? 255 : v)); }
+constexpr int kYR = 4899, kYG = 9617, kYB = 1868;
+constexpr int kBR = -2763, kBG = -5425, kBB = 8192;
+constexpr int kRR = 8192, kRG = -6855, kRB = -1327;
+constexpr int kIR = 22970, kIGB = -5638, kIGR = -11696, kIB = 29032;
+}  // namespace
+
+tc_error_t tc_rgb_to_ycbcr(const uint8_t *rgb, int rgb_stride, tc_pixel_t *y, int stride_y, tc_pixel_t *cb,
+                           int stride_cb, tc_pixel_t *cr, int stride_cr, int width, int height) {
+    if (!rgb || !y || !cb || !cr || width <= 0 || height <= 0) return TC_ERR_PARAM;
+    const int cw = width / 2, ch = height / 2;
+    for (int r = 0; r < height; ++r) {
+        const uint8_t *p = rgb + (size_t)r * rgb_stride;
+        for (int c = 0; c < width; ++c, p += 3)
+            y[(size_t)r * stride_y + c] = clip8((kYR * p[0] + kYG * p[1] + kYB * p[2] + 8192) >> 14);
+    }
+    // chroma: each 2x2 block's four (value + 128) summed, then / 4
+    for (int r = 0; r < ch; ++r)
+        for (int c = 0; c < cw; ++c) {
+            int sb = 0, sr = 0;
+            for (int dy = 0; dy < 2; ++dy)
+                for (int dx = 0; dx < 2; ++dx) {
+                    const uint8_t *p = rgb + (size_t)(2 * r + dy) * rgb_stride + (size_t)(2 * c + dx) * 3;
+                    sb += ((kBR * p[0] + kBG * p[1] + kBB * p[2] + 8192) >> 14) + 128;
+                    sr += ((kRR * p[0] + kRG * p[1] + kRB * p[2] + 8192) >> 14) + 128;
+                }
+            cb[(size_t)r * stride_cb + c] = clip8(sb / 4);
+            cr[(size_t)r * stride_cr + c] = clip8(sr / 4);
+        }
+    return TC_OK;
+}
+
+tc_error_t tc_ycbcr_to_rgb(const tc_pixel_t *y, int stride_y, const tc_pixel_t *cb, int stride_cb,
+                           const tc_pixel_t *cr, int stride_cr, uint8_t *rgb, int rgb_stride, int width,
+                           int height) {
+    if (!y || !cb || !cr || !rgb || width <= 0 || height <= 0) return TC_ERR_PARAM;
+    for (int r = 0; r < height; ++r) {
+        uint8_t *p = rgb + (size_t)r * rgb_stride;
+        for (int c = 0; c < width; ++c, p += 3) {
+            const int Y = y[(size_t)r * stride_y + c];
+            const int U = cb[(size_t)(r / 2) * stride_cb + c / 2] - 128, V = cr[(size_t)(r / 2) * stride_cr + c / 2] - 128;
+            p[0] = clip8(Y + ((kIR * V + 8192) >> 14));
+            p[1] = clip8(Y + ((kIGB * U + kIGR * V + 8192) >> 14));
+            p[2] = clip8(Y + ((kIB * U + 8192) >> 14));
+        }
+    }
+    return TC_OK;
 }
 
 }  // extern "C"

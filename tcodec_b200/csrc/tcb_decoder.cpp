@@ -678,7 +678,15 @@ void tc_decoder_destroy(tc_decoder_t *dec) {
 tc_error_t tc_decoder_decode(tc_decoder_t *dec, const uint8_t *data, size_t size, const tc_pixel_t **y,
                              int *stride_y, const tc_pixel_t **cb, int *stride_cb, const tc_pixel_t **cr,
                              int *stride_cr) {
-    if (!dec || !dec->impl || !data) return TC_ERR_PARAM;
+    // no frame unless one is output: callers that ignore the status read
+    // NULL planes rather than stale pointers
+    if (y) *y = nullptr;
+    if (cb) *cb = nullptr;
+    if (cr) *cr = nullptr;
+    if (stride_y) *stride_y = 0;
+    if (stride_cb) *stride_cb = 0;
+    if (stride_cr) *stride_cr = 0;
+    if (!dec || !dec->impl || !data || size == 0) return TC_ERR_PARAM;
     if (cudaSetDevice(dec->impl->device) != cudaSuccess) return TC_ERR_INTERNAL;
     return dec->impl->decode(data, size, y, stride_y, cb, stride_cb, cr, stride_cr);
 }

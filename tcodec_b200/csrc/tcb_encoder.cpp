@@ -748,6 +748,7 @@ void tc_encoder_destroy(tc_encoder_t *enc) {
 tc_error_t tc_encoder_encode(tc_encoder_t *enc, const tc_pixel_t *y, int stride_y,
                              const tc_pixel_t *cb, int stride_cb, const tc_pixel_t *cr,
                              int stride_cr, tc_packet_t *packet_out) {
+    if (packet_out) memset(packet_out, 0, sizeof(*packet_out));   // empty unless a packet is produced
     if (!enc || !enc->impl || !y || !cb || !cr || !packet_out) return TC_ERR_PARAM;
     EncImpl &e = *enc->impl;
     if (cudaSetDevice(e.device) != cudaSuccess) return TC_ERR_INTERNAL;
@@ -758,6 +759,7 @@ tc_error_t tc_encoder_encode(tc_encoder_t *enc, const tc_pixel_t *y, int stride_
 tc_error_t tcb_encoder_encode_device(tc_encoder_t *enc, const tc_pixel_t *d_y, int stride_y,
                                      const tc_pixel_t *d_cb, int stride_cb, const tc_pixel_t *d_cr,
                                      int stride_cr, tc_packet_t *packet_out) {
+    if (packet_out) memset(packet_out, 0, sizeof(*packet_out));
     if (!enc || !enc->impl || !d_y || !d_cb || !d_cr || !packet_out) return TC_ERR_PARAM;
     EncImpl &e = *enc->impl;
     if (cudaSetDevice(e.device) != cudaSuccess) return TC_ERR_INTERNAL;
@@ -790,6 +792,7 @@ void tcb_encoder_set_recon_readback(tc_encoder_t *enc, int enabled) {
 }
 
 tc_error_t tc_encoder_flush_tail(tc_encoder_t *enc, tc_packet_t *packet_out) {
+    if (packet_out) memset(packet_out, 0, sizeof(*packet_out));
     if (!enc || !enc->impl || !packet_out) return TC_ERR_PARAM;
     EncImpl &e = *enc->impl;
     if (!e.bf_b_mode) return TC_ERR_EOF;

@@ -22,6 +22,10 @@ enum RcCtx {
     CTX_CHROMA_BASE = 86, CTX_MAX = 119
 };
 
+// Range-coder LPS probability per state and LPS state transition.
+extern const uint8_t kLpsProb[64];
+extern const uint8_t kNextLps[64];
+
 // MSB-first bit writer over a caller-owned buffer (reference
 // src/bitstream.c:40-136 semantics: bytes are zeroed as they are entered).
 struct BitWriter {

@@ -32,7 +32,7 @@ def test_library_built_and_loads():
     assert L.tc_version() == (0 << 16) | (1 << 8)
 
 
-@pytest.mark.parametrize("header", ["tcodec.h", "tcodec_b200.h"])
+@pytest.mark.parametrize("header", ["tcodec.h", "tcodec_b200.h", "tcodec_b200_common.h"])
 def test_every_declared_symbol_is_exported(header):
     names = _declared(header)
     assert names
