@@ -350,6 +350,69 @@ def run_forms(lib, mixed_specs, mixed_clips, served_specs, served_clips):
     return out
 
 
+# ---------------------------------------------------------------- standalone kernels
+def run_standalone_kernels(lib, peak, iters=8, frames=64):
+    """HBM roofline of the standalone frame kernels on `frames` 1920x1080
+    frames per call (inputs + outputs far larger than L2; L2 flushed
+    before every timed call): deblocking (3 bytes per pixel of full CTUs),
+    SAO (4 B/px: source + reconstruction read, reconstruction written) and
+    motion compensation (3 B/px: luma + chroma read and written) with a
+    uniform fractional vector (+2.5, +0.75) px and with random vectors."""
+    import torch
+    from tcodec_b200 import api
+    W_, H_, N = 1920, 1080, frames
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1)
+    y = torch.randint(0, 256, (N, H_, W_), dtype=torch.uint8, device="cuda", generator=g)
+    src = (y.int() + torch.randint(-5, 6, (N, H_, W_), device="cuda", generator=g)).clamp(0, 255).to(torch.uint8)
+    cb = torch.randint(0, 256, (N, H_ // 2, W_ // 2), dtype=torch.uint8, device="cuda", generator=g)
+    cr = torch.randint(0, 256, (N, H_ // 2, W_ // 2), dtype=torch.uint8, device="cuda", generator=g)
+    py, pcb, pcr = torch.empty_like(y), torch.empty_like(cb), torch.empty_like(cr)
+    nctu = ((W_ + 63) // 64) * ((H_ + 63) // 64)
+    par = torch.zeros(N, nctu * 3, dtype=torch.int16, device="cuda")
+    gw, gh = (W_ + 7) // 8, (H_ + 7) // 8
+    mv_glob = torch.tensor([10, 3], dtype=torch.int16, device="cuda").repeat(N, gh * gw, 1).contiguous()
+    mv_rand = torch.randint(-96, 97, (N, gh * gw, 2), dtype=torch.int16, device="cuda", generator=g)
+    ff = (api.FilterFrame * N)()
+    for i, f in enumerate(ff):
+        f.width, f.height, f.stride_y, f.stride_c, f.stride_src, f.qp = W_, H_, W_, W_ // 2, W_, 32
+        f.y, f.cb, f.cr = y[i].data_ptr(), cb[i].data_ptr(), cr[i].data_ptr()
+        f.src_y, f.sao_params = src[i].data_ptr(), par[i].data_ptr()
+
+    def mc_frames(mv):
+        m = (api.McFrame * N)()
+        for i, f in enumerate(m):
+            f.width, f.height, f.stride_y, f.stride_c = W_, H_, W_, W_ // 2
+            f.ref_y, f.ref_cb, f.ref_cr = src[i].data_ptr(), cb[i].data_ptr(), cr[i].data_ptr()
+            f.pred_y, f.pred_cb, f.pred_cr = py[i].data_ptr(), pcb[i].data_ptr(), pcr[i].data_ptr()
+            f.mv = mv[i].data_ptr()
+        return m
+
+    st = torch.cuda.current_stream()
+    flush = torch.empty(256 * 2 ** 20, dtype=torch.uint8, device="cuda")
+    out = {}
+    cases = (("tcb_deblock_frames", lib.tcb_deblock_frames, ff, 3.0 * W_ * (H_ // 64 * 64)),
+             ("tcb_sao_frames", lib.tcb_sao_frames, ff, 4.0 * W_ * H_),
+             ("tcb_mc_frames (uniform fractional vector)", lib.tcb_mc_frames, mc_frames(mv_glob), 3.0 * W_ * H_),
+             ("tcb_mc_frames (random vectors)", lib.tcb_mc_frames, mc_frames(mv_rand), 3.0 * W_ * H_))
+    for name, fn, arg, per_frame in cases:
+        ts = []
+        for _ in range(iters):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            if fn(arg, N, st.cuda_stream) != 0:
+                raise RuntimeError(f"{name} failed")
+            e1.record(st)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        t = sorted(ts[2:])[len(ts[2:]) // 2] / 1000.0
+        achieved = per_frame * N / t / 1e9
+        out[name] = {"frames_per_call": N, "ms": t * 1000.0, "algorithmic_bytes": per_frame * N,
+                     "achieved_gbs": achieved, "frac_of_hbm": achieved / peak}
+    return out
+
+
 # ---------------------------------------------------------------- B200 arm
 def run_b200(args, rank, world):
     """Batched pass (device-resident and host inputs) and a plain
@@ -483,6 +546,9 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the mixed-batch and served forms")
     ap.add_argument("--served-sessions", type=int, default=64)
+    ap.add_argument("--no-kernels", action="store_true", help="skip the standalone-kernel roofline section")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="only time the standalone frame kernels (deblock, SAO, motion compensation)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -515,6 +581,11 @@ def main():
         print(json.dumps(line))
         return
 
+    if args.kernels_only:
+        peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]) \
+            if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+        print(json.dumps(run_standalone_kernels(api_lib(), peak, iters=max(3, args.steps))))
+        return
     forms = not args.no_forms and world == 1
     if forms:
         from tcodec_b200 import synth
@@ -605,6 +676,8 @@ def main():
     }
     if forms:
         line["forms"] = run_forms(api_lib(), mixed_specs, mixed_clips, served_specs, served_clips)
+    if not args.no_kernels and world == 1:
+        line["standalone_kernels"] = run_standalone_kernels(api_lib(), peak)
     if not args.no_cpu_baseline:
         try:
             from oracle import tcref

@@ -288,6 +288,22 @@ class FrameDesc(ctypes.Structure):
                 ("global_mv_y", ctypes.c_int)]
 
 
+class FilterFrame(ctypes.Structure):
+    """tcb_filter_frame_t: one frame for tcb_deblock_frames / tcb_sao_frames."""
+    _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("stride_y", ctypes.c_int),
+                ("stride_c", ctypes.c_int), ("y", ctypes.c_void_p), ("cb", ctypes.c_void_p), ("cr", ctypes.c_void_p),
+                ("src_y", ctypes.c_void_p), ("stride_src", ctypes.c_int), ("qp", ctypes.c_int),
+                ("sao_params", ctypes.c_void_p)]
+
+
+class McFrame(ctypes.Structure):
+    """tcb_mc_frame_t: one frame for tcb_mc_frames."""
+    _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("stride_y", ctypes.c_int),
+                ("stride_c", ctypes.c_int), ("ref_y", ctypes.c_void_p), ("ref_cb", ctypes.c_void_p),
+                ("ref_cr", ctypes.c_void_p), ("pred_y", ctypes.c_void_p), ("pred_cb", ctypes.c_void_p),
+                ("pred_cr", ctypes.c_void_p), ("mv", ctypes.c_void_p)]
+
+
 def bind_b200(lib: ctypes.CDLL) -> ctypes.CDLL:
     """Attach argtypes of the include/tcodec_b200.h encoder extensions."""
     vp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)
@@ -321,6 +337,11 @@ def bind_b200(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.tcb_ctu_encode_frame.restype = ctypes.c_int
     lib.tcb_ctu_encode_frame_static.argtypes = [ctypes.POINTER(FrameDesc), vp]
     lib.tcb_ctu_encode_frame_static.restype = ctypes.c_int
+    for fn in (lib.tcb_deblock_frames, lib.tcb_sao_frames):
+        fn.argtypes = [ctypes.POINTER(FilterFrame), ctypes.c_int, vp]
+        fn.restype = ctypes.c_int
+    lib.tcb_mc_frames.argtypes = [ctypes.POINTER(McFrame), ctypes.c_int, vp]
+    lib.tcb_mc_frames.restype = ctypes.c_int
     return lib
 
 

@@ -38,7 +38,7 @@ namespace {
 #define TCB_DEBLOCK_FT 128
 #endif
 #ifndef TCB_SAO_FT
-#define TCB_SAO_FT 64
+#define TCB_SAO_FT 128
 #endif
 constexpr int DFT = TCB_DEBLOCK_FT, SFT = TCB_SAO_FT;
 static_assert(384 % DFT == 0 && DFT >= 32, "deblock CTA: 384 16-byte pieces per CTU");
@@ -100,10 +100,14 @@ __global__ void __launch_bounds__(DFT) deblock_frames_kernel(DeblockJobs J) {
     __syncthreads();
     const int qp = F.qp, ltc = clampi(qp / 3, 1, 10);
     const int cqp = clampi(qp - 1, 0, 63), ctc = clampi(cqp / 4, 1, 6);
-    // ---- vertical edges: luma x = 4..60 (rows 0..63), Cb x = 4..28
-    for (int i = t; i < 15 * 64 + 7 * 32; i += DFT) {
-        if (i < 15 * 64) {
-            const int r = i / 15, x = (i - r * 15 + 1) * 4;
+    // ---- vertical edges: luma x = 4..60 (rows 0..63), Cb x = 4..28; items
+    // are (row, edge) on 16 / 8 slots per row so the decode is shifts and
+    // slot 0 (no edge) idles
+    for (int i = t; i < 16 * 64 + 8 * 32; i += DFT) {
+        if (i < 16 * 64) {
+            const int r = i >> 4, e = i & 15;
+            if (e == 0) continue;
+            const int x = e * 4;
             uint8_t *p = &ty[r * 64 + x];
             const int p1 = p[-2], p0 = p[-1], q0 = p[0], q1 = p[1];
             if (edge_strength(p0, q0, qp)) {
@@ -111,7 +115,9 @@ __global__ void __launch_bounds__(DFT) deblock_frames_kernel(DeblockJobs J) {
                 p[0] = (uint8_t)weak_filter(q1, q0, p0, p1, ltc);
             }
         } else {
-            const int j = i - 15 * 64, r = j / 7, x = (j - r * 7 + 1) * 4;
+            const int j = i - 16 * 64, r = j >> 3, e = j & 7;
+            if (e == 0) continue;
+            const int x = e * 4;
             uint8_t *p = &tc[0][r * 32 + x];
             const int p0 = p[-1], q0 = p[0];
             if (edge_strength(p0, q0, cqp)) {
@@ -126,7 +132,7 @@ __global__ void __launch_bounds__(DFT) deblock_frames_kernel(DeblockJobs J) {
     // e = 1..7, with the Cr strength deciding for both planes
     for (int i = t; i < 15 * 64 + 7 * 32; i += DFT) {
         if (i < 15 * 64) {
-            const int y = (i / 64 + 1) * 4, c = i & 63;
+            const int y = ((i >> 6) + 1) * 4, c = i & 63;
             uint8_t *p = &ty[y * 64 + c];
             const int p1 = p[-128], p0 = p[-64], q0 = p[0], q1 = p[64];
             if (edge_strength(p0, q0, qp)) {
@@ -134,7 +140,7 @@ __global__ void __launch_bounds__(DFT) deblock_frames_kernel(DeblockJobs J) {
                 p[0] = (uint8_t)weak_filter(q1, q0, p0, p1, ltc);
             }
         } else {
-            const int j = i - 15 * 64, y = (j / 32 + 1) * 4, c = j & 31;
+            const int j = i - 15 * 64, y = ((j >> 5) + 1) * 4, c = j & 31;
             uint8_t *pr = &tc[1][y * 32 + c], *pb = &tc[0][y * 32 + c];
             const int p0 = pr[0], q0 = pr[32], b0 = pb[0], b1 = pb[32];
             if (edge_strength(p0, q0, cqp)) {
@@ -225,22 +231,31 @@ __global__ void __launch_bounds__(SFT) sao_frames_kernel(SaoJobs J) {
 #pragma unroll
     for (int b = 0; b < 32; ++b) hist[b][t] = 0;
     if (t < 32) corr[t] = 0;
-    // ---- pass 1: per-band (count, sum) and the unfiltered SSE
+    // ---- pass 1: per-band (count, sum) and the unfiltered SSE (|d|^2
+    // four pixels at a time; padding bytes are zero in both vectors)
     int base = 0;
+    bool edge_band = false;                   // any pixel in band 0 or 31
 #pragma unroll
-    for (int j = 0; j < NSEG; ++j)
+    for (int j = 0; j < NSEG; ++j) {
+        const uint32_t rw[4] = {rv[j].x, rv[j].y, rv[j].z, rv[j].w}, ow[4] = {ov[j].x, ov[j].y, ov[j].z, ov[j].w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint32_t ad = __vabsdiffu4(rw[q], ow[q]);
+            base = (int)__dp4a(ad, ad, (unsigned)base);
+        }
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
             if (i < nvalid[j]) {
                 const int r = byte_of(rv[j], i), d = (int)byte_of(ov[j], i) - r;
-                base += d * d;
                 hist[r >> 3][t] += 65536 + d;
+                edge_band |= (unsigned)(r - 8) >= 240u;
             }
         }
+    }
     long long bsum = base;
     for (int o = 16; o > 0; o >>= 1) bsum += __shfl_xor_sync(0xffffffffu, bsum, o);
     if ((t & 31) == 0) red[t >> 5] = bsum;
-    __syncthreads();
+    const bool any_edge = __syncthreads_or(edge_band);
     // ---- per-band totals: TPB threads per band, SFT / TPB columns each
     {
         const int b = t / TPB, part = t - b * TPB;
@@ -264,7 +279,7 @@ __global__ void __launch_bounds__(SFT) sao_frames_kernel(SaoJobs J) {
         if (!cnt) return 0;
         return clampi((sum + (sum >= 0 ? cnt / 2 : -(cnt / 2))) / cnt, -7, 7);
     };
-    {
+    if (any_edge) {
         const int c_lo = cand_of(0), c_hi = cand_of(31);
         int lo = 0, hi = 0;
 #pragma unroll

@@ -7,26 +7,16 @@ import ctypes
 import numpy as np
 import pytest
 
+from tcodec_b200.api import FilterFrame
 from tests import orabind
 
 pytestmark = pytest.mark.gpu
 
 
-class FilterFrame(ctypes.Structure):
-    _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("stride_y", ctypes.c_int),
-                ("stride_c", ctypes.c_int), ("y", ctypes.c_void_p), ("cb", ctypes.c_void_p), ("cr", ctypes.c_void_p),
-                ("src_y", ctypes.c_void_p), ("stride_src", ctypes.c_int), ("qp", ctypes.c_int),
-                ("sao_params", ctypes.c_void_p)]
-
-
 @pytest.fixture(scope="module")
 def lib():
     from tcodec_b200 import api
-    L = api.load_library()
-    for fn in (L.tcb_deblock_frames, L.tcb_sao_frames):
-        fn.argtypes = [ctypes.POINTER(FilterFrame), ctypes.c_int, ctypes.c_void_p]
-        fn.restype = ctypes.c_int
-    return L
+    return api.bind_b200(api.load_library())
 
 
 def blocky(rng, h, w, step):

@@ -8,22 +8,15 @@ import ctypes
 import numpy as np
 import pytest
 
+from tcodec_b200.api import McFrame
 from tests import orabind
 
 pytestmark = pytest.mark.gpu
 
 
-class McFrame(ctypes.Structure):
-    _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("stride_y", ctypes.c_int),
-                ("stride_c", ctypes.c_int), ("ref_y", ctypes.c_void_p), ("ref_cb", ctypes.c_void_p),
-                ("ref_cr", ctypes.c_void_p), ("pred_y", ctypes.c_void_p), ("pred_cb", ctypes.c_void_p),
-                ("pred_cr", ctypes.c_void_p), ("mv", ctypes.c_void_p)]
-
-
 def bind(lib):
-    lib.tcb_mc_frames.argtypes = [ctypes.POINTER(McFrame), ctypes.c_int, ctypes.c_void_p]
-    lib.tcb_mc_frames.restype = ctypes.c_int
-    return lib
+    from tcodec_b200 import api
+    return api.bind_b200(lib)
 
 
 def make_case(rng, w, h, pad, kind):
@@ -55,7 +48,6 @@ def run_gpu(lib, cases):
     for f, c in zip(frames, cases):
         w, h, pad = c["w"], c["h"], c["pad"]
         ry, rcb, rcr = (torch.from_numpy(padded(c[k], pad)).cuda() for k in ("y", "cb", "cr"))
-        # chroma planes share stride_c = stride_y / 2 rounded down to an even pad
         py = torch.full_like(ry, 7)
         pcb, pcr = torch.full_like(rcb, 7), torch.full_like(rcr, 7)
         tmv = torch.from_numpy(np.ascontiguousarray(c["mv"])).cuda()
