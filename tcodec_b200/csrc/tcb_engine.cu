@@ -398,10 +398,11 @@ __device__ __forceinline__ int lpred(const Smem &S, int cu, int slot, int dc, in
 
 // Luma residual jobs, 8x8 TUs: one octet per (candidate, TU).
 __device__ void luma_jobs8(Smem &S, const Leaf &L, const int *cl, int ncl, const QuantParams &qp,
-                           bool accum, bool wrec, int16_t *emit) {
+                           bool accum, bool wrec, int16_t *emit, int woff = 0) {
     const int cu = L.cu, ntu = cu >> 3, ntu2 = ntu * ntu, J = ncl * ntu2;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, oct = lane >> 3, l8 = lane & 7;
-    int *scr = S.scratch[warp] + oct * 64;
+    const int hw = threadIdx.x >> 5, lane = threadIdx.x & 31, oct = lane >> 3, l8 = lane & 7;
+    const int warp = (hw + NW - woff % NW) % NW;   // job rank of this warp
+    int *scr = S.scratch[hw] + oct * 64;
     const int dc = S.dc;
     for (int base = 0; base < J; base += NW * 4) {
         const int j = base + warp * 4 + oct;
@@ -441,10 +442,11 @@ __device__ void luma_jobs8(Smem &S, const Leaf &L, const int *cl, int ncl, const
 // (candidate, TU, sub-block); the sub-block-0 quad adds the outer flag bit
 // (reference src/encoder.c:508-535).
 __device__ void luma_jobs4(Smem &S, const Leaf &L, const int *cl, int ncl, const QuantParams &qp,
-                           bool accum, bool wrec, int16_t *emit) {
+                           bool accum, bool wrec, int16_t *emit, int woff = 0) {
     const int cu = L.cu, ntu = cu >> 3, ntu2 = ntu * ntu, per = ntu2 * 4, J = ncl * per;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, qd = lane >> 2, l4 = lane & 3;
-    int *scr = S.scratch[warp] + qd * 16;
+    const int hw = threadIdx.x >> 5, lane = threadIdx.x & 31, qd = lane >> 2, l4 = lane & 3;
+    const int warp = (hw + NW - woff % NW) % NW;   // job rank of this warp
+    int *scr = S.scratch[hw] + qd * 16;
     const int dc = S.dc;
     for (int base = 0; base < J; base += NW * 8) {
         const int j = base + warp * 8 + qd;
@@ -486,11 +488,12 @@ __device__ void luma_jobs4(Smem &S, const Leaf &L, const int *cl, int ncl, const
 // 4x4 TUs, one quad per (option, component, TU).  Option o, component c
 // predicts from S.cpred[cbase + 2*o + c]; results accumulate in slot o.
 __device__ void chroma_jobs(Smem &S, const Leaf &L, int nopt, int cbase, const QuantParams &qp,
-                            bool accum, bool wrec, int16_t *emit) {
+                            bool accum, bool wrec, int16_t *emit, int woff = 0) {
     const int cs = L.cu >> 1, nt = cs >> 2, nt2 = nt * nt, per = 2 * nt2, J = nopt * per;
     const int lxc = L.lx >> 1, lyc = L.ly >> 1;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, qd = lane >> 2, l4 = lane & 3;
-    int *scr = S.scratch[warp] + qd * 16;
+    const int hw = threadIdx.x >> 5, lane = threadIdx.x & 31, qd = lane >> 2, l4 = lane & 3;
+    const int warp = (hw + NW - woff % NW) % NW;   // job rank of this warp
+    int *scr = S.scratch[hw] + qd * 16;
     for (int base = 0; base < J; base += NW * 8) {
         const int j = base + warp * 8 + qd;
         const bool act = j < J;
@@ -833,6 +836,11 @@ __device__ void leaf_code(Smem &S, const FrameParams &P, const Leaf &L, const Qu
                 S.cl2[0] = 0;
             }
             SYNC();
+            // Chroma prediction does not depend on this leaf's luma, so both
+            // predictions are formed first and the luma and chroma residual
+            // jobs then run side by side on different warps.
+            if (nd.ch_intra || cflat) chroma_dc_pred(S, L, 0);
+            else chroma_mc_bi(S, P, L, cr1, cr2, mvx, mvy);
             if (flat) {
                 for (int i = threadIdx.x; i < cu * cu; i += NT) S.pred[0][i] = 128;
                 SYNC();
@@ -840,12 +848,11 @@ __device__ void leaf_code(Smem &S, const FrameParams &P, const Leaf &L, const Qu
                 const int slots[1] = {0};
                 luma_mc_slots(S, P, L, 1, slots);
             }
+            const int ntu = cu >> 3;
+            const int wl = nd.dct_size ? mini(NW, (ntu * ntu + 3) / 4) : mini(NW, (ntu * ntu * 4 + 7) / 8);
             if (nd.dct_size) luma_jobs8(S, L, S.cl2, 1, ql, false, true, el);
             else luma_jobs4(S, L, S.cl2, 1, ql, false, true, el);
-            SYNC();
-            if (nd.ch_intra || cflat) chroma_dc_pred(S, L, 0);
-            else chroma_mc_bi(S, P, L, cr1, cr2, mvx, mvy);
-            chroma_jobs(S, L, 1, 0, qc, false, true, ec);
+            chroma_jobs(S, L, 1, 0, qc, false, true, ec, wl);
         } else {
             coded = false;
             const int n = cu * cu;
@@ -1018,9 +1025,14 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
         sad_jobs(S, L, S.cl, ncl);
         SYNC();
     } else {
+        // The three job lists start on different warps so that small
+        // leaves spread them over the CTA instead of stacking them on the
+        // first warps (accumulation is by integer atomics: order-free).
+        const int ntu2 = (cu >> 3) * (cu >> 3);
+        const int w8 = mini(NW, (ncl * ntu2 + 3) / 4), w4 = use4 ? mini(NW, (ncl * ntu2 * 4 + 7) / 8) : 0;
         luma_jobs8(S, L, S.cl, ncl, ql, true, false, nullptr);
-        if (use4) luma_jobs4(S, L, S.cl, ncl, ql, true, false, nullptr);
-        if (n8only) luma_jobs8(S, L, S.cl2, n8only, ql, true, false, nullptr);
+        if (use4) luma_jobs4(S, L, S.cl, ncl, ql, true, false, nullptr, w8);
+        if (n8only) luma_jobs8(S, L, S.cl2, n8only, ql, true, false, nullptr, w8 + w4);
         SYNC();
         PHASE(3);
         if (is_p && medium) {
@@ -1469,14 +1481,18 @@ __device__ void encode_ctu(Smem &S, const FrameParams &P, int row, int col) {
     if (threadIdx.x == 0) { S.ncoef = 0; S.tu8mask = 0; }
     SYNC();
 
-    QuantParams ql, qc;
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-        ql.eff[b] = P.eff_l[b]; ql.rcp[b] = P.rcp_l[b];
-        qc.eff[b] = P.eff_c[b]; qc.rcp[b] = P.rcp_c[b];
+    // Quantiser parameters in shared memory: every residual job reads them
+    // at fixed offsets.
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < 4; ++b) {
+            S.qparam[0].set_band(b, P.eff_l[b], P.rcp_l[b]);
+            S.qparam[1].set_band(b, P.eff_c[b], P.rcp_c[b]);
+        }
+        S.qparam[0].lambda = P.lambda;
+        S.qparam[1].lambda = P.lambda_c;
     }
-    ql.lambda = P.lambda;
-    qc.lambda = P.lambda_c;
+    SYNC();
+    const QuantParams &ql = S.qparam[0], &qc = S.qparam[1];
 
     // ---- decide, then write in syntax order ----------------------------
     PHASE_T0();
@@ -2004,13 +2020,16 @@ decode_kernel(const FrameParams *__restrict__ params, const int *__restrict__ it
     for (int i = threadIdx.x; i < QT_NODES; i += NT) S.nodes[i] = rec->nodes[i];
     if (threadIdx.x == 0) { S.ncoef = 0; S.tu8mask = rec->tu8mask; }
     SYNC();
-    QuantParams ql, qc;
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-        ql.eff[b] = P.eff_l[b]; ql.rcp[b] = P.rcp_l[b];
-        qc.eff[b] = P.eff_c[b]; qc.rcp[b] = P.rcp_c[b];
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < 4; ++b) {
+            S.qparam[0].set_band(b, P.eff_l[b], P.rcp_l[b]);
+            S.qparam[1].set_band(b, P.eff_c[b], P.rcp_c[b]);
+        }
+        S.qparam[0].lambda = 0;
+        S.qparam[1].lambda = 0;
     }
-    ql.lambda = 0; qc.lambda = 0;
+    SYNC();
+    const QuantParams &ql = S.qparam[0], &qc = S.qparam[1];
     qt_dec<0>(S, P, ctu_x, ctu_y, 0, 0, rec->coef, ql, qc);
     SYNC();
     if (w == 64 && h == 64) deblock_tile(S, P.qp);

@@ -71,6 +71,7 @@ struct Smem {
     int scratch[NW][256];
     MeGroup me[NGROUP];
     MeWindow win[NGROUP];
+    QuantParams qparam[2];     // luma, chroma quantiser of the current CTU
     int acc_sse[NCAND][2];
     int acc_bits[NCAND][2];
     long long acc64[4];

@@ -55,8 +55,24 @@ static inline cudaError_t upload_dct_tables() {
 struct QuantParams {
     int eff[4];
     uint32_t rcp[4];
+    int off[4];           // eff / 3: quantiser rounding offset
+    int bias[4];          // eff / 6: centroid dequantiser bias
     long long lambda;     // RDOQ lambda
+    __host__ __device__ void set_band(int b, int e, uint32_t r) {
+        eff[b] = e; rcp[b] = r; off[b] = e / 3; bias[b] = e / 6;
+    }
 };
+
+// Frequency band of coefficient (row k, column col) of an N x N TU in
+// raster order: DC, first quarter, second quarter, rest (the raster-index
+// bands of freq_band).  With k a compile-time constant only the DC case
+// depends on col.
+template <int N>
+__device__ __forceinline__ int band_rc(int k, int col) {
+    if (k == 0) return col == 0 ? 0 : 1;
+    if (N == 8) return k < 2 ? 1 : (k < 4 ? 2 : 3);
+    return k < 2 ? 2 : 3;
+}
 
 __device__ __forceinline__ int oct_sum(int v) {
     v += __shfl_xor_sync(0xffffffffu, v, 4, 8);
@@ -81,19 +97,28 @@ __device__ __forceinline__ int quad_max(int v) {
     return v;
 }
 
-// Quantise + RDOQ-lite one coefficient at raster position `pos` of an
-// n-coefficient TU (reference src/encoder.c:333-355).
-__device__ __forceinline__ int quant_rdoq(int c, int pos, int n, const QuantParams &qp) {
-    const int band = freq_band(pos, n);
+// Quantise + RDOQ-lite one coefficient of band `band` (reference
+// src/encoder.c:333-355): dead-zone quantiser with offset eff / 3, then a
+// level of magnitude 1 is dropped when zero costs less.
+__device__ __forceinline__ int quant_rdoq(int c, int band, const QuantParams &qp) {
     const int eff = qp.eff[band];
-    int q = quant_coeff(c, eff, qp.rcp[band]);
+    const uint32_t rcp = qp.rcp[band];
+    const int off = qp.off[band];
+    int q = 0;
+    if (c > 0) q = udiv_rcp((uint32_t)(c + off), eff, rcp);
+    else if (c < 0) q = -udiv_rcp((uint32_t)(-c + off), eff, rcp);
     if (q == 1 || q == -1) {
-        const int dq = dequant_coeff(q, eff);
+        const int dq = q > 0 ? eff + qp.bias[band] : -eff - qp.bias[band];
         const long long dz = (long long)c * c + qp.lambda;
         const long long dk = (long long)(c - dq) * (c - dq) + 2 * qp.lambda;
         if (dz < dk) q = 0;
     }
     return q;
+}
+
+__device__ __forceinline__ int dequant_band(int q, int band, const QuantParams &qp) {
+    const int eff = qp.eff[band], bias = qp.bias[band];
+    return q > 0 ? q * eff + bias : (q < 0 ? q * eff - bias : 0);
 }
 
 // Bit-model term of one quantised level (reference src/encoder.c:360-370).
@@ -130,7 +155,7 @@ __device__ __forceinline__ int tu8_code(int l8, const int res_row[8], int *scr,
         for (int n = 0; n < 8; ++n) acc += c_dct8[k][n] * col[n];
         const int c = (int16_t)((acc + 8192) >> 14);
         const int pos = k * 8 + l8;
-        const int q = (int16_t)quant_rdoq(c, pos, 64, qp);
+        const int q = (int16_t)quant_rdoq(c, band_rc<8>(k, l8), qp);
         q_col[k] = q;
         if (q) { ++nz; last = pos; }
     }
@@ -146,7 +171,7 @@ __device__ __forceinline__ int tu8_code(int l8, const int res_row[8], int *scr,
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         const int pos = k * 8 + l8;
-        scr[pos] = (int16_t)dequant_coeff(q_col[k], qp.eff[freq_band(pos, 64)]);
+        scr[pos] = (int16_t)dequant_band(q_col[k], band_rc<8>(k, l8), qp);
     }
     __syncwarp();
     int row[8];
@@ -201,7 +226,7 @@ __device__ __forceinline__ int tu4_code(int l4, const int res_row[4], int *scr,
         for (int n = 0; n < 4; ++n) acc += c_dct4[k][n] * col[n];
         const int c = (int16_t)((acc + 8192) >> 14);
         const int pos = k * 4 + l4;
-        const int q = (int16_t)quant_rdoq(c, pos, 16, qp);
+        const int q = (int16_t)quant_rdoq(c, band_rc<4>(k, l4), qp);
         q_col[k] = q;
         if (q) { ++nz; last = pos; }
     }
@@ -216,7 +241,7 @@ __device__ __forceinline__ int tu4_code(int l4, const int res_row[4], int *scr,
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const int pos = k * 4 + l4;
-        scr[pos] = (int16_t)dequant_coeff(q_col[k], qp.eff[freq_band(pos, 16)]);
+        scr[pos] = (int16_t)dequant_band(q_col[k], band_rc<4>(k, l4), qp);
     }
     __syncwarp();
     int row[4];
