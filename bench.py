@@ -517,22 +517,32 @@ def api_lib():
     return api.bind_b200(api.load_library())
 
 
-def max_over_ranks(x, world):
+def _reduce(x, world, op):
     if world <= 1:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    dev = "cuda" if torch.distributed.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    torch.distributed.all_reduce(t, op=op)
     return float(t.item())
+
+
+def max_over_ranks(x, world):
+    """Slowest rank's time: the job's time."""
+    import torch
+    return _reduce(x, world, torch.distributed.ReduceOp.MAX if world > 1 else None)
 
 
 def sum_over_ranks(x, world):
-    if world <= 1:
-        return x
+    """All ranks' frames: the job's work."""
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(x, world, torch.distributed.ReduceOp.SUM if world > 1 else None)
+
+
+def job_throughput(frames_per_rank, ms_per_rank, world):
+    """Whole-job frames/s: every rank's frames over the slowest rank's
+    device time (ranks encode independent streams; weak scaling)."""
+    return sum_over_ranks(frames_per_rank, world) / (max_over_ranks(ms_per_rank, world) / 1000.0)
 
 
 def main():
