@@ -1069,102 +1069,79 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
 
     PHASE(4);
     // ---- in-order candidate scan (strict <, first minimum wins) ---------
-    if (tid == 0) {
+    // Each lane of warp 0 scores one candidate of the scan order (inter
+    // candidates, then the intra modes), then a warp argmin on (cost,
+    // position) picks the first minimum exactly as a sequential scan with
+    // strict < does.  The node takes the winner's fields, the others keep
+    // their defaults (a sequential scan leaves the same result because every
+    // candidate sets all the fields later candidates could have changed).
+    if (tid < 32) {
+        enum { C_NONE, C_P_ME0, C_P_ME1, C_P_GLB, C_P_TMP, C_P_MRG, C_P_SKIP,
+               C_B_DIR0, C_B_DIR1, C_B_M2, C_B_M3, C_B_M4, C_INTRA };
+        const int lane = tid;
         const long long lam = P.lambda;
-        long long best = (long long)1 << 60;
-        int b_intra = 0, b_skip = 0, b_merge = 0, b_dct = 1, b_ref = 0, b_bi = 0, b_mvdx = 0, b_mvdy = 0;
-        int b_imode = 1, best_imode = 1;
         const int base_x = mvpx + L.px * 4, base_y = mvpy + L.py * 4;
+        int kinds[6], nk = 0;
         if (is_b) {
-            for (int dir = 0; dir < 2; ++dir) {
-                if ((dir == 0 ? rf : rb) < 0) continue;
-                const int slot = K_B0 + dir;
-                const int dx = S.cand_mvx[slot] - base_x, dy = S.cand_mvy[slot] - base_y;
-                long long dl; int lb, dct = 1;
-                if (fast) {
-                    const long long sad = S.acc_sse[slot][0];
-                    dl = (sad * sad) / (long long)(cu * cu);
-                    lb = 3;
-                } else {
-                    dl = best_of(S, slot, use4, lam, lb, dct);
-                }
-                const long long cost = dl + lam * (6 + se_bits(dx) + se_bits(dy) + lb);
-                if (cost < best) { best = cost; b_dct = dct; b_mvdx = dx; b_mvdy = dy; b_ref = dir; b_bi = 0; }
-            }
+            if (rf >= 0) kinds[nk++] = C_B_DIR0;
+            if (rb >= 0) kinds[nk++] = C_B_DIR1;
             if (medium && !fast) {
-                const int order[3] = {2, 3, 4};
-                for (int i = 0; i < 3; ++i) {
-                    const int k = order[i];
-                    const bool ok = k == 2 ? (rf >= 0 && rb >= 0) : (k == 3 ? rf >= 0 : rb >= 0);
-                    if (!ok) continue;
-                    const int slot = K_B0 + k;
-                    const long long cost = (long long)S.acc_sse[slot][0] + lam * (6 + S.acc_bits[slot][0]);
-                    if (cost < best) {
-                        best = cost; b_merge = 1; b_mvdx = 0; b_mvdy = 0; b_dct = 1;
-                        b_ref = k == 4 ? 1 : 0; b_bi = k == 2 ? 1 : 0;
-                    }
-                }
+                if (rf >= 0 && rb >= 0) kinds[nk++] = C_B_M2;
+                if (rf >= 0) kinds[nk++] = C_B_M3;
+                if (rb >= 0) kinds[nk++] = C_B_M4;
             }
         } else if (is_p) {
-            // Explicit inter from the MVP centre.
-            {
-                const int dx = S.cand_mvx[K_ME0] - base_x, dy = S.cand_mvy[K_ME0] - base_y;
-                long long dl; int lb, dct = 1;
-                if (fast) {
-                    const long long sad = S.acc_sse[K_ME0][0];
-                    dl = (sad * sad) / (long long)(cu * cu);
-                    lb = 3;
-                } else {
-                    dl = best_of(S, K_ME0, use4, lam, lb, dct);
-                }
-                int bits = 6 + se_bits(dx) + se_bits(dy) + lb + (P.multiref ? 2 : 0);
-                const long long cost = dl + lam * bits;
-                if (cost < best) { best = cost; b_dct = dct; b_mvdx = dx; b_mvdy = dy; b_ref = 0; }
-            }
-            if (has_me1) {
-                const int dx = S.cand_mvx[K_ME1] - base_x, dy = S.cand_mvy[K_ME1] - base_y;
-                int lb, dct;
-                const long long dl = best_of(S, K_ME1, use4, lam, lb, dct);
-                const int bits = 8 + se_bits(dx) + se_bits(dy) + lb;
-                const long long cost = dl + lam * bits;
-                if (cost < best) { best = cost; b_dct = dct; b_mvdx = dx; b_mvdy = dy; b_ref = 1; }
-            }
-            if (has_glb) {
-                const int dx = S.cand_mvx[K_GLB] - base_x, dy = S.cand_mvy[K_GLB] - base_y;
-                int lb, dct;
-                const long long dl = best_of(S, K_GLB, use4, lam, lb, dct);
-                const int bits = 6 + se_bits(dx) + se_bits(dy) + lb + (P.multiref ? 1 : 0);
-                const long long cost = dl + lam * bits;
-                if (cost < best) { best = cost; b_dct = dct; b_mvdx = dx; b_mvdy = dy; b_ref = 0; }
-            }
-            if (has_tmp) {
-                const int dx = S.cand_mvx[K_TMP] - base_x, dy = S.cand_mvy[K_TMP] - base_y;
-                int lb, dct;
-                const long long dl = best_of(S, K_TMP, use4, lam, lb, dct);
-                const int bits = 6 + se_bits(dx) + se_bits(dy) + lb + (P.multiref ? 2 : 0);
-                const long long cost = dl + lam * bits;
-                if (cost < best) { best = cost; b_dct = dct; b_mvdx = dx; b_mvdy = dy; b_ref = 0; }
-            }
+            kinds[nk++] = C_P_ME0;
+            if (has_me1) kinds[nk++] = C_P_ME1;
+            if (has_glb) kinds[nk++] = C_P_GLB;
+            if (has_tmp) kinds[nk++] = C_P_TMP;
             if (medium) {
-                const long long dl = S.acc_sse[K_MRG][0];
-                const int bits = 6 + S.acc_bits[K_MRG][0];
-                const long long cost = dl + lam * bits;
-                if (cost < best) {
-                    best = cost; b_merge = 1; b_dct = 1; b_ref = 0;
-                    b_mvdx = S.cand_mvx[K_ME0] - base_x; b_mvdy = S.cand_mvy[K_ME0] - base_y;
-                }
-                if (P.ref_valid[0] && S.acc64[0] == 0 && S.acc64[1] == 0) {
-                    const long long cost_skip = lam * 2;
-                    if (cost_skip < best) {
-                        best = cost_skip; b_skip = 1; b_merge = 0; b_dct = 1; b_mvdx = 0; b_mvdy = 0; b_ref = 0;
-                    }
-                }
+                kinds[nk++] = C_P_MRG;
+                if (P.ref_valid[0] && S.acc64[0] == 0 && S.acc64[1] == 0) kinds[nk++] = C_P_SKIP;
             }
         }
-        if (try_intra) {
-            for (int k = ninter; k < ncl; ++k) {
-                const int slot = S.cl[k], m = slot - K_INTRA;
-                long long dl; int lb, dct = 1;
+        const int n = nk + (try_intra ? ncl - ninter : 0);
+        int kind = C_NONE, slot = 0;
+        if (lane < nk) kind = kinds[lane];
+        else if (lane < n) { kind = C_INTRA; slot = S.cl[ninter + lane - nk]; }
+        long long cost = (long long)1 << 60;   // no candidate: defaults, as the sequential scan
+        int f_intra = 0, f_skip = 0, f_merge = 0, f_bi = 0, f_dct = 1, f_ref = 0, f_mx = 0, f_my = 0, f_mode = 1;
+        auto explicit_inter = [&](int sl, int extra_bits, bool sad_proxy, int lb_proxy) {
+            const int dx = S.cand_mvx[sl] - base_x, dy = S.cand_mvy[sl] - base_y;
+            long long dl;
+            int lb, dct = 1;
+            if (sad_proxy) {
+                const long long sad = S.acc_sse[sl][0];
+                dl = (sad * sad) / (long long)(cu * cu);
+                lb = lb_proxy;
+            } else {
+                dl = best_of(S, sl, use4, lam, lb, dct);
+            }
+            cost = dl + lam * (extra_bits + se_bits(dx) + se_bits(dy) + lb);
+            f_dct = dct; f_mx = dx; f_my = dy;
+        };
+        switch (kind) {
+            case C_P_ME0: explicit_inter(K_ME0, 6 + (P.multiref ? 2 : 0), fast, 3); break;
+            case C_P_ME1: explicit_inter(K_ME1, 8, false, 0); f_ref = 1; break;
+            case C_P_GLB: explicit_inter(K_GLB, 6 + (P.multiref ? 1 : 0), false, 0); break;
+            case C_P_TMP: explicit_inter(K_TMP, 6 + (P.multiref ? 2 : 0), false, 0); break;
+            case C_P_MRG:
+                cost = (long long)S.acc_sse[K_MRG][0] + lam * (6 + S.acc_bits[K_MRG][0]);
+                f_merge = 1;
+                f_mx = S.cand_mvx[K_ME0] - base_x; f_my = S.cand_mvy[K_ME0] - base_y;
+                break;
+            case C_P_SKIP: cost = lam * 2; f_skip = 1; break;
+            case C_B_DIR0: explicit_inter(K_B0 + 0, 6, fast, 3); f_ref = 0; break;
+            case C_B_DIR1: explicit_inter(K_B0 + 1, 6, fast, 3); f_ref = 1; break;
+            case C_B_M2: case C_B_M3: case C_B_M4: {
+                const int k = kind == C_B_M2 ? 2 : (kind == C_B_M3 ? 3 : 4), sl = K_B0 + k;
+                cost = (long long)S.acc_sse[sl][0] + lam * (6 + S.acc_bits[sl][0]);
+                f_merge = 1; f_ref = k == 4 ? 1 : 0; f_bi = k == 2 ? 1 : 0;
+                break;
+            }
+            case C_INTRA: {
+                long long dl;
+                int lb, dct = 1;
                 if (fast) {
                     const long long sad = S.acc_sse[slot][0];
                     dl = (sad * sad) / (long long)(cu * cu);
@@ -1172,21 +1149,30 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
                 } else {
                     dl = best_of(S, slot, use4, lam, lb, dct);
                 }
-                const long long cost = dl + lam * (8 + lb);
-                if (cost < best) {
-                    best = cost; b_intra = 1; best_imode = m; b_dct = dct; b_skip = 0; b_merge = 0;
-                    b_mvdx = 0; b_mvdy = 0; b_ref = 0; b_bi = 0;
-                }
+                cost = dl + lam * (8 + lb);
+                f_intra = 1; f_mode = slot - K_INTRA; f_dct = dct;
+                break;
             }
-            if (b_intra) b_imode = best_imode;
+            default: break;
         }
-        Node &nd = S.nodes[qt_index(L.depth, L.cx, L.cy)];
-        nd.intra = (uint8_t)b_intra; nd.skip = (uint8_t)b_skip; nd.merge = (uint8_t)b_merge; nd.bi = (uint8_t)b_bi;
-        nd.intra_mode = (uint8_t)b_imode; nd.intra_cmode = 0; nd.ch_intra = 0;
-        nd.ref_sel = (uint8_t)b_ref; nd.dct_size = (uint8_t)b_dct;
-        nd.mvd_x = (int16_t)b_mvdx; nd.mvd_y = (int16_t)b_mvdy;
-        nd.split = 0;
-        S.best_cost = best;
+        // first minimum: smallest cost, then smallest scan position
+        long long bc = cost;
+        int bl = lane;
+        for (int o = 16; o > 0; o >>= 1) {
+            const long long oc = __shfl_xor_sync(0xffffffffu, bc, o);
+            const int ol = __shfl_xor_sync(0xffffffffu, bl, o);
+            if (oc < bc || (oc == bc && ol < bl)) { bc = oc; bl = ol; }
+        }
+        if (lane == bl) {
+            Node &nd = S.nodes[qt_index(L.depth, L.cx, L.cy)];
+            nd.intra = (uint8_t)f_intra; nd.skip = (uint8_t)f_skip; nd.merge = (uint8_t)f_merge;
+            nd.bi = (uint8_t)f_bi;
+            nd.intra_mode = (uint8_t)f_mode; nd.intra_cmode = 0; nd.ch_intra = 0;
+            nd.ref_sel = (uint8_t)f_ref; nd.dct_size = (uint8_t)f_dct;
+            nd.mvd_x = (int16_t)f_mx; nd.mvd_y = (int16_t)f_my;
+            nd.split = 0;
+            S.best_cost = bc;
+        }
     }
     SYNC();
 
