@@ -428,6 +428,7 @@ __device__ void luma_jobs8(Smem &S, const Leaf &L, const int *cl, int ncl, const
             const int d = (int)S.cur_y[(L.ly + y) * 64 + L.lx + x] - v;
             sse += d * d;
             if (act && wrec) RY(S, L.lx + x, L.ly + y) = (uint8_t)v;
+            if (act && accum && cu <= 16) S.crec[slot][0][y * cu + x] = (uint8_t)v;
             if (act && emit) emit[t * 64 + kk * 8 + l8] = (int16_t)qc[kk];
         }
         sse = oct_sum(sse);
@@ -474,6 +475,7 @@ __device__ void luma_jobs4(Smem &S, const Leaf &L, const int *cl, int ncl, const
             const int d = (int)S.cur_y[(L.ly + y) * 64 + L.lx + x] - v;
             sse += d * d;
             if (act && wrec) RY(S, L.lx + x, L.ly + y) = (uint8_t)v;
+            if (act && accum && cu <= 16) S.crec[slot][1][y * cu + x] = (uint8_t)v;
             if (act && emit) emit[t * 64 + q * 16 + kk * 4 + l4] = (int16_t)qc[kk];
         }
         sse = quad_sum(sse);
@@ -774,8 +776,19 @@ __device__ void chroma_mc_bi(Smem &S, const FrameParams &P, const Leaf &L, int r
 // Leaf coding of a decided node: replay in the decide pass, syntax-order
 // coefficient emission in the write pass (reference src/encoder.c:587-781).
 // ====================================================================
+// The winner's luma reconstruction from the decide pass's cache (leaves up
+// to 16x16): the same samples its residual job produced when it was scored.
+__device__ void luma_from_cache(Smem &S, const Leaf &L, int slot, bool dct8) {
+    const int cu = L.cu;
+    const uint8_t *src = S.crec[slot][dct8 ? 0 : 1];
+    for (int i = threadIdx.x; i < cu * cu; i += NT) {
+        const int y = i / cu, x = i - y * cu;
+        RY(S, L.lx + x, L.ly + y) = src[i];
+    }
+}
+
 __device__ void leaf_code(Smem &S, const FrameParams &P, const Leaf &L, const QuantParams &ql,
-                          const QuantParams &qc, bool emit, CtuOut *out) {
+                          const QuantParams &qc, bool emit, CtuOut *out, bool use_cache = false) {
     const Node nd = S.nodes[qt_index(L.depth, L.cx, L.cy)];
     int mvpx, mvpy;
     mvp_at(S.grid, L.cx, L.cy, mvpx, mvpy);
@@ -784,11 +797,15 @@ __device__ void leaf_code(Smem &S, const FrameParams &P, const Leaf &L, const Qu
     int16_t *ec = emit ? el + cu * cu : nullptr;
     bool coded = true;
     if (nd.intra) {
-        build_refs(S, L, nd.intra_mode < 18 ? 1u << nd.intra_mode : 0u);
-        if (threadIdx.x == 0) { S.cl2[0] = K_INTRA + nd.intra_mode; }
-        SYNC();
-        if (nd.dct_size) luma_jobs8(S, L, S.cl2, 1, ql, false, true, el);
-        else luma_jobs4(S, L, S.cl2, 1, ql, false, true, el);
+        if (use_cache) {
+            luma_from_cache(S, L, K_INTRA + nd.intra_mode, nd.dct_size);
+        } else {
+            build_refs(S, L, nd.intra_mode < 18 ? 1u << nd.intra_mode : 0u);
+            if (threadIdx.x == 0) { S.cl2[0] = K_INTRA + nd.intra_mode; }
+            SYNC();
+            if (nd.dct_size) luma_jobs8(S, L, S.cl2, 1, ql, false, true, el);
+            else luma_jobs4(S, L, S.cl2, 1, ql, false, true, el);
+        }
         SYNC();
         if (nd.ch_intra) {
             chroma_dc_pred(S, L, 0);
@@ -841,18 +858,23 @@ __device__ void leaf_code(Smem &S, const FrameParams &P, const Leaf &L, const Qu
             // jobs then run side by side on different warps.
             if (nd.ch_intra || cflat) chroma_dc_pred(S, L, 0);
             else chroma_mc_bi(S, P, L, cr1, cr2, mvx, mvy);
-            if (flat) {
-                for (int i = threadIdx.x; i < cu * cu; i += NT) S.pred[0][i] = 128;
-                SYNC();
+            if (use_cache) {
+                luma_from_cache(S, L, S.win_slot, nd.dct_size);
+                chroma_jobs(S, L, 1, 0, qc, false, true, ec);
             } else {
-                const int slots[1] = {0};
-                luma_mc_slots(S, P, L, 1, slots);
+                if (flat) {
+                    for (int i = threadIdx.x; i < cu * cu; i += NT) S.pred[0][i] = 128;
+                    SYNC();
+                } else {
+                    const int slots[1] = {0};
+                    luma_mc_slots(S, P, L, 1, slots);
+                }
+                const int ntu = cu >> 3;
+                const int wl = nd.dct_size ? mini(NW, (ntu * ntu + 3) / 4) : mini(NW, (ntu * ntu * 4 + 7) / 8);
+                if (nd.dct_size) luma_jobs8(S, L, S.cl2, 1, ql, false, true, el);
+                else luma_jobs4(S, L, S.cl2, 1, ql, false, true, el);
+                chroma_jobs(S, L, 1, 0, qc, false, true, ec, wl);
             }
-            const int ntu = cu >> 3;
-            const int wl = nd.dct_size ? mini(NW, (ntu * ntu + 3) / 4) : mini(NW, (ntu * ntu * 4 + 7) / 8);
-            if (nd.dct_size) luma_jobs8(S, L, S.cl2, 1, ql, false, true, el);
-            else luma_jobs4(S, L, S.cl2, 1, ql, false, true, el);
-            chroma_jobs(S, L, 1, 0, qc, false, true, ec, wl);
         } else {
             coded = false;
             const int n = cu * cu;
@@ -1164,6 +1186,22 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
             if (oc < bc || (oc == bc && ol < bl)) { bc = oc; bl = ol; }
         }
         if (lane == bl) {
+            int ws = -1;
+            switch (kind) {
+                case C_P_ME0: ws = K_ME0; break;
+                case C_P_ME1: ws = K_ME1; break;
+                case C_P_GLB: ws = K_GLB; break;
+                case C_P_TMP: ws = K_TMP; break;
+                case C_P_MRG: ws = K_MRG; break;
+                case C_B_DIR0: ws = K_B0; break;
+                case C_B_DIR1: ws = K_B0 + 1; break;
+                case C_B_M2: ws = K_B0 + 2; break;
+                case C_B_M3: ws = K_B0 + 3; break;
+                case C_B_M4: ws = K_B0 + 4; break;
+                case C_INTRA: ws = slot; break;
+                default: ws = -1; break;
+            }
+            S.win_slot = ws;
             Node &nd = S.nodes[qt_index(L.depth, L.cx, L.cy)];
             nd.intra = (uint8_t)f_intra; nd.skip = (uint8_t)f_skip; nd.merge = (uint8_t)f_merge;
             nd.bi = (uint8_t)f_bi;
@@ -1180,10 +1218,14 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
     // ---- intra chroma choice: MC vs CfL-blended DC (src/encoder.c:1194-1221)
     const Node nd0 = S.nodes[qt_index(L.depth, L.cx, L.cy)];
     if (nd0.intra && !fast && medium) {
-        if (tid == 0) S.cl2[0] = K_INTRA + nd0.intra_mode;
-        SYNC();
-        if (nd0.dct_size) luma_jobs8(S, L, S.cl2, 1, ql, false, true, nullptr);
-        else luma_jobs4(S, L, S.cl2, 1, ql, false, true, nullptr);
+        if (cu <= 16) {
+            luma_from_cache(S, L, K_INTRA + nd0.intra_mode, nd0.dct_size);
+        } else {
+            if (tid == 0) S.cl2[0] = K_INTRA + nd0.intra_mode;
+            SYNC();
+            if (nd0.dct_size) luma_jobs8(S, L, S.cl2, 1, ql, false, true, nullptr);
+            else luma_jobs4(S, L, S.cl2, 1, ql, false, true, nullptr);
+        }
         SYNC();
         if (P.ref_valid[0]) chroma_mc(S, P, L, 0, mvpx + L.px * 4, mvpy + L.py * 4, 0, false);
         else chroma_dc_pred(S, L, 0);
@@ -1205,7 +1247,9 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
     const long long best = S.best_cost;
     PHASE(6);
     // ---- replay of the winner ------------------------------------------
-    leaf_code(S, P, L, ql, qc, false, nullptr);
+    // (luma from the scoring pass's cache where it holds the winner)
+    const Node ndw = S.nodes[qt_index(L.depth, L.cx, L.cy)];
+    leaf_code(S, P, L, ql, qc, false, nullptr, !fast && cu <= 16 && !ndw.skip && S.win_slot >= 0);
     PHASE(7);
     return best;
 }

@@ -72,6 +72,11 @@ struct Smem {
     MeGroup me[NGROUP];
     MeWindow win[NGROUP];
     QuantParams qparam[2];     // luma, chroma quantiser of the current CTU
+    // Luma reconstruction of every scored candidate of the current leaf
+    // (leaves up to 16x16), [slot][8x8 TUs, 4x4 TUs]: the replay of the
+    // winner copies it instead of coding the winner again.
+    uint8_t crec[NCAND][2][16 * 16];
+    int win_slot;              // candidate slot of the last scan's winner (-1: skip)
     int acc_sse[NCAND][2];
     int acc_bits[NCAND][2];
     long long acc64[4];
