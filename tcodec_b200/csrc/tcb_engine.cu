@@ -220,87 +220,6 @@ __device__ int group_subpel_sad(Smem &S, int g, int gt, const uint8_t *ref, int 
     return sum;
 }
 
-// Fills the group's refinement window around the integer best (bx, by).
-// Every quarter-pel point the refinement can visit lies within 3 quarter
-// samples of (4 bx, 4 by), so its integer part is in [bx-1, bx] x
-// [by-1, by] and the planes cover samples bx-1..bx+blk+1.  Reads are
-// clamped to the frame; entries that used clamped samples are read only by
-// points failing the six-tap margin test, which take the bilinear path
-// from the frame instead.
-__device__ void me_window_fill(Smem &S, int g, int gt, const uint8_t *ref, int s, int W, int H,
-                               int bx, int by, int blk) {
-    MeWindow &w = S.win[g];
-    const int nr = blk + 8, np = blk + 3;
-    for (int i = gt; i < nr * nr; i += GT) {
-        const int r = i / nr, c = i - r * nr;
-        const int y = clampi(by - 3 + r, 0, H - 1), x = clampi(bx - 3 + c, 0, W - 1);
-        w.raw[r * WIN_RAW + c] = __ldg(ref + (size_t)y * s + x);
-    }
-    group_bar(g);
-    for (int i = gt; i < nr * np + np * np; i += GT) {
-        if (i < nr * np) {                  // hb: raw rows 0..blk+7, taps at cols k..k+5
-            const int r = i / np, k = i - r * np;
-            const uint8_t *q = w.raw + r * WIN_RAW + k;
-            w.hb[r * WIN_PL + k] = (int16_t)((q[0] - 5 * q[1] + 20 * q[2] + 20 * q[3] - 5 * q[4] + q[5] + 16) >> 5);
-        } else {                            // cv: raw rows r..r+5 of col k+2
-            const int j = i - nr * np, r = j / np, k = j - r * np;
-            const uint8_t *q = w.raw + r * WIN_RAW + k + 2;
-            w.cv[r * WIN_PL + k] = (int16_t)((q[0] - 5 * q[WIN_RAW] + 20 * q[2 * WIN_RAW] + 20 * q[3 * WIN_RAW] -
-                                              5 * q[4 * WIN_RAW] + q[5 * WIN_RAW] + 16) >> 5);
-        }
-    }
-    group_bar(g);
-    for (int i = gt; i < np * np; i += GT) {  // dd: hb rows r..r+5
-        const int r = i / np, k = i - r * np;
-        const int16_t *q = w.hb + r * WIN_PL + k;
-        w.dd[r * WIN_PL + k] = (int16_t)((q[0] - 5 * q[WIN_PL] + 20 * q[2 * WIN_PL] + 20 * q[3 * WIN_PL] -
-                                          5 * q[4 * WIN_PL] + q[5 * WIN_PL] + 16) >> 5);
-    }
-    group_bar(g);
-}
-
-// Six-tap sub-pel SAD of one point from the group's window: the same result
-// as group_subpel_sad with six = true (reference src/motion.c:190-260).
-__device__ int group_subpel_sad_win(Smem &S, int g, int gt, const uint8_t *cur, int blk, int bx, int by,
-                                    int qx, int qy) {
-    const MeWindow &w = S.win[g];
-    const int fx = qx >> 2, fy = qy >> 2, dx = qx & 3, dy = qy & 3;
-    const int k0 = fx - (bx - 1), i0 = fy - (by - 1);
-    int acc = 0;
-    const int total = blk * blk;
-    for (int t = gt; t < total; t += GT) {
-        const int yy = t / blk, xx = t - yy * blk;
-        const int k = k0 + xx, i = i0 + yy;
-        const uint8_t *a = w.raw + (i + 2) * WIN_RAW + k + 2;
-        const int a00 = a[0], a10 = a[1], a01 = a[WIN_RAW], a11 = a[WIN_RAW + 1];
-        const int b = w.hb[(i + 2) * WIN_PL + k], e = w.hb[(i + 3) * WIN_PL + k];
-        const int c = w.cv[i * WIN_PL + k], f = w.cv[i * WIN_PL + k + 1], d = w.dd[i * WIN_PL + k];
-        int top, mid, bot;
-        switch (dx) {
-            case 0:  top = a00;               mid = c;               bot = a01; break;
-            case 1:  top = (a00 + b + 1) >> 1; mid = (c + d + 1) >> 1; bot = (a01 + e + 1) >> 1; break;
-            case 2:  top = b;                 mid = d;               bot = e; break;
-            default: top = (b + a10 + 1) >> 1; mid = (d + f + 1) >> 1; bot = (e + a11 + 1) >> 1; break;
-        }
-        int r;
-        switch (dy) {
-            case 0:  r = top; break;
-            case 1:  r = (top + mid + 1) >> 1; break;
-            case 2:  r = mid; break;
-            default: r = (mid + bot + 1) >> 1; break;
-        }
-        acc += absi((int)cur[yy * 64 + xx] - clampi(r, 0, 255));
-    }
-    acc = __reduce_add_sync(0xffffffffu, acc);
-    if ((gt & 31) == 0) S.me[g].part[gt >> 5][0] = acc;
-    group_bar(g);
-    int sum = 0;
-#pragma unroll
-    for (int q = 0; q < GT / 32; ++q) sum += S.me[g].part[q][0];
-    group_bar(g);
-    return sum;
-}
-
 __device__ void me_run(Smem &S, int g, int gt, const uint8_t *ref, int s, int W, int H,
                        int lx, int ly, int blk, int center_x, int center_y, int sr) {
     ME_T0();
@@ -317,15 +236,12 @@ __device__ void me_run(Smem &S, int g, int gt, const uint8_t *ref, int s, int W,
     // Quarter-pel refinement around the running best, first improvement
     // commits (reference src/motion.c:450-481).
     int mx = bx * 4, my = by * 4;
-    const bool win = blk <= 32;
-    if (win) me_window_fill(S, g, gt, ref, s, W, H, bx, by, blk);
     for (int p = 1; p < 9; ++p) {
         const int qx = mx + c_qpel[p][0], qy = my + c_qpel[p][1];
         const int fx = qx >> 2, fy = qy >> 2;
         if (fx < 0 || fy < 0 || fx + blk + 1 > W || fy + blk + 1 > H) continue;
         const bool six = fx >= 2 && fy >= 2 && fx + blk + 2 < W && fy + blk + 2 < H;
-        const int sad = (six && win) ? group_subpel_sad_win(S, g, gt, cur, blk, bx, by, qx, qy)
-                                     : group_subpel_sad(S, g, gt, ref, s, cur, blk, qx, qy, six);
+        const int sad = group_subpel_sad(S, g, gt, ref, s, cur, blk, qx, qy, six);
         if (sad < bsad) { bsad = sad; mx = qx; my = qy; }
     }
     ME_MARK(12);
@@ -338,7 +254,7 @@ __device__ void me_run(Smem &S, int g, int gt, const uint8_t *ref, int s, int W,
 
 // v2 intra reference samples (reference src/predict.c:480-520): above-right
 // and below-left are replicated.  S.ra[0] / S.rl[0] hold the corner.
-// For leaves up to 32x32 the predictions of the intra modes in `mode_mask`
+// For leaves up to IPRED_MAX the predictions of the intra modes in `mode_mask`
 // (DC excepted: it is the constant S.dc) are also evaluated once into
 // S.ipred, so residual jobs read them instead of re-deriving every sample.
 __device__ void build_refs(Smem &S, const Leaf &L, uint32_t mode_mask) {
@@ -364,7 +280,7 @@ __device__ void build_refs(Smem &S, const Leaf &L, uint32_t mode_mask) {
         S.rl[0] = (uint8_t)tl;
     }
     SYNC();
-    const uint32_t fill = N <= 32 ? (mode_mask & ~2u & ((1u << 18) - 1)) : 0u;
+    const uint32_t fill = N <= IPRED_MAX ? (mode_mask & ~2u & ((1u << 18) - 1)) : 0u;
     if (threadIdx.x < 32) {
         // DC value (reference src/predict.c:140-161): samples 1..N of each run.
         int sum = 0;

@@ -27,27 +27,21 @@ enum {
     K_GLB = 2,      // explicit inter, global-motion centre
     K_TMP = 3,      // explicit inter, temporal centre
     K_MRG = 4,      // merge at the MVP
-    K_B0 = 5,       // B: forward / backward / average / single merges (5..9)
-    K_INTRA = 10,   // intra modes 0..17 -> slots 10..27
-    NCAND = 28
+    K_B0 = 0,       // B: forward / backward / average / single merges (0..4;
+                    // B frames use no P slot, so the two sets share buffers)
+    K_INTRA = 5,    // intra modes 0..17 -> slots 5..22
+    NCAND = 23
 };
-constexpr int NPRED = 10;           // inter prediction buffers (slots 0..9)
+constexpr int NPRED = 5;
+#ifndef TCB_IPRED_MAX
+#define TCB_IPRED_MAX 32
+#endif
+constexpr int IPRED_MAX = TCB_IPRED_MAX;   // largest leaf whose intra predictions are kept            // inter prediction buffers (slots 0..4)
 
 struct MeGroup {
     int sad[8];
     int part[GT / 32][8];
     int mvx, mvy, best;
-};
-
-// Quarter-pel refinement window of one motion search (blocks up to 32x32):
-// source samples and the three half-sample planes the nine-anchor
-// interpolation combines, around the integer best (bx, by).
-constexpr int WIN_RAW = 40, WIN_PL = 35;   // raw: (blk+8)^2, planes: (blk+3)^2, blk <= 32
-struct MeWindow {
-    uint8_t raw[WIN_RAW * WIN_RAW];        // rows by-3.., cols bx-3..
-    int16_t hb[WIN_RAW * WIN_PL];          // horizontal half-pel, rows by-3.., cols bx-1..
-    int16_t cv[WIN_PL * WIN_PL];           // vertical half-pel, rows by-1.., cols bx-1..
-    int16_t dd[WIN_PL * WIN_PL];           // centre half-pel (h then v)
 };
 
 struct Smem {
@@ -66,11 +60,10 @@ struct Smem {
     uint8_t pred[NPRED][64 * 64];
     uint8_t cpred[4][32 * 32];
     uint8_t ra[2 * 64 + 4], rl[2 * 64 + 4];     // index i+1 holds ref[i], i in -1..2N
-    uint8_t ipred[18][32 * 32];                  // intra predictions of the current leaf (<= 32x32)
+    uint8_t ipred[18][IPRED_MAX * IPRED_MAX];    // intra predictions of the current leaf (<= IPRED_MAX)
     uint32_t ipred_ok;                           // modes held in ipred
     int scratch[NW][256];
     MeGroup me[NGROUP];
-    MeWindow win[NGROUP];
     QuantParams qparam[2];     // luma, chroma quantiser of the current CTU
     // Luma reconstruction of every scored candidate of the current leaf
     // (leaves up to 16x16), [slot][8x8 TUs, 4x4 TUs]: the replay of the
