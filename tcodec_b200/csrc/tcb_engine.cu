@@ -1515,6 +1515,9 @@ ctu_persistent_kernel(const FrameParams *__restrict__ params, const int *__restr
     Smem &S = *reinterpret_cast<Smem *>(smem_raw);
     __shared__ FrameParams P;
     __shared__ int s_item;
+#ifdef TCB_PHASE_PROFILE
+    const long long k0 = clock64();   // residency of the CTA (slot 14); neighbour waits in slot 13
+#endif
     for (;;) {
         if (threadIdx.x == 0) {
             const int i = atomicAdd(&ctrl[0], 1);
@@ -1522,7 +1525,12 @@ ctu_persistent_kernel(const FrameParams *__restrict__ params, const int *__restr
         }
         SYNC();
         const int item = s_item;
-        if (item < 0) break;
+        if (item < 0) {
+#ifdef TCB_PHASE_PROFILE
+            if (threadIdx.x == 0) atomicAdd(&tcb_phase_cycles[14], (unsigned long long)(clock64() - k0));
+#endif
+            break;
+        }
         const int row = (item >> 10) & 1023, col = item & 1023;
         if (threadIdx.x == 0) {
             P = params[item >> 20];
@@ -1531,11 +1539,17 @@ ctu_persistent_kernel(const FrameParams *__restrict__ params, const int *__restr
             const int *du = row > 0 ? P.done + (row - 1) * P.ctu_cols + col : nullptr;
             unsigned ns = 32;
             long long spins = 0;
+#ifdef TCB_PHASE_PROFILE
+            const long long w0 = clock64();
+#endif
             while ((dl && ld_acquire(dl) != epoch) || (du && ld_acquire(du) != epoch)) {
                 __nanosleep(ns);
                 if (ns < 2048) ns <<= 1;
                 if (++spins > (1ll << 22)) { atomicExch(&ctrl[1], 1); break; }
             }
+#ifdef TCB_PHASE_PROFILE
+            atomicAdd(&tcb_phase_cycles[13], (unsigned long long)(clock64() - w0));
+#endif
         }
         SYNC();
         encode_ctu(S, P, row, col);

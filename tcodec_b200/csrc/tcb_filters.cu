@@ -10,23 +10,27 @@
 //                          apply (src/filter.c:251-266); writes the chosen
 //                          (present, band, offset) of every CTU.
 //
-// Both are HBM-bound byte kernels: one 256-thread CTA per CTU, the tile
-// moved with 16-byte loads and stores (a byte path serves unaligned
-// planes), each byte read once and written at most once.
+// Both are byte kernels: one 128-thread CTA per CTU, the tile moved with
+// 16-byte loads and stores (a byte path serves unaligned planes), each byte
+// read once and written at most once.  Deblocking filters two edge
+// positions per instruction on packed 16-bit lanes (tcb_deblock_pairs.cuh).
 //
-// SAO statistics without atomics: every thread owns 16 pixels of one row
-// (kept in registers for the whole CTU) and a private column of a
-// [band][thread] table in shared memory, so its read-modify-writes never
+// SAO statistics without atomics: every thread owns two 16-pixel row
+// segments (kept in registers for the whole CTU) and a private column of a
+// [row][thread] table in shared memory, so its read-modify-writes never
 // conflict.  A table word packs count and difference sum as
-// count * 65536 + sum (|sum| <= 16 * 255), which one integer add per pixel
-// maintains exactly.  The per-band SSE after an offset follows in closed
-// form from (count, sum) and the unfiltered SSE; only pixels of bands 0 and
-// 31, where the offset can clip, get an exact per-pixel correction.
+// count * 65536 + sum (|sum| <= 32 * 255), which one integer add per pixel
+// maintains exactly.  Rows are the 30 inner bands plus the 16 single
+// sample values of bands 0 and 31, where an offset can clip; the SSE of
+// every band after its offset then follows in closed form, clipping
+// included (tcb_sao_decide.cuh), with no second pass over the pixels.
 #include <cuda_runtime.h>
 
 #include "tcb_common.cuh"
+#include "tcb_deblock_pairs.cuh"
 #include "tcb_filters.h"
 #include "tcb_pixel.cuh"
+#include "tcb_sao_decide.cuh"
 
 namespace tcb {
 
@@ -65,7 +69,8 @@ __global__ void __launch_bounds__(DFT) deblock_frames_kernel(DeblockJobs J) {
     const int x0 = (local % cols) << 6, y0 = (local / cols) << 6;
     const int t = threadIdx.x;
     uint8_t *gy = F.y + (size_t)y0 * F.sy + x0;
-    uint8_t *gc[2] = {F.cb + (size_t)(y0 >> 1) * F.sc + (x0 >> 1), F.cr + (size_t)(y0 >> 1) * F.sc + (x0 >> 1)};
+    uint8_t *const gcb = F.cb + (size_t)(y0 >> 1) * F.sc + (x0 >> 1), *const gcr = F.cr + (size_t)(y0 >> 1) * F.sc + (x0 >> 1);
+    auto gc = [&](int c) { return c ? gcr : gcb; };   // a select, not an indexed (local-memory) array
     const bool vec = aligned16(F.y, F.sy) && aligned16(F.cb, F.sc) && aligned16(F.cr, F.sc);
     // ---- load: 16-byte pieces 0..255 luma (row p>>2, segment p&3),
     // 256..383 chroma (plane, row, segment); all issued before any use
@@ -78,7 +83,7 @@ __global__ void __launch_bounds__(DFT) deblock_frames_kernel(DeblockJobs J) {
                 v[j] = __ldcs((const uint4 *)(gy + (size_t)(p >> 2) * F.sy + (p & 3) * 16));
             } else {
                 const int q = p - 256, c = q >> 6, r = (q >> 1) & 31, sg = q & 1;
-                v[j] = __ldcs((const uint4 *)(gc[c] + (size_t)r * F.sc + sg * 16));
+                v[j] = __ldcs((const uint4 *)(gc(c) + (size_t)r * F.sc + sg * 16));
             }
         }
 #pragma unroll
@@ -94,65 +99,18 @@ __global__ void __launch_bounds__(DFT) deblock_frames_kernel(DeblockJobs J) {
         for (int i = t; i < 64 * 64; i += DFT) ty[i] = gy[(size_t)(i >> 6) * F.sy + (i & 63)];
         for (int i = t; i < 2 * 32 * 32; i += DFT) {
             const int c = i >> 10, p = i & 1023;
-            tc[c][p] = gc[c][(size_t)(p >> 5) * F.sc + (p & 31)];
+            tc[c][p] = gc(c)[(size_t)(p >> 5) * F.sc + (p & 31)];
         }
     }
     __syncthreads();
-    const int qp = F.qp, ltc = clampi(qp / 3, 1, 10);
-    const int cqp = clampi(qp - 1, 0, 63), ctc = clampi(cqp / 4, 1, 6);
-    // ---- vertical edges: luma x = 4..60 (rows 0..63), Cb x = 4..28; items
-    // are (row, edge) on 16 / 8 slots per row so the decode is shifts and
-    // slot 0 (no edge) idles
-    for (int i = t; i < 16 * 64 + 8 * 32; i += DFT) {
-        if (i < 16 * 64) {
-            const int r = i >> 4, e = i & 15;
-            if (e == 0) continue;
-            const int x = e * 4;
-            uint8_t *p = &ty[r * 64 + x];
-            const int p1 = p[-2], p0 = p[-1], q0 = p[0], q1 = p[1];
-            if (edge_strength(p0, q0, qp)) {
-                p[-1] = (uint8_t)weak_filter(p1, p0, q0, q1, ltc);
-                p[0] = (uint8_t)weak_filter(q1, q0, p0, p1, ltc);
-            }
-        } else {
-            const int j = i - 16 * 64, r = j >> 3, e = j & 7;
-            if (e == 0) continue;
-            const int x = e * 4;
-            uint8_t *p = &tc[0][r * 32 + x];
-            const int p0 = p[-1], q0 = p[0];
-            if (edge_strength(p0, q0, cqp)) {
-                const int d = clampi((q0 - p0 + 1) >> 1, -ctc, ctc);
-                p[-1] = (uint8_t)clampi(p0 + d, 0, 255);
-                p[0] = (uint8_t)clampi(q0 - d, 0, 255);
-            }
-        }
-    }
+    // ---- vertical edges, then horizontal edges, as independent two-lane
+    // items (tcb_deblock_pairs.cuh): 640 vertical items (5 per thread at
+    // 128 threads), 296 horizontal
+    DeblockQp q;
+    q.init(F.qp);
+    for (int i = t; i < DEBLOCK_VERT_ITEMS; i += DFT) deblock_vert(ty, tc[0], i, q);
     __syncthreads();
-    // ---- horizontal edges: luma y = 4..60; chroma rows (4e, 4e+1),
-    // e = 1..7, with the Cr strength deciding for both planes
-    for (int i = t; i < 15 * 64 + 7 * 32; i += DFT) {
-        if (i < 15 * 64) {
-            const int y = ((i >> 6) + 1) * 4, c = i & 63;
-            uint8_t *p = &ty[y * 64 + c];
-            const int p1 = p[-128], p0 = p[-64], q0 = p[0], q1 = p[64];
-            if (edge_strength(p0, q0, qp)) {
-                p[-64] = (uint8_t)weak_filter(p1, p0, q0, q1, ltc);
-                p[0] = (uint8_t)weak_filter(q1, q0, p0, p1, ltc);
-            }
-        } else {
-            const int j = i - 15 * 64, y = ((j >> 5) + 1) * 4, c = j & 31;
-            uint8_t *pr = &tc[1][y * 32 + c], *pb = &tc[0][y * 32 + c];
-            const int p0 = pr[0], q0 = pr[32], b0 = pb[0], b1 = pb[32];
-            if (edge_strength(p0, q0, cqp)) {
-                int d = clampi((q0 - p0 + 1) >> 1, -ctc, ctc);
-                pr[0] = (uint8_t)clampi(p0 + d, 0, 255);
-                pr[32] = (uint8_t)clampi(q0 - d, 0, 255);
-                d = clampi((b1 - b0 + 1) >> 1, -ctc, ctc);
-                pb[0] = (uint8_t)clampi(b0 + d, 0, 255);
-                pb[32] = (uint8_t)clampi(b1 - d, 0, 255);
-            }
-        }
-    }
+    for (int i = t; i < DEBLOCK_HORIZ_ITEMS; i += DFT) deblock_horiz(ty, tc[0], tc[1], i, q);
     __syncthreads();
     // ---- store
     if (vec) {
@@ -163,40 +121,44 @@ __global__ void __launch_bounds__(DFT) deblock_frames_kernel(DeblockJobs J) {
                 __stcs((uint4 *)(gy + (size_t)(p >> 2) * F.sy + (p & 3) * 16), *(const uint4 *)&ty[p * 16]);
             } else {
                 const int q = p - 256, c = q >> 6, r = (q >> 1) & 31, sg = q & 1;
-                __stcs((uint4 *)(gc[c] + (size_t)r * F.sc + sg * 16), *(const uint4 *)&tc[c][r * 32 + sg * 16]);
+                __stcs((uint4 *)(gc(c) + (size_t)r * F.sc + sg * 16), *(const uint4 *)&tc[c][r * 32 + sg * 16]);
             }
         }
     } else {
         for (int i = t; i < 64 * 64; i += DFT) gy[(size_t)(i >> 6) * F.sy + (i & 63)] = ty[i];
         for (int i = t; i < 2 * 32 * 32; i += DFT) {
             const int c = i >> 10, p = i & 1023;
-            gc[c][(size_t)(p >> 5) * F.sc + (p & 31)] = tc[c][p];
+            gc(c)[(size_t)(p >> 5) * F.sc + (p & 31)] = tc[c][p];
         }
     }
 }
 
 // ---------------------------------------------------------------- SAO
 
-__device__ __forceinline__ uint8_t byte_of(const uint4 &v, int k) {
-    const uint32_t w = k < 8 ? (k < 4 ? v.x : v.y) : (k < 12 ? v.z : v.w);
-    return (uint8_t)(w >> ((k & 3) * 8));
+// Byte k (0..3) of w.
+__device__ __forceinline__ int byte_k(uint32_t w, int k) { return (int)__byte_perm(w, 0, 0x4440 | k); }
+// Byte i (0..15) of v, by selects (an indexed register array would live
+// in local memory).
+__device__ __forceinline__ int byte_i(const uint4 &v, int i) {
+    const uint32_t w = i < 8 ? (i < 4 ? v.x : v.y) : (i < 12 ? v.z : v.w);
+    return byte_k(w, i & 3);
 }
 
-// Packs bytes b[0..15] into a uint4 (little endian within each word).
-__device__ __forceinline__ uint4 pack16(const uint8_t *b) {
-    uint4 v;
-    v.x = b[0] | b[1] << 8 | b[2] << 16 | (uint32_t)b[3] << 24;
-    v.y = b[4] | b[5] << 8 | b[6] << 16 | (uint32_t)b[7] << 24;
-    v.z = b[8] | b[9] << 8 | b[10] << 16 | (uint32_t)b[11] << 24;
-    v.w = b[12] | b[13] << 8 | b[14] << 16 | (uint32_t)b[15] << 24;
-    return v;
+// One sample pair into the thread's statistics column: the word at
+// row_word[r] (the row's offset in the table) gains count 1 and o - r.
+__device__ __forceinline__ void sao_count(int *col, const int *row_word, int r, int o) {
+    col[row_word[r]] += 65536 + o - r;
 }
 
 __global__ void __launch_bounds__(SFT) sao_frames_kernel(SaoJobs J) {
     constexpr int NSEG = 256 / SFT;           // 16-pixel segments per thread
-    constexpr int TPB = SFT / 32;             // threads summing one band
-    __shared__ int hist[32][SFT];             // count * 65536 + sum, per thread
-    __shared__ int band_cnt[32], band_sum[32], corr[32];
+    // Four columns of the table are summed before unpacking: a column
+    // holds at most 16 * NSEG pixels, so four columns keep |sum| below
+    // 4 * 16 * NSEG * 255 = 32640 for NSEG = 2, inside the 16-bit field.
+    static_assert(SFT == 128, "SAO table reduction sized for 128 threads");
+    __shared__ __align__(16) int hist[SAO_ROWS][SFT];   // count * 65536 + sum of (org - rec), per thread
+    __shared__ int row_word[256];             // sample value -> word offset of its statistics row
+    __shared__ int row_cnt[SAO_ROWS], row_sum[SAO_ROWS];
     __shared__ long long red[SFT / 32];
     __shared__ int dec[3];
     const int k = find_frame(J.ctu_off, J.n, blockIdx.x);
@@ -222,19 +184,21 @@ __global__ void __launch_bounds__(SFT) sao_frames_kernel(SaoJobs J) {
             rv[j] = __ldcs((const uint4 *)gr);
             ov[j] = __ldcs((const uint4 *)go);
         } else if (nvalid[j] > 0) {
-            uint8_t rb[16] = {0}, ob[16] = {0};
-            for (int i = 0; i < nvalid[j]; ++i) { rb[i] = gr[i]; ob[i] = go[i]; }
-            rv[j] = pack16(rb);
-            ov[j] = pack16(ob);
+            uint32_t r4[4] = {0, 0, 0, 0}, o4[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                if (i < nvalid[j]) { r4[i >> 2] |= (uint32_t)gr[i] << (8 * (i & 3)); o4[i >> 2] |= (uint32_t)go[i] << (8 * (i & 3)); }
+            rv[j] = make_uint4(r4[0], r4[1], r4[2], r4[3]);
+            ov[j] = make_uint4(o4[0], o4[1], o4[2], o4[3]);
         }
     }
-#pragma unroll
-    for (int b = 0; b < 32; ++b) hist[b][t] = 0;
-    if (t < 32) corr[t] = 0;
-    // ---- pass 1: per-band (count, sum) and the unfiltered SSE (|d|^2
-    // four pixels at a time; padding bytes are zero in both vectors)
+    for (int i = t; i < 256; i += SFT) row_word[i] = sao_row_of(i) * SFT;
+    for (int i = t; i < SAO_ROWS * SFT / 4; i += SFT) ((int4 *)&hist[0][0])[i] = make_int4(0, 0, 0, 0);
+    __syncthreads();
+    // ---- pass 1: per-row (count, sum) and the unfiltered SSE (|d|^2 four
+    // pixels at a time; padding bytes are zero in both vectors)
+    int *col = &hist[0][t];
     int base = 0;
-    bool edge_band = false;                   // any pixel in band 0 or 31
 #pragma unroll
     for (int j = 0; j < NSEG; ++j) {
         const uint32_t rw[4] = {rv[j].x, rv[j].y, rv[j].z, rv[j].w}, ow[4] = {ov[j].x, ov[j].y, ov[j].z, ov[j].w};
@@ -243,85 +207,59 @@ __global__ void __launch_bounds__(SFT) sao_frames_kernel(SaoJobs J) {
             const uint32_t ad = __vabsdiffu4(rw[q], ow[q]);
             base = (int)__dp4a(ad, ad, (unsigned)base);
         }
+        if (nvalid[j] == 16) {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            if (i < nvalid[j]) {
-                const int r = byte_of(rv[j], i), d = (int)byte_of(ov[j], i) - r;
-                hist[r >> 3][t] += 65536 + d;
-                edge_band |= (unsigned)(r - 8) >= 240u;
-            }
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) sao_count(col, row_word, byte_k(rw[q], b), byte_k(ow[q], b));
+        } else {
+            for (int i = 0; i < nvalid[j]; ++i) sao_count(col, row_word, byte_i(rv[j], i), byte_i(ov[j], i));
         }
     }
     long long bsum = base;
     for (int o = 16; o > 0; o >>= 1) bsum += __shfl_xor_sync(0xffffffffu, bsum, o);
     if ((t & 31) == 0) red[t >> 5] = bsum;
-    const bool any_edge = __syncthreads_or(edge_band);
-    // ---- per-band totals: TPB threads per band, SFT / TPB columns each
-    {
-        const int b = t / TPB, part = t - b * TPB;
+    __syncthreads();
+    // ---- row totals: two threads per row, each summing 64 columns four at
+    // a time (16-byte loads) before unpacking
+    if (t < 2 * SAO_ROWS) {
+        const int row = t >> 1, half = t & 1;
+        const int4 *p = (const int4 *)&hist[row][half * (SFT / 2)];
         int cnt = 0, sum = 0;
-        for (int j = part; j < SFT; j += TPB) {
-            const int v = hist[b][j];
-            const int sv = (int)(int16_t)(v & 0xffff);
+#pragma unroll
+        for (int i = 0; i < SFT / 8; ++i) {
+            const int4 v = p[i];
+            const int x = v.x + v.y + v.z + v.w;
+            const int sv = (int)(int16_t)(x & 0xffff);
             sum += sv;
-            cnt += (v - sv) >> 16;
+            cnt += (x - sv) >> 16;
         }
-        for (int o = 1; o < TPB; o <<= 1) {
-            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-            sum += __shfl_xor_sync(0xffffffffu, sum, o);
-        }
-        if (part == 0) { band_cnt[b] = cnt; band_sum[b] = sum; }
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, 1);
+        sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+        if (!half) { row_cnt[row] = cnt; row_sum[row] = sum; }
     }
     __syncthreads();
-    // ---- pass 2: exact correction where the offset clips (bands 0, 31)
-    auto cand_of = [&](int b) {
-        const int cnt = band_cnt[b], sum = band_sum[b];
-        if (!cnt) return 0;
-        return clampi((sum + (sum >= 0 ? cnt / 2 : -(cnt / 2))) / cnt, -7, 7);
-    };
-    if (any_edge) {
-        const int c_lo = cand_of(0), c_hi = cand_of(31);
-        int lo = 0, hi = 0;
-#pragma unroll
-        for (int j = 0; j < NSEG; ++j)
-#pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                if (i < nvalid[j]) {
-                    const int r = byte_of(rv[j], i), o = byte_of(ov[j], i), d = o - r;
-                    const int cand = r < 8 ? c_lo : (r >= 248 ? c_hi : 0);
-                    const int v = r + cand;
-                    if (cand && (v < 0 || v > 255)) {
-                        const int e = o - clampi(v, 0, 255);
-                        const int fix = (e * e - d * d) - (cand * cand - 2 * d * cand);
-                        if (r < 8) lo += fix; else hi += fix;
-                    }
-                }
-            }
-        if (lo) atomicAdd(&corr[0], lo);
-        if (hi) atomicAdd(&corr[31], hi);
-    }
-    __syncthreads();
-    // ---- decision (warp 0): first band with the smallest SSE, rate gate
+    // ---- decision (warp 0): lane b scores band b; first band with the
+    // smallest SSE; rate gate of 6 lambda
     if (t < 32) {
         long long b0 = 0;
         for (int i = 0; i < SFT / 32; ++i) b0 += red[i];
-        const int cand = cand_of(t);
-        long long sse = b0;
-        const bool ok = band_cnt[t] > 0 && cand != 0;
-        if (ok) sse = b0 - 2LL * cand * band_sum[t] + (long long)band_cnt[t] * cand * cand + corr[t];
-        long long best = ok ? sse : b0;
-        int bb = ok ? t : 32;
+        int cand;
+        const long long sse = sao_band_sse(t, b0, row_cnt, row_sum, &cand);
+        long long best = cand ? sse : b0;
+        int bb = cand ? t : 32;
         for (int o = 16; o > 0; o >>= 1) {
             const long long ob = __shfl_xor_sync(0xffffffffu, best, o);
             const int obb = __shfl_xor_sync(0xffffffffu, bb, o);
-            if (ob < best || (ob == best && obb < bb)) { best = ob; bb = obb; }
+            const int oc = __shfl_xor_sync(0xffffffffu, cand, o);
+            if (ob < best || (ob == best && obb < bb)) { best = ob; bb = obb; cand = oc; }
         }
         if (t == 0) {
             int has = bb < 32 && best < b0;
             if (has && best + (long long)F.lambda_sao * 6 >= b0) has = 0;
             dec[0] = has;
             dec[1] = has ? bb : 0;
-            dec[2] = has ? cand_of(bb) : 0;
+            dec[2] = has ? cand : 0;
             if (F.params) {
                 int16_t *pp = F.params + 3 * local;
                 pp[0] = (int16_t)dec[0]; pp[1] = (int16_t)dec[1]; pp[2] = (int16_t)dec[2];
@@ -329,26 +267,40 @@ __global__ void __launch_bounds__(SFT) sao_frames_kernel(SaoJobs J) {
         }
     }
     __syncthreads();
-    // ---- apply (only segments holding pixels of the chosen band are written)
+    // ---- apply: bytes of the chosen band (exact per-byte test: band
+    // indices are <= 31, so adding 0x7F sets bit 7 of every nonzero byte
+    // without carries), offset on pairs; only segments with a hit are
+    // written
     if (dec[0]) {
-        const int band = dec[1], off = dec[2];
+        const uint32_t bandx4 = (uint32_t)dec[1] * 0x01010101u, one = 0x00010001u;
+        const uint32_t add = (uint32_t)(dec[2] + 128) * one, lo = 128u * one, hi = (128u + 255u) * one;
 #pragma unroll
         for (int j = 0; j < NSEG; ++j) {
             if (nvalid[j] <= 0) continue;
-            const int sg = t + j * SFT, row = sg >> 2, c0 = (sg & 3) * 16;
-            uint8_t *gr = F.rec + (size_t)(y0 + row) * F.sr + x0 + c0;
-            uint8_t nb[16];
+            uint32_t wv[4] = {rv[j].x, rv[j].y, rv[j].z, rv[j].w}, hit[4];
             bool any = false;
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                const int r = byte_of(rv[j], i);
-                const bool hit = i < nvalid[j] && (r >> 3) == band;
-                nb[i] = hit ? (uint8_t)clampi(r + off, 0, 255) : (uint8_t)r;
-                any |= hit;
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t tq = ((wv[q] >> 3) & 0x1F1F1F1Fu) ^ bandx4;
+                hit[q] = ~(tq + 0x7F7F7F7Fu) & 0x80808080u;
+                any |= hit[q] != 0;
             }
             if (!any) continue;
-            if (vec[j]) __stcs((uint4 *)gr, pack16(nb));
-            else for (int i = 0; i < nvalid[j]; ++i) gr[i] = nb[i];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t a = pair_min(pair_max(pair_lo(wv[q]) + add, lo), hi) - lo;
+                const uint32_t b = pair_min(pair_max(pair_hi(wv[q]) + add, lo), hi) - lo;
+                const uint32_t m = (hit[q] >> 7) * 0xFFu;
+                wv[q] = (pair_pack(a, b) & m) | (wv[q] & ~m);
+            }
+            const int sg = t + j * SFT, row = sg >> 2, c0 = (sg & 3) * 16;
+            uint8_t *gr = F.rec + (size_t)(y0 + row) * F.sr + x0 + c0;
+            if (vec[j]) {
+                __stcs((uint4 *)gr, make_uint4(wv[0], wv[1], wv[2], wv[3]));
+            } else {
+                const uint4 nv = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+                for (int i = 0; i < nvalid[j]; ++i) gr[i] = (uint8_t)byte_i(nv, i);
+            }
         }
     }
 }

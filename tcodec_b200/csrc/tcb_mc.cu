@@ -5,16 +5,18 @@
 // tc_inter_predict_chroma (src/motion.c:597-632: 1/8-sample bilinear with
 // clamped coordinates) applied to every 8x8 luma / 4x4 chroma block.
 //
-// One 256-thread CTA per 64x64 luma tile (64 blocks): four threads per
-// block, each producing two luma rows (8 bytes each, one 8-byte store) and
-// one row of each chroma plane (4 bytes each).  The sample arithmetic is
-// the CTU engine's (tcb_pixel.cuh), so predictions equal the encoder's.
+// Two threads per 8x8 block, blocks in raster order (a warp covers 16
+// neighbouring blocks, so its loads and stores are contiguous runs): thread
+// h produces luma columns 4h..4h+3 of the block and chroma plane h (Cb, Cr).
+// The six-tap and bilinear paths run on packed sample pairs
+// (tcb_mc_pairs.cuh); blocks near the frame edge take the per-sample
+// arithmetic of the CTU engine (tcb_pixel.cuh), so predictions equal the
+// encoder's.
 #include <cuda_runtime.h>
-
-#include <vector>
 
 #include "../../include/tcodec_b200.h"
 #include "tcb_common.cuh"
+#include "tcb_mc_pairs.cuh"
 #include "tcb_pixel.cuh"
 
 namespace tcb {
@@ -30,60 +32,117 @@ struct McFrame {
 struct McJobs {                      // passed by value as the kernel parameter
     static constexpr int MAX = 32;
     int n;
-    int tile_off[MAX + 1];           // first CTA (64x64 tile) of each frame
+    int cta_off[MAX + 1];            // first CTA of each frame
     McFrame f[MAX];
 };
 
-constexpr int MT = 256;
+constexpr int MT = 256;              // threads per CTA: 128 blocks
+#ifndef TCB_MC_CTAS
+#define TCB_MC_CTAS 3                // resident CTAs per SM the register budget is cut for
+#endif
 
-__global__ void __launch_bounds__(MT, 4) mc_frames_kernel(McJobs J) {
+// Four bytes v to dst, only the first w of them at a clipped block edge.
+__device__ __forceinline__ void store4(uint8_t *dst, uint32_t v, int w) {
+    if (w == 4 && (((uintptr_t)dst) & 3) == 0) {
+        *(uint32_t *)dst = v;
+    } else {
+        for (int c = 0; c < w; ++c) dst[c] = (uint8_t)(v >> (8 * c));
+    }
+}
+
+template <int DX, int DY>
+__device__ __forceinline__ void luma_fixed(const uint8_t *ref, int s, int fx, int fy, int h, uint32_t out[8]) {
+    mc_luma_six_tap(ref, s, fx, fy, h, PairPhaseFixed<DX, DY>(), out);
+}
+// The full six-tap block with its quarter phase (dx * 4 + dy, 1..15) fixed.
+__device__ __forceinline__ void luma_six_tap_fixed(const uint8_t *ref, int s, int fx, int fy, int h, int phase,
+                                                   uint32_t out[8]) {
+    switch (phase) {
+        case 1: luma_fixed<0, 1>(ref, s, fx, fy, h, out); break;
+        case 2: luma_fixed<0, 2>(ref, s, fx, fy, h, out); break;
+        case 3: luma_fixed<0, 3>(ref, s, fx, fy, h, out); break;
+        case 4: luma_fixed<1, 0>(ref, s, fx, fy, h, out); break;
+        case 5: luma_fixed<1, 1>(ref, s, fx, fy, h, out); break;
+        case 6: luma_fixed<1, 2>(ref, s, fx, fy, h, out); break;
+        case 7: luma_fixed<1, 3>(ref, s, fx, fy, h, out); break;
+        case 8: luma_fixed<2, 0>(ref, s, fx, fy, h, out); break;
+        case 9: luma_fixed<2, 1>(ref, s, fx, fy, h, out); break;
+        case 10: luma_fixed<2, 2>(ref, s, fx, fy, h, out); break;
+        case 11: luma_fixed<2, 3>(ref, s, fx, fy, h, out); break;
+        case 12: luma_fixed<3, 0>(ref, s, fx, fy, h, out); break;
+        case 13: luma_fixed<3, 1>(ref, s, fx, fy, h, out); break;
+        case 14: luma_fixed<3, 2>(ref, s, fx, fy, h, out); break;
+        default: luma_fixed<3, 3>(ref, s, fx, fy, h, out); break;
+    }
+}
+
+__global__ void __launch_bounds__(MT, TCB_MC_CTAS) mc_frames_kernel(McJobs J) {
     int k = 0;
-    while (k + 1 < J.n && J.tile_off[k + 1] <= (int)blockIdx.x) ++k;
+    while (k + 1 < J.n && J.cta_off[k + 1] <= (int)blockIdx.x) ++k;
     const McFrame &F = J.f[k];
-    const int local = blockIdx.x - J.tile_off[k], tcols = (F.W + 63) >> 6;
-    const int t = threadIdx.x, b = t >> 2, q = t & 3;
-    const int X = ((local % tcols) << 6) + (b & 7) * 8, Y = ((local / tcols) << 6) + (b >> 3) * 8;
-    if (X >= F.W || Y >= F.H) return;
-    const int gw = (F.W + 7) >> 3;
-    const int2 v = make_int2(F.mv[2 * ((Y >> 3) * gw + (X >> 3))], F.mv[2 * ((Y >> 3) * gw + (X >> 3)) + 1]);
-    const int mvx = X * 4 + v.x, mvy = Y * 4 + v.y;
-    // ---- luma: rows 2q, 2q+1 of the 8x8 block
-    LumaMC m;
-    m.init(F.ry, F.sy, F.W, F.H, mvx, mvy, 8);
-    const int wl = min(8, F.W - X);
+    const int gw = (F.W + 7) >> 3, gh = (F.H + 7) >> 3;
+    const int g = ((int)blockIdx.x - J.cta_off[k]) * MT + (int)threadIdx.x;
+    const int blk = g >> 1, h = g & 1;
+    if (blk >= gw * gh) return;
+    const int by = blk / gw, bx = blk - by * gw;
+    const int X = bx * 8, Y = by * 8;
+    const int mvx = X * 4 + F.mv[2 * blk], mvy = Y * 4 + F.mv[2 * blk + 1];
+    // ---- luma: columns 4h..4h+3
+    {
+        const int fx = mvx >> 2, fy = mvy >> 2, dx = mvx & 3, dy = mvy & 3;
+        uint32_t out[8];
+        if (dx == 0 && dy == 0 && fx >= 0 && fy >= 0 && fx + 8 <= F.W && fy + 8 <= F.H) {
 #pragma unroll
-    for (int rr = 0; rr < 2; ++rr) {
-        const int r = 2 * q + rr;
-        if (Y + r >= F.H) break;
-        uint8_t px[8];
-#pragma unroll
-        for (int c = 0; c < 8; ++c) px[c] = (uint8_t)m.at(c, r);
-        uint8_t *dst = F.py + (size_t)(Y + r) * F.sy + X;
-        if (wl == 8 && (((uintptr_t)dst) & 7) == 0) {
-            uint2 w;
-            w.x = px[0] | px[1] << 8 | px[2] << 16 | (uint32_t)px[3] << 24;
-            w.y = px[4] | px[5] << 8 | px[6] << 16 | (uint32_t)px[7] << 24;
-            *(uint2 *)dst = w;
+            for (int y = 0; y < 8; ++y) out[y] = mc_load4(F.ry + (size_t)(fy + y) * F.sy + fx + 4 * h);
+        } else if ((dx | dy) != 0 && fx >= 2 && fx + 10 < F.W && fy >= 2 && fy + 10 < F.H) {
+            // Blocks of one warp that share the phase (coherent motion) take
+            // the path specialised for it; mixed phases take the selecting one.
+            const int phase = dx * 4 + dy;
+            const unsigned m = __activemask();
+            if (__all_sync(m, phase == __shfl_sync(m, phase, __ffs(m) - 1))) {
+                luma_six_tap_fixed(F.ry, F.sy, fx, fy, h, phase, out);
+            } else {
+                PairPhase ph;
+                ph.init(dx, dy);
+                mc_luma_six_tap(F.ry, F.sy, fx, fy, h, ph, out);
+            }
         } else {
-            for (int c = 0; c < wl; ++c) dst[c] = px[c];
+            for (int y = 0; y < 8; ++y) {
+                uint32_t v = 0;
+                for (int c = 0; c < 4; ++c)
+                    v |= (uint32_t)interp_luma_safe(F.ry, F.sy, F.W, F.H, fx + 4 * h + c, fy + y, dx, dy) << (8 * c);
+                out[y] = v;
+            }
+        }
+        const int x0 = X + 4 * h, wl = min(4, F.W - x0), hl = min(8, F.H - Y);
+        if (wl > 0) {
+            uint8_t *dst = F.py + (size_t)Y * F.sy + x0;
+#pragma unroll
+            for (int y = 0; y < 8; ++y)
+                if (y < hl) store4(dst + (size_t)y * F.sy, out[y], wl);
         }
     }
-    // ---- chroma: row q of the 4x4 block, both planes
-    const int Wc = F.W >> 1, Hc = F.H >> 1, cx = X >> 1, cy = (Y >> 1) + q;
-    if (cy < Hc) {
-        const int wc = min(4, Wc - cx);
-#pragma unroll
-        for (int pl = 0; pl < 2; ++pl) {
-            const uint8_t *ref = pl ? F.rcr : F.rcb;
-            uint8_t *dst = (pl ? F.pcr : F.pcb) + (size_t)cy * F.sc + cx;
-            uint8_t px[4];
-#pragma unroll
-            for (int c = 0; c < 4; ++c) px[c] = (uint8_t)chroma_mc_at(ref, F.sc, Wc, Hc, mvx, mvy, c, q);
-            if (wc == 4 && (((uintptr_t)dst) & 3) == 0)
-                *(uint32_t *)dst = px[0] | px[1] << 8 | px[2] << 16 | (uint32_t)px[3] << 24;
-            else
-                for (int c = 0; c < wc; ++c) dst[c] = px[c];
+    // ---- chroma: plane h, the 4x4 block at (X/2, Y/2)
+    {
+        const int Wc = F.W >> 1, Hc = F.H >> 1, cx = X >> 1, cy = Y >> 1;
+        const uint8_t *ref = h ? F.rcr : F.rcb;
+        const int xi = mvx >> 3, yi = mvy >> 3;
+        uint32_t out[4];
+        if (xi >= 0 && xi + 4 < Wc && yi >= 0 && yi + 4 < Hc) {
+            mc_chroma_bilinear(ref, F.sc, xi, yi, mvx & 7, mvy & 7, out);
+        } else {
+            for (int y = 0; y < 4; ++y) {
+                uint32_t v = 0;
+                for (int c = 0; c < 4; ++c)
+                    v |= (uint32_t)chroma_mc_at(ref, F.sc, Wc, Hc, mvx, mvy, c, y) << (8 * c);
+                out[y] = v;
+            }
         }
+        const int wc = min(4, Wc - cx), hc = min(4, Hc - cy);
+        uint8_t *dst = (h ? F.pcr : F.pcb) + (size_t)cy * F.sc + cx;
+#pragma unroll
+        for (int y = 0; y < 4; ++y)
+            if (y < hc) store4(dst + (size_t)y * F.sc, out[y], wc);
     }
 }
 
@@ -109,12 +168,13 @@ extern "C" tc_error_t tcb_mc_frames(const tcb_mc_frame_t *frames, int n, void *s
             const tcb_mc_frame_t &f = frames[i];
             J.f[J.n] = {f.ref_y, f.ref_cb, f.ref_cr, f.pred_y, f.pred_cb, f.pred_cr, f.mv,
                         f.width, f.height, f.stride_y, f.stride_c};
-            J.tile_off[J.n] = total;
-            total += ((f.width + 63) >> 6) * ((f.height + 63) >> 6);
+            J.cta_off[J.n] = total;
+            const int blocks = ((f.width + 7) >> 3) * ((f.height + 7) >> 3);
+            total += (2 * blocks + MT - 1) / MT;
             ++J.n;
             ++i;
         }
-        J.tile_off[J.n] = total;
+        J.cta_off[J.n] = total;
         mc_frames_kernel<<<total, MT, 0, (cudaStream_t)stream>>>(J);
         if (cudaGetLastError() != cudaSuccess) return TC_ERR_INTERNAL;
     }

@@ -126,3 +126,23 @@ def test_sao_frames_match_oracle(lib):
         assert np.array_equal(g["y"], y), (c["w"], c["h"], c["qp"])
         n_sao += int(params[:, 0].sum())
     assert n_sao > 0   # the cases exercise the apply path
+
+
+def test_filters_random_content(lib):
+    """Uniformly random samples (the standalone bench's content): every CTU
+    has samples in bands 0 and 31 and edges of every strength."""
+    rng = np.random.default_rng(8)
+    cases = []
+    for w, h, qp, pad in ((256, 128, 30, 0), (136, 100, 45, 4)):
+        c = dict(w=w, h=h, qp=qp, pad=pad)
+        for k, (hh, ww) in (("y", (h, w)), ("cb", (h // 2, w // 2)), ("cr", (h // 2, w // 2)), ("src", (h, w))):
+            c[k] = rng.integers(0, 256, (hh, ww)).astype(np.uint8)
+        cases.append(c)
+    got = run(lib, lib.tcb_deblock_frames, cases)
+    for c, g in zip(cases, got):
+        y, cb, cr = oracle_deblock(c)
+        assert np.array_equal(g["y"], y) and np.array_equal(g["cb"], cb) and np.array_equal(g["cr"], cr)
+    got = run(lib, lib.tcb_sao_frames, cases)
+    for c, g in zip(cases, got):
+        y, params = oracle_sao(c)
+        assert np.array_equal(g["params"], params) and np.array_equal(g["y"], y)
