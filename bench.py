@@ -64,6 +64,7 @@ W, H, QP, PRESET, PROFILE = 1920, 1080, 32, 2, 1
 METRIC = "1080p v2 encode frames/s (bit-exact), batched/served vs plain GPU; p50/p99 latency"
 UNIT = "frames/s"
 GOLDEN = os.path.join(ROOT, "tests", "golden", "bench_1080p_gop4b.json")
+GRAPHS = False   # --graphs: batched / served steps replayed as CUDA graphs
 TRAFFIC = os.path.join(ROOT, "profiles", "ctu_engine_traffic.txt")   # JSON body
 MIXED_GOLDEN = os.path.join(ROOT, "tests", "golden", "mixed_streams.json")
 SERVED_BUDGET = 150 * 10**9          # HBM budget of the served form (bytes)
@@ -238,6 +239,7 @@ def run_mixed_batch(lib, specs, clips):
     pinned = [[tuple(torch.from_numpy(np.ascontiguousarray(p)).pin_memory().numpy() for p in f) for f in c]
               for c in clips]
     batch = api.BatchEncoder(lib, cfgs)
+    batch.set_graphs(GRAPHS)
     lib.tcb_batch_set_timing(batch.h, 1)
     n = len(specs)
     nf = max(len(c) for c in clips)
@@ -330,7 +332,8 @@ def run_forms(lib, mixed_specs, mixed_clips, served_specs, served_clips):
     import torch
     free, total = torch.cuda.mem_get_info()
     budget = min(SERVED_BUDGET, int(free * 0.9))
-    sv = serving.serve(lib, served_specs, served_clips, budget, max_active=256, preset=PRESET, profile=PROFILE)
+    sv = serving.serve(lib, served_specs, served_clips, budget, max_active=256, preset=PRESET, profile=PROFILE,
+                       graphs=GRAPHS)
     exact_s = None
     if golden and len(golden.get("served", [])) >= len(served_specs):
         exact_s = all(stream_digest(sv["packets"][j]) == golden["served"][j]["digest"]
@@ -452,6 +455,7 @@ def run_b200(args, rank, world):
 
     def batch_pass(on_device):
         batch = api.BatchEncoder(lib, [make_cfg(lib) for _ in range(S)])
+        batch.set_graphs(GRAPHS)
         lib.tcb_batch_set_timing(batch.h, 1)
         pinned = None
         if not on_device:
@@ -557,9 +561,13 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the mixed-batch and served forms")
     ap.add_argument("--served-sessions", type=int, default=64)
     ap.add_argument("--no-kernels", action="store_true", help="skip the standalone-kernel roofline section")
+    ap.add_argument("--graphs", action="store_true",
+                    help="replay every batched / served step's device work as one CUDA graph")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only time the standalone frame kernels (deblock, SAO, motion compensation)")
     args = ap.parse_args()
+    global GRAPHS
+    GRAPHS = args.graphs
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -676,7 +684,7 @@ def main():
         "host_ms_per_step": {k: v / steps for k, v in zip(("plan_launch", "wait_device", "entropy"),
                                                           dev_run["host"])},
         "batch": {"streams_per_gpu": args.streams, "form": "batched: every stream's CTUs in one persistent "
-                  "wavefront launch per step (tcb_batch_encode)"},
+                  "wavefront launch per step (tcb_batch_encode)", "cuda_graphs": GRAPHS},
         "plain_gpu": (None if plain is None else {"value": plain["frames"] / (plain["ms"] / 1000.0), "unit": UNIT,
                       "what": "one stream alone through the same kernels (tcb_encoder_encode_device)"}),
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(import_rec),

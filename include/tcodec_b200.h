@@ -81,6 +81,16 @@ void tcb_batch_get_timing(tcb_batch_t *batch, double *ctu_ms, int64_t *ctu_launc
 /* Host wall-clock split of the timed steps (timing enabled): planning and
  * launch, waiting for the device, entropy coding.  Reading resets. */
 void tcb_batch_get_host_timing(tcb_batch_t *batch, double *plan_ms, double *wait_ms, double *entropy_ms);
+/* CUDA-graph replay of each step's device work (default off): the step's
+ * launch sequence (parameter uploads, global-motion kernel, work queue,
+ * CTU engine, copy-back) is captured and replayed as one graph launch;
+ * executable graphs are cached per step shape and updated in place with
+ * the step's pointers.  Packets are identical either way.  graph_builds
+ * counts instantiations, graph_launches replays; reading resets.  Returns
+ * 0, or, for the last in-place update the runtime refused since the
+ * previous read, 1000 * (cudaGraphNodeType + 1) + the node's position. */
+void tcb_batch_set_graphs(tcb_batch_t *batch, int enabled);
+int tcb_batch_get_graph_stats(tcb_batch_t *batch, int64_t *graph_launches, int64_t *graph_builds);
 
 /* ---------------------------------------------------------------------
  * Served form (no reference counterpart): encode sessions that arrive and
@@ -131,6 +141,8 @@ int tcb_server_session_state(tcb_server_t *server, int session);
 int tcb_server_step(tcb_server_t *server, tcb_server_packet_t *out, int cap);
 void tcb_server_stats(tcb_server_t *server, int *waiting, int *active, int *retired,
                       size_t *bytes_in_use, size_t *bytes_budget);
+/* CUDA-graph replay of every step's device work (as tcb_batch_set_graphs). */
+void tcb_server_set_graphs(tcb_server_t *server, int enabled);
 
 /* ---------------------------------------------------------------------
  * Part 2: standalone kernels.

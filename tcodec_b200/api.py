@@ -329,6 +329,9 @@ def bind_b200(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.tcb_batch_set_timing.argtypes = [vp, ctypes.c_int]
     lib.tcb_batch_get_timing.argtypes = [vp] + [vp] * 5
     lib.tcb_batch_get_host_timing.argtypes = [vp] + [vp] * 3
+    lib.tcb_batch_set_graphs.argtypes = [vp, ctypes.c_int]
+    lib.tcb_batch_get_graph_stats.argtypes = [vp, vp, vp]
+    lib.tcb_batch_get_graph_stats.restype = ctypes.c_int
     lib.tcb_ctu_record_bytes.restype = ctypes.c_size_t
     lib.tcb_mv_cell_bytes.restype = ctypes.c_size_t
     lib.tcb_ctu_scratch_bytes.argtypes = [ctypes.c_int, ctypes.c_int]
@@ -359,6 +362,17 @@ class BatchEncoder:
         if not self.h:
             raise RuntimeError("tcb_batch_create failed")
         self.cfgs = cfgs
+
+    def set_graphs(self, on: bool = True):
+        """Replay each step's device work as one CUDA graph (tcb_batch_set_graphs)."""
+        self.lib.tcb_batch_set_graphs(self.h, 1 if on else 0)
+
+    def graph_stats(self):
+        """(graph launches, graph instantiations, last refused-update result)
+        since the last call."""
+        a, b = ctypes.c_int64(), ctypes.c_int64()
+        r = self.lib.tcb_batch_get_graph_stats(self.h, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value, r
 
     def close(self):
         if self.h:
@@ -475,6 +489,7 @@ def bind_server(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.tcb_server_step.argtypes = [vp, ctypes.POINTER(ServerPacket), ctypes.c_int]
     lib.tcb_server_step.restype = ctypes.c_int
     lib.tcb_server_stats.argtypes = [vp] + [vp] * 5
+    lib.tcb_server_set_graphs.argtypes = [vp, ctypes.c_int]
     return lib
 
 
@@ -489,6 +504,10 @@ class Server:
             raise RuntimeError("tcb_server_create failed")
         self.max_active = max_active
         self._out = (ServerPacket * max_active)()
+
+    def set_graphs(self, on: bool = True):
+        """Replay each step's device work as one CUDA graph (tcb_server_set_graphs)."""
+        self.lib.tcb_server_set_graphs(self.h, 1 if on else 0)
 
     def close(self):
         if self.h:

@@ -39,6 +39,20 @@ struct tcb_batch {
     long long ctu_launches = 0, ctu_count = 0, steps = 0, kernel_launches = 0;
     double host_plan_ms = 0.0, host_wait_ms = 0.0, host_entropy_ms = 0.0;   // wall-clock split of steps
     int device = 0;
+    int *h_items_pin = nullptr;              // pinned staging of h_items (the upload is capturable)
+    size_t h_items_pin_cap = 0;
+    // CUDA-graph replay of the step's device work: executable graphs keyed
+    // by the captured node sequence (P and B steps differ in topology).
+    bool graphs = false;
+    struct GraphSlot {
+        uint64_t sig;
+        cudaGraph_t tmpl;                    // the graph exec was instantiated from
+        cudaGraphExec_t exec;
+        std::vector<cudaGraphNode_t> nodes;  // tmpl's nodes, in cudaGraphGetNodes order
+    };
+    std::vector<GraphSlot> gcache;
+    long long graph_launches = 0, graph_builds = 0;
+    int graph_update_fail = 0;               // 1000 * (node type + 1) + position of the last refused node
 };
 
 namespace {
@@ -49,31 +63,133 @@ void release(tcb_batch *b) {
         if (e && e->impl) e->impl->st = e->impl->own_st;
         if (e) tc_encoder_destroy(e);
     }
+    for (auto &g : b->gcache) {
+        cudaGraphExecDestroy(g.exec);
+        cudaGraphDestroy(g.tmpl);
+    }
     cudaFree(b->d_params);
     cudaFree(b->d_items);
     cudaFree(b->d_ctrl);
+    cudaFreeHost(b->h_items_pin);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->st) cudaStreamDestroy(b->st);
     delete b;
 }
 
-// Run stage_a..stage_d for the streams whose plan produced a frame.
 double ms_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
-tc_error_t run_step(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkts, int *status) {
-    const int n = (int)b->encs.size();
-    auto t0 = std::chrono::steady_clock::now();
-    for (int s : part) {
-        EncImpl &e = *b->encs[s]->impl;
-        const tc_error_t r = e.stage_a(e.pend.poc, e.pend.qp_off);
-        if (r != TC_OK) return r;
+std::vector<cudaGraphNode_t> graph_nodes(cudaGraph_t g) {
+    size_t n = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess) return {};
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (n && cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return {};
+    return nodes;
+}
+
+// FNV-1a over the node types and kernel functions of a captured graph.
+uint64_t graph_signature(const std::vector<cudaGraphNode_t> &nodes) {
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) { h = (h ^ v) * 1099511628211ull; };
+    mix(nodes.size());
+    for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) != cudaSuccess) return 0;
+        mix((uint64_t)t);
+        if (t == cudaGraphNodeTypeKernel) {
+            cudaKernelNodeParams kp;
+            if (cudaGraphKernelNodeGetParams(nd, &kp) != cudaSuccess) return 0;
+            mix((uint64_t)(uintptr_t)kp.func);
+        }
     }
-    bool need_sync = false;
-    for (int s : part) need_sync |= b->encs[s]->impl->pend.need_hist != 0;
-    if (need_sync && cudaStreamSynchronize(b->st) != cudaSuccess) return TC_ERR_INTERNAL;
+    return h;
+}
+
+// Copy every node's parameters from a new capture of the same shape into
+// the executable graph (node i of the capture onto node i of the
+// template).  Returns 0, or 1000 * (node type + 1) + i for the first node
+// the runtime refused.
+int update_exec(tcb_batch::GraphSlot &slot, const std::vector<cudaGraphNode_t> &nodes) {
+    if (nodes.size() != slot.nodes.size()) return 1;
+    for (size_t i = 0; i < nodes.size(); ++i) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[i], &t) != cudaSuccess) return 2;
+        cudaError_t e = cudaErrorNotSupported;
+        if (t == cudaGraphNodeTypeKernel) {
+            cudaKernelNodeParams p;
+            e = cudaGraphKernelNodeGetParams(nodes[i], &p);
+            if (e == cudaSuccess) e = cudaGraphExecKernelNodeSetParams(slot.exec, slot.nodes[i], &p);
+        } else if (t == cudaGraphNodeTypeMemcpy) {
+            cudaMemcpy3DParms p;
+            e = cudaGraphMemcpyNodeGetParams(nodes[i], &p);
+            if (e == cudaSuccess) e = cudaGraphExecMemcpyNodeSetParams(slot.exec, slot.nodes[i], &p);
+        } else if (t == cudaGraphNodeTypeMemset) {
+            cudaMemsetParams p;
+            e = cudaGraphMemsetNodeGetParams(nodes[i], &p);
+            if (e == cudaSuccess) e = cudaGraphExecMemsetNodeSetParams(slot.exec, slot.nodes[i], &p);
+        } else if (t == cudaGraphNodeTypeEventRecord) {
+            cudaEvent_t ev;
+            e = cudaGraphEventRecordNodeGetEvent(nodes[i], &ev);
+            if (e == cudaSuccess) e = cudaGraphExecEventRecordNodeSetEvent(slot.exec, slot.nodes[i], ev);
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return 1000 * ((int)t + 1) + (int)i;
+        }
+    }
+    return 0;
+}
+
+// Launch a captured step: update the cached executable graph of the same
+// shape in place (new pointers and sizes), or instantiate one.  Takes
+// ownership of g.
+tc_error_t launch_graph(tcb_batch *b, cudaGraph_t g) {
+    const std::vector<cudaGraphNode_t> nodes = graph_nodes(g);
+    const uint64_t sig = graph_signature(nodes);
+    tcb_batch::GraphSlot *hit = nullptr;
+    for (auto &slot : b->gcache)
+        if (slot.sig == sig) { hit = &slot; break; }
+    if (hit) {
+        const int r = update_exec(*hit, nodes);
+        if (r == 0) {
+            cudaGraphDestroy(g);
+        } else {                                   // refused: rebuild this shape's executable graph
+            b->graph_update_fail = r;
+            cudaGraphExecDestroy(hit->exec);
+            cudaGraphDestroy(hit->tmpl);
+            hit->tmpl = g;
+            hit->nodes = nodes;
+            hit->exec = nullptr;
+            if (cudaGraphInstantiate(&hit->exec, g, 0) != cudaSuccess) return TC_ERR_INTERNAL;
+            ++b->graph_builds;
+        }
+    } else {
+        if (b->gcache.size() >= 8) {              // bounded cache: drop the oldest shape
+            cudaGraphExecDestroy(b->gcache.front().exec);
+            cudaGraphDestroy(b->gcache.front().tmpl);
+            b->gcache.erase(b->gcache.begin());
+        }
+        cudaGraphExec_t exec = nullptr;
+        if (cudaGraphInstantiate(&exec, g, 0) != cudaSuccess) {
+            cudaGraphDestroy(g);
+            return TC_ERR_INTERNAL;
+        }
+        ++b->graph_builds;
+        b->gcache.push_back({sig, g, exec, nodes});
+        hit = &b->gcache.back();
+    }
+    if (cudaGraphLaunch(hit->exec, b->st) != cudaSuccess) return TC_ERR_INTERNAL;
+    ++b->graph_launches;
+    return TC_OK;
+}
+
+// Device work of one step (parameter uploads, global-motion walks, work
+// queue, CTU engine, copy-back), enqueued on the batch stream.  Host
+// sources are pinned, so the whole sequence can be captured.
+tc_error_t enqueue_step(tcb_batch *b, const std::vector<int> &part, const std::vector<int> &off,
+                        const std::vector<int> &cnt) {
     for (int s : part) {
         EncImpl &e = *b->encs[s]->impl;
         const tc_error_t r = e.stage_b();
@@ -93,28 +209,14 @@ tc_error_t run_step(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkt
         if (launch_glob_mv_multi(jobs.data(), (int)jobs.size(), b->st) != cudaSuccess) return TC_ERR_INTERNAL;
         b->kernel_launches += ((int)jobs.size() + GlobJobs::MAX - 1) / GlobJobs::MAX;
     }
-    // Merged anti-diagonal item lists of the participating streams.
-    std::vector<int> off(b->max_diag), cnt(b->max_diag);
-    b->h_items.clear();
-    for (int d = 0; d < b->max_diag; ++d) {
-        off[d] = (int)b->h_items.size();
-        for (int s : part) {
-            const auto &sd = b->stream_diag[s];
-            if (d < (int)sd.size()) b->h_items.insert(b->h_items.end(), sd[d].begin(), sd[d].end());
-        }
-        cnt[d] = (int)b->h_items.size() - off[d];
-    }
-    if (b->h_items.size() > b->items_cap) {
-        cudaFree(b->d_items);
-        b->items_cap = b->h_items.size();
-        if (cudaMalloc(&b->d_items, sizeof(int) * b->items_cap) != cudaSuccess) return TC_ERR_MEMORY;
-    }
-    if (cudaMemcpyAsync(b->d_items, b->h_items.data(), sizeof(int) * b->h_items.size(), cudaMemcpyHostToDevice,
+    if (cudaMemcpyAsync(b->d_items, b->h_items_pin, sizeof(int) * b->h_items.size(), cudaMemcpyHostToDevice,
                         b->st) != cudaSuccess)
         return TC_ERR_INTERNAL;
     // One persistent launch drains the merged queue (per-stream publish
-    // flags keep every stream's wavefront order).
-    if (b->timing) cudaEventRecord(b->ev0, b->st);
+    // flags keep every stream's wavefront order).  Inside a captured graph
+    // the timing events become external event-record nodes.
+    const unsigned evf = b->graphs ? cudaEventRecordExternal : cudaEventRecordDefault;
+    if (b->timing && cudaEventRecordWithFlags(b->ev0, b->st, evf) != cudaSuccess) return TC_ERR_INTERNAL;
     const bool persistent = b->encs[part[0]]->impl->persistent;
     if (persistent) {
         if (cudaMemsetAsync(b->d_ctrl, 0, 2 * sizeof(int), b->st) != cudaSuccess ||
@@ -128,15 +230,81 @@ tc_error_t run_step(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkt
                 return TC_ERR_INTERNAL;
         for (int d = 0; d < b->max_diag; ++d) b->kernel_launches += cnt[d] ? 1 : 0;
     }
-    if (b->timing) cudaEventRecord(b->ev1, b->st);
+    if (b->timing && cudaEventRecordWithFlags(b->ev1, b->st, evf) != cudaSuccess) return TC_ERR_INTERNAL;
     for (int s : part) {
-        const tc_error_t r = b->encs[s]->impl->stage_c();
+        // Host reconstruction copies are 2D copies of padded planes, which
+        // an executable graph cannot take new addresses for: in graph mode
+        // they follow the graph launch as ordinary stream copies.
+        const tc_error_t r = b->encs[s]->impl->stage_c(!b->graphs);
         if (r != TC_OK) return r;
         // the queue's error word is the batch's
         if (persistent && cudaMemcpyAsync(b->encs[s]->impl->h_ctrl, b->d_ctrl, 2 * sizeof(int),
                                           cudaMemcpyDeviceToHost, b->st) != cudaSuccess)
             return TC_ERR_INTERNAL;
     }
+    return TC_OK;
+}
+
+// Run stage_a..stage_d for the streams whose plan produced a frame.
+tc_error_t run_step(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkts, int *status) {
+    const int n = (int)b->encs.size();
+    auto t0 = std::chrono::steady_clock::now();
+    for (int s : part) {
+        EncImpl &e = *b->encs[s]->impl;
+        const tc_error_t r = e.stage_a(e.pend.poc, e.pend.qp_off);
+        if (r != TC_OK) return r;
+    }
+    bool need_sync = false;
+    for (int s : part) need_sync |= b->encs[s]->impl->pend.need_hist != 0;
+    if (need_sync && cudaStreamSynchronize(b->st) != cudaSuccess) return TC_ERR_INTERNAL;
+    // Merged anti-diagonal item lists of the participating streams (the
+    // queue order), staged in pinned memory.
+    std::vector<int> off(b->max_diag), cnt(b->max_diag);
+    b->h_items.clear();
+    for (int d = 0; d < b->max_diag; ++d) {
+        off[d] = (int)b->h_items.size();
+        for (int s : part) {
+            const auto &sd = b->stream_diag[s];
+            if (d < (int)sd.size()) b->h_items.insert(b->h_items.end(), sd[d].begin(), sd[d].end());
+        }
+        cnt[d] = (int)b->h_items.size() - off[d];
+    }
+    if (b->h_items.size() > b->items_cap) {
+        cudaFree(b->d_items);
+        b->d_items = nullptr;
+        b->items_cap = 0;
+        if (cudaMalloc(&b->d_items, sizeof(int) * b->h_items.size()) != cudaSuccess) return TC_ERR_MEMORY;
+        b->items_cap = b->h_items.size();
+    }
+    if (b->h_items.size() > b->h_items_pin_cap) {
+        cudaFreeHost(b->h_items_pin);
+        b->h_items_pin = nullptr;
+        b->h_items_pin_cap = 0;
+        if (cudaMallocHost(&b->h_items_pin, sizeof(int) * b->h_items.size()) != cudaSuccess) return TC_ERR_MEMORY;
+        b->h_items_pin_cap = b->h_items.size();
+    }
+    memcpy(b->h_items_pin, b->h_items.data(), sizeof(int) * b->h_items.size());
+    if (b->graphs) {
+        if (cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return TC_ERR_INTERNAL;
+        const tc_error_t r = enqueue_step(b, part, off, cnt);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(b->st, &g);   // ends the capture on every path
+        if (r != TC_OK || ce != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return r != TC_OK ? r : TC_ERR_INTERNAL;
+        }
+        const tc_error_t lr = launch_graph(b, g);
+        if (lr != TC_OK) return lr;
+        for (int s : part) {
+            const tc_error_t rr = b->encs[s]->impl->readback_recon();
+            if (rr != TC_OK) return rr;
+        }
+    } else {
+        const tc_error_t r = enqueue_step(b, part, off, cnt);
+        if (r != TC_OK) return r;
+    }
+    const bool persistent = b->encs[part[0]]->impl->persistent;
     if (b->timing) { b->host_plan_ms += ms_since(t0); t0 = std::chrono::steady_clock::now(); }
     if (cudaStreamSynchronize(b->st) != cudaSuccess) return TC_ERR_INTERNAL;
     if (b->timing) { b->host_wait_ms += ms_since(t0); t0 = std::chrono::steady_clock::now(); }
@@ -222,6 +390,10 @@ tc_encoder_t *tcb::batch_slot(tcb_batch *b, int s) {
 
 cudaStream_t tcb::batch_stream(tcb_batch *b) { return b->st; }
 
+void tcb::batch_set_graphs(tcb_batch *b, bool on) {
+    if (b) b->graphs = on;
+}
+
 tc_error_t tcb::batch_run(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkts, int *status) {
     if (part.empty()) return TC_OK;
     if (cudaSetDevice(b->device) != cudaSuccess) return TC_ERR_INTERNAL;
@@ -300,6 +472,18 @@ tc_error_t tcb_batch_flush(tcb_batch_t *b, tc_packet_t *packets, int *status) {
 
 void tcb_batch_set_timing(tcb_batch_t *b, int enabled) {
     if (b) b->timing = enabled != 0;
+}
+
+void tcb_batch_set_graphs(tcb_batch_t *b, int enabled) { tcb::batch_set_graphs(b, enabled != 0); }
+
+int tcb_batch_get_graph_stats(tcb_batch_t *b, int64_t *graph_launches, int64_t *graph_builds) {
+    if (!b) return 0;
+    if (graph_launches) *graph_launches = b->graph_launches;
+    if (graph_builds) *graph_builds = b->graph_builds;
+    const int r = b->graph_update_fail;
+    b->graph_launches = b->graph_builds = 0;
+    b->graph_update_fail = 0;
+    return r;
 }
 
 void tcb_batch_get_host_timing(tcb_batch_t *b, double *plan_ms, double *wait_ms, double *entropy_ms) {

@@ -22,6 +22,7 @@ int batch_attach(tcb_batch *b, tc_encoder_t *e);
 void batch_detach(tcb_batch *b, int slot);
 tc_encoder_t *batch_slot(tcb_batch *b, int slot);
 cudaStream_t batch_stream(tcb_batch *b);
+void batch_set_graphs(tcb_batch *b, bool on);
 // Runs one frame of every slot in `part` (each already planned with
 // plan_input / plan_flush); packets[slot] / status[slot] receive the result.
 tc_error_t batch_run(tcb_batch *b, const std::vector<int> &part, tc_packet_t *packets, int *status);

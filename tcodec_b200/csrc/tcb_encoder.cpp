@@ -158,6 +158,7 @@ bool EncImpl::init(const tc_config_t &c) {
     CK(cudaMemset(d_done, 0, sizeof(int) * ctu_cols * ctu_rows));
     CK(dmalloc(&d_ctrl, 2 * sizeof(int)));
     CK(cudaMallocHost(&h_ctrl, 2 * sizeof(int)));
+    CK(cudaMallocHost(&h_params_pin, sizeof(FrameParams)));
     CK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
     {
         const char *wf = getenv("TCB_WAVEFRONT");
@@ -203,7 +204,7 @@ void EncImpl::release() {
     dfree(d_out); cudaFreeHost(h_out);
     dfree(d_params); dfree(d_hist); cudaFreeHost(h_hist);
     dfree(d_sse); cudaFreeHost(h_sse); dfree(d_err); dfree(d_items);
-    dfree(d_done); dfree(d_ctrl); cudaFreeHost(h_ctrl);
+    dfree(d_done); dfree(d_ctrl); cudaFreeHost(h_ctrl); cudaFreeHost(h_params_pin);
     for (auto &f : bf_frames) { dfree(f.y); dfree(f.cb); dfree(f.cr); }
     for (auto &f : bf_free) { dfree(f.y); dfree(f.cb); dfree(f.cr); }
     bf_frames.clear();
@@ -376,7 +377,8 @@ tc_error_t EncImpl::stage_b() {
     P.err = d_err;
     P.done = d_done;
     P.epoch = ++epoch;
-    if (cudaMemcpyAsync(d_params, &P, sizeof(P), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    *h_params_pin = P;   // the previous frame's upload has completed (every step ends synchronised)
+    if (cudaMemcpyAsync(d_params, h_params_pin, sizeof(P), cudaMemcpyHostToDevice, st) != cudaSuccess)
         return TC_ERR_INTERNAL;
     pend.glob = frame_type == 1 && P.ref_valid[0];
     pend.glob_ref = P.ref_y[0];
@@ -410,9 +412,9 @@ tc_error_t EncImpl::launch_own() {
     return TC_OK;
 }
 
-tc_error_t EncImpl::stage_c() {
-    const DevFrame rec = pool[pend.rs];
+tc_error_t EncImpl::stage_c(bool with_recon) {
     const int nctu = ctu_cols * ctu_rows;
+    const DevFrame rec = pool[pend.rs];
     if (cudaMemcpyAsync(h_out, d_out, sizeof(CtuOut) * nctu, cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return TC_ERR_INTERNAL;
     if (launch_frame_sse(cur.y, rec.y, W, H, sy, d_sse, st) != cudaSuccess) return TC_ERR_INTERNAL;
@@ -420,6 +422,12 @@ tc_error_t EncImpl::stage_c() {
     if (cudaMemcpyAsync(h_sse, d_sse, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaMemcpyAsync(h_ctrl, d_ctrl, 2 * sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return TC_ERR_INTERNAL;
+    return with_recon ? readback_recon() : TC_OK;
+}
+
+// Host copy of the reconstruction (tc_encoder_t.recon), when enabled.
+tc_error_t EncImpl::readback_recon() {
+    const DevFrame rec = pool[pend.rs];
     if (recon_host && recon_readback) {
         if (cudaMemcpy2DAsync(recon_host->y, recon_host->stride_y, rec.y, sy, W, H, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaMemcpy2DAsync(recon_host->cb, recon_host->stride_c, rec.cb, sc, W / 2, H / 2, cudaMemcpyDeviceToHost, st) != cudaSuccess ||

@@ -42,6 +42,7 @@ struct EncImpl {
     int grid_cur = 0;
     CtuOut *d_out = nullptr, *h_out = nullptr;
     FrameParams h_params{};
+    FrameParams *h_params_pin = nullptr;   // pinned staging of h_params for the upload (capturable)
     FrameParams *d_params = nullptr;
     int *d_items = nullptr;
     std::vector<int> diag_off, diag_cnt;
@@ -118,7 +119,8 @@ struct EncImpl {
     tc_error_t stage_a(int poc, int b_layer_qp_off);
     tc_error_t stage_b();
     tc_error_t launch_own();
-    tc_error_t stage_c();
+    tc_error_t stage_c(bool with_recon = true);   // copy-back; the host recon copy unless with_recon is false
+    tc_error_t readback_recon();
     tc_error_t stage_d(tc_packet_t *pkt);
     tc_error_t encode_planned(tc_packet_t *pkt);
     tc_error_t bf_plan_scheduled();

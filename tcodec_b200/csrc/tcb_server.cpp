@@ -230,6 +230,10 @@ int tcb_server_step(tcb_server_t *s, tcb_server_packet_t *out, int cap) {
     return n;
 }
 
+void tcb_server_set_graphs(tcb_server_t *s, int enabled) {
+    if (s) batch_set_graphs(s->batch, enabled != 0);
+}
+
 void tcb_server_stats(tcb_server_t *s, int *waiting, int *active, int *done, size_t *bytes_in_use,
                       size_t *bytes_budget) {
     if (!s) return;

@@ -17,7 +17,7 @@ from . import api
 
 
 def serve(lib, sessions: List[dict], clips: List[list], hbm_budget_bytes: int, max_active: int = 64,
-          preset: int = api.PRESET_MEDIUM, profile: int = 1, on_step=None) -> Dict:
+          preset: int = api.PRESET_MEDIUM, profile: int = 1, on_step=None, graphs: bool = False) -> Dict:
     """Run every session to completion.  sessions[i] has arrival_s, w, h, qp;
     clips[i] is its list of (y, cb, cr) frames.  Returns packets per
     session, per-frame latencies (s), makespan (s) and step statistics."""
@@ -25,6 +25,7 @@ def serve(lib, sessions: List[dict], clips: List[list], hbm_budget_bytes: int, m
     cfgs = [api.make_config(lib, s["w"], s["h"], qp=s["qp"], preset=preset, profile=profile,
                             keyframe_interval=1000) for s in sessions]
     srv = api.Server(lib, hbm_budget_bytes, max_active)
+    srv.set_graphs(graphs)
     sid: Dict[int, int] = {}
     inv: Dict[int, int] = {}
     fed = [0] * n
