@@ -393,6 +393,14 @@ def run_standalone_kernels(lib, peak, iters=8, frames=64):
 
     st = torch.cuda.current_stream()
     flush = torch.empty(256 * 2 ** 20, dtype=torch.uint8, device="cuda")
+    # Tile shape (threads per CTA) of each kernel from the autotuner, timed
+    # on 32 scratch 1080p frames; the kernels below then run that variant.
+    torch.cuda.synchronize()
+    if lib.tcb_autotune_frame_kernels(W_, H_, 32) != 0:
+        raise RuntimeError("tcb_autotune_frame_kernels failed")
+    tuned = {k: lib.tcb_autotune_threads(v, W_, H_) for k, v in
+             (("tcb_deblock_frames", api.KERNEL_DEBLOCK), ("tcb_sao_frames", api.KERNEL_SAO),
+              ("tcb_mc_frames", api.KERNEL_MC))}
     out = {}
     cases = (("tcb_deblock_frames", lib.tcb_deblock_frames, ff, 3.0 * W_ * (H_ // 64 * 64)),
              ("tcb_sao_frames", lib.tcb_sao_frames, ff, 4.0 * W_ * H_),
@@ -412,7 +420,8 @@ def run_standalone_kernels(lib, peak, iters=8, frames=64):
         t = sorted(ts[2:])[len(ts[2:]) // 2] / 1000.0
         achieved = per_frame * N / t / 1e9
         out[name] = {"frames_per_call": N, "ms": t * 1000.0, "algorithmic_bytes": per_frame * N,
-                     "achieved_gbs": achieved, "frac_of_hbm": achieved / peak}
+                     "achieved_gbs": achieved, "frac_of_hbm": achieved / peak,
+                     "threads_per_cta": tuned[name.split(" ")[0]]}
     return out
 
 
@@ -555,7 +564,7 @@ def main():
     ap.add_argument("--steps", type=int, default=16)
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--streams", type=int, default=16, help="1080p streams per GPU in the batched form")
+    ap.add_argument("--streams", type=int, default=32, help="1080p streams per GPU in the batched form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the mixed-batch and served forms")
@@ -658,8 +667,11 @@ def main():
     achieved = alg_bytes_per_launch / per_launch_s / 1e9
     traffic = None
     if os.path.exists(TRAFFIC):
-        t = json.load(open(TRAFFIC))
-        traffic = t.get("dram_bytes_per_launch")
+        # DRAM bytes of a captured launch, scaled by the CTUs of this run's
+        # launches (each CTU writes its records, spills and reconstruction once)
+        t = json.load(open(TRAFFIC))["measured"]
+        per_ctu = (t["dram_read_bytes"] + t["dram_write_bytes"]) / t["ctus"]
+        traffic = per_ctu * dev_run["ctu_count"] / launches
     lat = sorted(dev_run["lat"])
     p50 = lat[len(lat) // 2] * 1000 if lat else None
     p99 = lat[min(len(lat) - 1, int(0.99 * len(lat)))] * 1000 if lat else None

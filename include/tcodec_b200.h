@@ -252,6 +252,35 @@ tc_error_t tcb_deblock_frames(const tcb_filter_frame_t *frames, int n, void *str
  * (tc_sao_ctu_luma, src/filter.c:251-266) against src_y. */
 tc_error_t tcb_sao_frames(const tcb_filter_frame_t *frames, int n, void *stream);
 
+/* Autotuner of the frame kernels' tile shape (threads per CTA: deblocking
+ * 64 / 128 / 256, SAO 64 / 128, motion compensation 64 / 128 / 256).
+ * tcb_autotune_frame_kernels times every variant of the three kernels on
+ * `frames` (1..32) scratch frames of width x height with random content and
+ * vectors (device memory allocated and freed inside; the call
+ * synchronises), keeps the fastest per kernel for that frame size, and
+ * later calls whose first frame has that size use it (process-wide).
+ * tcb_autotune_threads returns the tuned threads per CTA of a kernel at a
+ * size, plus TCB_STAGING_TMA for deblocking when TMA staging won (0: not
+ * tuned; the kernel then uses its default, 128 / 128 / 256 threads and
+ * vector loads). */
+#define TCB_KERNEL_DEBLOCK 0
+#define TCB_KERNEL_SAO 1
+#define TCB_KERNEL_MC 2
+/* Added to a deblocking variant: the CTU tiles are staged through the
+ * tensor-memory accelerator (2D tile copies into shared memory and back)
+ * instead of 16-byte vector loads, for launches whose planes are 16-byte
+ * aligned with 16-byte multiple strides. */
+#define TCB_STAGING_TMA 0x10000
+tc_error_t tcb_autotune_frame_kernels(int width, int height, int frames);
+int tcb_autotune_threads(int kernel, int width, int height);
+/* Record a choice directly (a table saved from an earlier tuning run):
+ * threads must be a variant of the kernel, 0 removes the entry. */
+tc_error_t tcb_autotune_set_threads(int kernel, int width, int height, int threads);
+/* Bounded waits of the frame kernels that gave up since the last call
+ * (a staged tile that never arrived; the CTU is then left unfiltered).
+ * 0 in a healthy run; reading resets.  Synchronises the device. */
+unsigned int tcb_frame_kernels_errors(void);
+
 #ifdef __cplusplus
 }
 #endif

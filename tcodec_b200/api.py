@@ -20,6 +20,8 @@ LIB_PATH = os.path.join(_HERE, "libtcodec_b200.so")
 TC_OK, TC_ERR_MEMORY, TC_ERR_PARAM, TC_ERR_BITSTREAM, TC_ERR_EOF, TC_ERR_INTERNAL, TC_ERR_NEED_MORE = (
     0, -1, -2, -3, -4, -5, -6)
 PRESET_ULTRAFAST, PRESET_FAST, PRESET_MEDIUM, PRESET_SLOW = 0, 1, 2, 3
+KERNEL_DEBLOCK, KERNEL_SAO, KERNEL_MC = 0, 1, 2   # tcb_autotune_* kernel ids
+STAGING_TMA = 0x10000                             # TCB_STAGING_TMA: deblocking tiles staged by TMA
 
 
 class Config(ctypes.Structure):
@@ -345,6 +347,14 @@ def bind_b200(lib: ctypes.CDLL) -> ctypes.CDLL:
         fn.restype = ctypes.c_int
     lib.tcb_mc_frames.argtypes = [ctypes.POINTER(McFrame), ctypes.c_int, vp]
     lib.tcb_mc_frames.restype = ctypes.c_int
+    lib.tcb_autotune_frame_kernels.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.tcb_autotune_frame_kernels.restype = ctypes.c_int
+    lib.tcb_autotune_threads.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.tcb_autotune_threads.restype = ctypes.c_int
+    lib.tcb_autotune_set_threads.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.tcb_autotune_set_threads.restype = ctypes.c_int
+    lib.tcb_frame_kernels_errors.argtypes = []
+    lib.tcb_frame_kernels_errors.restype = ctypes.c_uint
     return lib
 
 

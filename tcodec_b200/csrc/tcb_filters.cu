@@ -24,6 +24,10 @@
 // sample values of bands 0 and 31, where an offset can clip; the SSE of
 // every band after its offset then follows in closed form, clipping
 // included (tcb_sao_decide.cuh), with no second pass over the pixels.
+#include <string.h>
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include "tcb_common.cuh"
@@ -36,17 +40,13 @@ namespace tcb {
 
 namespace {
 
-// Threads per CTA (one CTU each).  Small CTAs let many CTUs' loads be in
-// flight per SM while other CTUs of the same SM filter.
-#ifndef TCB_DEBLOCK_FT
-#define TCB_DEBLOCK_FT 128
-#endif
-#ifndef TCB_SAO_FT
-#define TCB_SAO_FT 128
-#endif
-constexpr int DFT = TCB_DEBLOCK_FT, SFT = TCB_SAO_FT;
-static_assert(384 % DFT == 0 && DFT >= 32, "deblock CTA: 384 16-byte pieces per CTU");
-static_assert(256 % SFT == 0 && SFT >= 32 && SFT <= 256, "SAO CTA: 256 16-pixel segments per CTU");
+// Threads per CTA (one CTU each) are a template parameter: deblocking 64,
+// 128 or 256, SAO 64 or 128 (its statistics table holds one column per
+// thread; 256 would pass the 48 KB of static shared memory); the autotuner
+// times each per frame size, 128 without tuning.  Small
+// CTAs let many CTUs' loads be in flight per SM while other CTUs of the
+// same SM filter.
+constexpr int FILTER_DEFAULT_THREADS = 128;
 
 __device__ __forceinline__ int find_frame(const int *off, int n, int g) {
     int k = 0;
@@ -60,7 +60,10 @@ __device__ __forceinline__ bool aligned16(const void *p, int stride) {
 
 // ---------------------------------------------------------------- deblock
 
+template <int DFT>
 __global__ void __launch_bounds__(DFT) deblock_frames_kernel(DeblockJobs J) {
+    static_assert(DFT >= 32 && DFT % 32 == 0, "whole warps");
+    constexpr int NPIECE = (384 + DFT - 1) / DFT;   // 16-byte pieces per thread (384 per CTU)
     __shared__ __align__(16) uint8_t ty[64 * 64];
     __shared__ __align__(16) uint8_t tc[2][32 * 32];
     const int k = find_frame(J.ctu_off, J.n, blockIdx.x);
@@ -75,10 +78,11 @@ __global__ void __launch_bounds__(DFT) deblock_frames_kernel(DeblockJobs J) {
     // ---- load: 16-byte pieces 0..255 luma (row p>>2, segment p&3),
     // 256..383 chroma (plane, row, segment); all issued before any use
     if (vec) {
-        uint4 v[384 / DFT];
+        uint4 v[NPIECE];
 #pragma unroll
-        for (int j = 0; j < 384 / DFT; ++j) {
+        for (int j = 0; j < NPIECE; ++j) {
             const int p = t + j * DFT;
+            if (p >= 384) break;
             if (p < 256) {
                 v[j] = __ldcs((const uint4 *)(gy + (size_t)(p >> 2) * F.sy + (p & 3) * 16));
             } else {
@@ -87,8 +91,9 @@ __global__ void __launch_bounds__(DFT) deblock_frames_kernel(DeblockJobs J) {
             }
         }
 #pragma unroll
-        for (int j = 0; j < 384 / DFT; ++j) {
+        for (int j = 0; j < NPIECE; ++j) {
             const int p = t + j * DFT;
+            if (p >= 384) break;
             if (p < 256) *(uint4 *)&ty[p * 16] = v[j];
             else {
                 const int q = p - 256, c = q >> 6, r = (q >> 1) & 31, sg = q & 1;
@@ -115,8 +120,9 @@ __global__ void __launch_bounds__(DFT) deblock_frames_kernel(DeblockJobs J) {
     // ---- store
     if (vec) {
 #pragma unroll
-        for (int j = 0; j < 384 / DFT; ++j) {
+        for (int j = 0; j < NPIECE; ++j) {
             const int p = t + j * DFT;
+            if (p >= 384) break;
             if (p < 256) {
                 __stcs((uint4 *)(gy + (size_t)(p >> 2) * F.sy + (p & 3) * 16), *(const uint4 *)&ty[p * 16]);
             } else {
@@ -133,6 +139,95 @@ __global__ void __launch_bounds__(DFT) deblock_frames_kernel(DeblockJobs J) {
     }
 }
 
+// ---------------------------------------------------------------- deblock, TMA staging
+
+// The same filter with the CTU tile moved by the tensor-memory accelerator:
+// one thread issues three 2D tile copies (luma 64x64, Cb / Cr 32x32) that
+// complete on an mbarrier, and after filtering three tile stores write it
+// back.  Used for launches whose planes are 16-byte aligned with 16-byte
+// multiple strides (what a tensor map requires); CTU x-coordinates are
+// multiples of 64 (luma) and 32 (chroma) bytes and only full CTUs are
+// filtered, so every box starts aligned and lies inside its plane.
+struct DeblockTmaJobs {            // passed as a __grid_constant__ kernel parameter (about 12.7 KB)
+    static constexpr int MAX = 32;
+    CUtensorMap ty[MAX], tcb[MAX], tcr[MAX];
+    int n;
+    int ctu_off[MAX + 1];
+    int cols[MAX], qp[MAX];
+};
+
+__device__ unsigned int g_tma_wait_expired;   // bounded TMA waits that gave up (0 in a healthy run)
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(dst), "l"(map), "r"(x), "r"(y), "r"(bar) : "memory");
+}
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, uint32_t src, int x, int y) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];"
+                 ::"l"(map), "r"(x), "r"(y), "r"(src) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                 : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+    return ok != 0;
+}
+
+template <int DFT>
+__global__ void __launch_bounds__(DFT) deblock_tma_kernel(const __grid_constant__ DeblockTmaJobs J) {
+    __shared__ __align__(128) uint8_t ty[64 * 64];
+    __shared__ __align__(128) uint8_t tc[2][32 * 32];
+    __shared__ __align__(8) uint64_t bar;
+    const int k = find_frame(J.ctu_off, J.n, blockIdx.x);
+    const int local = blockIdx.x - J.ctu_off[k];
+    const int x0 = (local % J.cols[k]) << 6, y0 = (local / J.cols[k]) << 6;
+    const int t = threadIdx.x;
+    const uint32_t b = smem_addr(&bar);
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(64 * 64 + 2 * 32 * 32)
+                     : "memory");
+        tma_load_2d(smem_addr(ty), &J.ty[k], x0, y0, b);
+        tma_load_2d(smem_addr(tc[0]), &J.tcb[k], x0 >> 1, y0 >> 1, b);
+        tma_load_2d(smem_addr(tc[1]), &J.tcr[k], x0 >> 1, y0 >> 1, b);
+    }
+    __syncthreads();   // the barrier is initialised before anyone waits on it
+    bool landed = false;
+    for (int i = 0; i < (1 << 22) && !landed; ++i) landed = mbar_try_wait(b, 0);
+    if (!__syncthreads_and(landed)) {
+        // The tile never arrived: record it, give the copies in flight a
+        // second bounded wait (the shared memory must not be released under
+        // them) and leave this CTU unfiltered.
+        if (t == 0) {
+            atomicAdd(&g_tma_wait_expired, 1u);
+            for (int i = 0; i < (1 << 22) && !mbar_try_wait(b, 0); ++i) {
+            }
+        }
+        __syncthreads();
+        return;
+    }
+    DeblockQp q;
+    q.init(J.qp[k]);
+    for (int i = t; i < DEBLOCK_VERT_ITEMS; i += DFT) deblock_vert(ty, tc[0], i, q);
+    __syncthreads();
+    for (int i = t; i < DEBLOCK_HORIZ_ITEMS; i += DFT) deblock_horiz(ty, tc[0], tc[1], i, q);
+    // the filters' shared-memory writes become visible to the bulk-copy
+    // (async) proxy before the stores read the tile
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (t == 0) {
+        tma_store_2d(&J.ty[k], smem_addr(ty), x0, y0);
+        tma_store_2d(&J.tcb[k], smem_addr(tc[0]), x0 >> 1, y0 >> 1);
+        tma_store_2d(&J.tcr[k], smem_addr(tc[1]), x0 >> 1, y0 >> 1);
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");   // tile read out before the CTA ends
+    }
+}
+
 // ---------------------------------------------------------------- SAO
 
 // Byte k (0..3) of w.
@@ -144,20 +239,26 @@ __device__ __forceinline__ int byte_i(const uint4 &v, int i) {
     return byte_k(w, i & 3);
 }
 
-// One sample pair into the thread's statistics column: the word at
-// row_word[r] (the row's offset in the table) gains count 1 and o - r.
-__device__ __forceinline__ void sao_count(int *col, const int *row_word, int r, int o) {
-    col[row_word[r]] += 65536 + o - r;
+// One sample pair into the thread's statistics column: the word of the
+// sample's row (sao_row_of, computed: a lookup table would add a shared
+// load with bank conflicts to every pixel) gains count 1 and o - r.
+template <int SFT>
+__device__ __forceinline__ void sao_count(int *col, int r, int o) {
+    int row = r >> 3;
+    if ((unsigned)(r - 8) >= 240u) row = 32 + (r & 7) + ((r >> 4) & 8);   // values 0..7 -> 32.., 248..255 -> 40..
+    col[row * SFT] += 65536 + o - r;
 }
 
+template <int SFT>
 __global__ void __launch_bounds__(SFT) sao_frames_kernel(SaoJobs J) {
     constexpr int NSEG = 256 / SFT;           // 16-pixel segments per thread
-    // Four columns of the table are summed before unpacking: a column
-    // holds at most 16 * NSEG pixels, so four columns keep |sum| below
-    // 4 * 16 * NSEG * 255 = 32640 for NSEG = 2, inside the 16-bit field.
-    static_assert(SFT == 128, "SAO table reduction sized for 128 threads");
+    static_assert(SFT == 64 || SFT == 128, "SAO CTA: 256 16-pixel segments per CTU, table within 48 KB");
+    // G columns of the table are summed before unpacking: a column holds
+    // at most 16 * NSEG pixels, so G columns keep |sum| <= G * 16 * NSEG *
+    // 255 = 32640, inside the 16-bit field.
+    constexpr int G = NSEG <= 2 ? 4 : 2;
+    constexpr int TPR = SFT >= 2 * SAO_ROWS ? 2 : 1;   // threads summing one row
     __shared__ __align__(16) int hist[SAO_ROWS][SFT];   // count * 65536 + sum of (org - rec), per thread
-    __shared__ int row_word[256];             // sample value -> word offset of its statistics row
     __shared__ int row_cnt[SAO_ROWS], row_sum[SAO_ROWS];
     __shared__ long long red[SFT / 32];
     __shared__ int dec[3];
@@ -192,7 +293,6 @@ __global__ void __launch_bounds__(SFT) sao_frames_kernel(SaoJobs J) {
             ov[j] = make_uint4(o4[0], o4[1], o4[2], o4[3]);
         }
     }
-    for (int i = t; i < 256; i += SFT) row_word[i] = sao_row_of(i) * SFT;
     for (int i = t; i < SAO_ROWS * SFT / 4; i += SFT) ((int4 *)&hist[0][0])[i] = make_int4(0, 0, 0, 0);
     __syncthreads();
     // ---- pass 1: per-row (count, sum) and the unfiltered SSE (|d|^2 four
@@ -211,32 +311,45 @@ __global__ void __launch_bounds__(SFT) sao_frames_kernel(SaoJobs J) {
 #pragma unroll
             for (int q = 0; q < 4; ++q)
 #pragma unroll
-                for (int b = 0; b < 4; ++b) sao_count(col, row_word, byte_k(rw[q], b), byte_k(ow[q], b));
+                for (int b = 0; b < 4; ++b) sao_count<SFT>(col, byte_k(rw[q], b), byte_k(ow[q], b));
         } else {
-            for (int i = 0; i < nvalid[j]; ++i) sao_count(col, row_word, byte_i(rv[j], i), byte_i(ov[j], i));
+            for (int i = 0; i < nvalid[j]; ++i) sao_count<SFT>(col, byte_i(rv[j], i), byte_i(ov[j], i));
         }
     }
     long long bsum = base;
     for (int o = 16; o > 0; o >>= 1) bsum += __shfl_xor_sync(0xffffffffu, bsum, o);
     if ((t & 31) == 0) red[t >> 5] = bsum;
     __syncthreads();
-    // ---- row totals: two threads per row, each summing 64 columns four at
-    // a time (16-byte loads) before unpacking
-    if (t < 2 * SAO_ROWS) {
-        const int row = t >> 1, half = t & 1;
-        const int4 *p = (const int4 *)&hist[row][half * (SFT / 2)];
+    // ---- row totals: TPR threads per row, summing G columns at a time
+    // (16-byte loads) before unpacking
+    if (t < TPR * SAO_ROWS) {
+        const int row = t / TPR, part = t % TPR;
+        const int4 *p = (const int4 *)&hist[row][part * (SFT / TPR)];
         int cnt = 0, sum = 0;
-#pragma unroll
-        for (int i = 0; i < SFT / 8; ++i) {
-            const int4 v = p[i];
-            const int x = v.x + v.y + v.z + v.w;
+        auto unpack = [&](int x) {
             const int sv = (int)(int16_t)(x & 0xffff);
             sum += sv;
             cnt += (x - sv) >> 16;
+        };
+        // start each thread at its own 16-byte column group: the rows are
+        // 128 words apart, so unrotated every lane would read the same banks
+        constexpr int NV = SFT / TPR / 4;
+        const int rot = (row * TPR + part) % NV;
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            const int4 v = p[(i + rot) % NV];
+            if (G == 4) {
+                unpack(v.x + v.y + v.z + v.w);
+            } else {
+                unpack(v.x + v.y);
+                unpack(v.z + v.w);
+            }
         }
-        cnt += __shfl_xor_sync(0xffffffffu, cnt, 1);
-        sum += __shfl_xor_sync(0xffffffffu, sum, 1);
-        if (!half) { row_cnt[row] = cnt; row_sum[row] = sum; }
+        if (TPR == 2) {
+            cnt += __shfl_xor_sync(0xffffffffu, cnt, 1);
+            sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+        }
+        if (!part) { row_cnt[row] = cnt; row_sum[row] = sum; }
     }
     __syncthreads();
     // ---- decision (warp 0): lane b scores band b; first band with the
@@ -307,29 +420,109 @@ __global__ void __launch_bounds__(SFT) sao_frames_kernel(SaoJobs J) {
 
 }  // namespace
 
-cudaError_t launch_deblock_frames(const DeblockFrame *frames, int n, cudaStream_t st) {
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }();
+    return fn;
+}
+
+// 2D uint8 tensor map of a w x h plane with a box x box tile.
+bool encode_plane(CUtensorMap *m, uint8_t *base, int w, int h, int stride, int box) {
+    const auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)w, (cuuint64_t)h}, strides[1] = {(cuuint64_t)stride};
+    const cuuint32_t boxd[2] = {(cuuint32_t)box, (cuuint32_t)box}, estr[2] = {1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, boxd, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool tma_ok(const DeblockFrame &f) {
+    auto al = [](const void *p, int s) { return (((uintptr_t)p) & 15) == 0 && (s & 15) == 0; };
+    return al(f.y, f.sy) && al(f.cb, f.sc) && al(f.cr, f.sc) && f.W >= 64 && f.H >= 64;
+}
+
+}  // namespace
+
+unsigned int tma_waits_expired() {
+    unsigned int v = 0, z = 0;
+    cudaMemcpyFromSymbol(&v, g_tma_wait_expired, sizeof(v));
+    cudaMemcpyToSymbol(g_tma_wait_expired, &z, sizeof(z));
+    return v;
+}
+
+namespace {
+
+cudaError_t launch_group_tma(const DeblockFrame *frames, int m, cudaStream_t st, int threads) {
+    DeblockTmaJobs J;
+    memset(&J, 0, sizeof(J));
+    int total = 0;
+    for (int j = 0; j < m; ++j) {
+        const DeblockFrame &f = frames[j];
+        if (!encode_plane(&J.ty[j], f.y, f.W, f.H, f.sy, 64) ||
+            !encode_plane(&J.tcb[j], f.cb, f.W / 2, f.H / 2, f.sc, 32) ||
+            !encode_plane(&J.tcr[j], f.cr, f.W / 2, f.H / 2, f.sc, 32))
+            return cudaErrorInvalidValue;
+        J.ctu_off[j] = total;
+        J.cols[j] = f.W >> 6;
+        J.qp[j] = f.qp;
+        total += (f.W >> 6) * (f.H >> 6);
+    }
+    J.n = m;
+    J.ctu_off[m] = total;
+    if (total == 0) return cudaSuccess;
+    if (threads == 64) deblock_tma_kernel<64><<<total, 64, 0, st>>>(J);
+    else if (threads == 256) deblock_tma_kernel<256><<<total, 256, 0, st>>>(J);
+    else deblock_tma_kernel<128><<<total, 128, 0, st>>>(J);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_group_vec(const DeblockFrame *frames, int m, cudaStream_t st, int threads) {
+    DeblockJobs J;
+    J.n = m;
+    int total = 0;
+    for (int j = 0; j < m; ++j) {
+        J.f[j] = frames[j];
+        J.ctu_off[j] = total;
+        total += (frames[j].W >> 6) * (frames[j].H >> 6);
+    }
+    J.ctu_off[m] = total;
+    if (total == 0) return cudaSuccess;
+    if (threads == 64) deblock_frames_kernel<64><<<total, 64, 0, st>>>(J);
+    else if (threads == 256) deblock_frames_kernel<256><<<total, 256, 0, st>>>(J);
+    else deblock_frames_kernel<128><<<total, 128, 0, st>>>(J);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_deblock_frames(const DeblockFrame *frames, int n, cudaStream_t st, int variant) {
+    // TMA staging when the variant asks for it and every frame of a launch
+    // group meets the tensor-map alignment; 16-byte vector loads otherwise
+    const bool want_tma = (variant & TCB_STAGING_TMA) != 0;
+    const int threads = variant & ~TCB_STAGING_TMA;
+    static_assert((int)DeblockJobs::MAX == (int)DeblockTmaJobs::MAX, "one group size");
     for (int i = 0; i < n;) {
-        DeblockJobs J;
-        J.n = 0;
-        int total = 0;
-        while (i < n && J.n < DeblockJobs::MAX) {
-            J.f[J.n] = frames[i];
-            J.ctu_off[J.n] = total;
-            total += (frames[i].W >> 6) * (frames[i].H >> 6);
-            ++J.n;
-            ++i;
-        }
-        J.ctu_off[J.n] = total;
-        if (total > 0) {
-            deblock_frames_kernel<<<total, DFT, 0, st>>>(J);
-            const cudaError_t e = cudaGetLastError();
-            if (e != cudaSuccess) return e;
-        }
+        const int m = n - i < DeblockJobs::MAX ? n - i : DeblockJobs::MAX;
+        bool tma = want_tma && tensor_map_encoder() != nullptr;
+        for (int j = 0; tma && j < m; ++j) tma = tma_ok(frames[i + j]);
+        const cudaError_t e = tma ? launch_group_tma(frames + i, m, st, threads)
+                                  : launch_group_vec(frames + i, m, st, threads);
+        if (e != cudaSuccess) return e;
+        i += m;
     }
     return cudaSuccess;
 }
 
-cudaError_t launch_sao_frames(const SaoFrame *frames, int n, cudaStream_t st) {
+cudaError_t launch_sao_frames(const SaoFrame *frames, int n, cudaStream_t st, int threads) {
     for (int i = 0; i < n;) {
         SaoJobs J;
         J.n = 0;
@@ -343,7 +536,8 @@ cudaError_t launch_sao_frames(const SaoFrame *frames, int n, cudaStream_t st) {
         }
         J.ctu_off[J.n] = total;
         if (total > 0) {
-            sao_frames_kernel<<<total, SFT, 0, st>>>(J);
+            if (threads == 64) sao_frames_kernel<64><<<total, 64, 0, st>>>(J);
+            else sao_frames_kernel<128><<<total, 128, 0, st>>>(J);
             const cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) return e;
         }
@@ -380,7 +574,9 @@ tc_error_t tcb_deblock_frames(const tcb_filter_frame_t *frames, int n, void *str
         if (!frame_ok(f)) return TC_ERR_PARAM;
         v[i] = {f.y, f.cb, f.cr, f.width, f.height, f.stride_y, f.stride_c, f.qp};
     }
-    return tcb::launch_deblock_frames(v.data(), n, (cudaStream_t)stream) == cudaSuccess ? TC_OK : TC_ERR_INTERNAL;
+    const int threads = n ? tcb::tuned_threads(TCB_KERNEL_DEBLOCK, frames[0].width, frames[0].height) : 0;
+    return tcb::launch_deblock_frames(v.data(), n, (cudaStream_t)stream, threads) == cudaSuccess ? TC_OK
+                                                                                               : TC_ERR_INTERNAL;
 }
 
 tc_error_t tcb_sao_frames(const tcb_filter_frame_t *frames, int n, void *stream) {
@@ -391,7 +587,9 @@ tc_error_t tcb_sao_frames(const tcb_filter_frame_t *frames, int n, void *stream)
         if (!frame_ok(f) || !f.src_y || f.stride_src < f.width) return TC_ERR_PARAM;
         v[i] = {f.y, f.src_y, f.width, f.height, f.stride_y, f.stride_src, (int)tcb::tc_lambda_host(f.qp), f.sao_params};
     }
-    return tcb::launch_sao_frames(v.data(), n, (cudaStream_t)stream) == cudaSuccess ? TC_OK : TC_ERR_INTERNAL;
+    const int threads = n ? tcb::tuned_threads(TCB_KERNEL_SAO, frames[0].width, frames[0].height) : 0;
+    return tcb::launch_sao_frames(v.data(), n, (cudaStream_t)stream, threads) == cudaSuccess ? TC_OK
+                                                                                           : TC_ERR_INTERNAL;
 }
 
 }  // extern "C"

@@ -6,6 +6,8 @@
 
 #include <cuda_runtime.h>
 
+#include "../../include/tcodec_b200.h"
+
 namespace tcb {
 
 struct DeblockFrame {
@@ -33,7 +35,22 @@ struct SaoJobs {
     SaoFrame f[MAX];
 };
 
-cudaError_t launch_deblock_frames(const DeblockFrame *frames, int n, cudaStream_t st);
-cudaError_t launch_sao_frames(const SaoFrame *frames, int n, cudaStream_t st);
+// threads: CTA size variant (deblocking 64 / 128 / 256, SAO 64 / 128;
+// anything else selects 128); for deblocking, TCB_STAGING_TMA added to it
+// moves the tiles with the tensor-memory accelerator where the planes allow.
+cudaError_t launch_deblock_frames(const DeblockFrame *frames, int n, cudaStream_t st, int threads);
+// Bounded TMA waits in the deblocking kernel that gave up since the last
+// call (0 in a healthy run); reading resets.
+unsigned int tma_waits_expired();
+cudaError_t launch_sao_frames(const SaoFrame *frames, int n, cudaStream_t st, int threads);
+
+// Motion compensation over tcb_mc_frame_t descriptors (tcb_mc.cu);
+// threads 64 / 128 / 256 per CTA, anything else selects 256.
+cudaError_t launch_mc_frames(const tcb_mc_frame_t *frames, int n, cudaStream_t st, int threads);
+
+// Tile-shape choices of the frame-kernel autotuner (tcb_autotune.cpp):
+// threads per CTA tuned for kernel k at a frame size, 0 if not tuned.
+int tuned_threads(int kernel, int width, int height);
+void set_tuned_threads(int kernel, int width, int height, int threads);
 
 }  // namespace tcb

@@ -16,6 +16,7 @@
 
 #include "../../include/tcodec_b200.h"
 #include "tcb_common.cuh"
+#include "tcb_filters.h"
 #include "tcb_mc_pairs.cuh"
 #include "tcb_pixel.cuh"
 
@@ -36,10 +37,10 @@ struct McJobs {                      // passed by value as the kernel parameter
     McFrame f[MAX];
 };
 
-constexpr int MT = 256;              // threads per CTA: 128 blocks
-#ifndef TCB_MC_CTAS
-#define TCB_MC_CTAS 3                // resident CTAs per SM the register budget is cut for
-#endif
+// Threads per CTA are a template parameter (64, 128 or 256; the autotuner
+// times each per frame size, 256 without tuning); the register budget is
+// cut for 768 resident threads per SM (80 registers).
+constexpr int MC_DEFAULT_THREADS = 256;
 
 // Four bytes v to dst, only the first w of them at a clipped block edge.
 __device__ __forceinline__ void store4(uint8_t *dst, uint32_t v, int w) {
@@ -76,7 +77,8 @@ __device__ __forceinline__ void luma_six_tap_fixed(const uint8_t *ref, int s, in
     }
 }
 
-__global__ void __launch_bounds__(MT, TCB_MC_CTAS) mc_frames_kernel(McJobs J) {
+template <int MT>
+__global__ void __launch_bounds__(MT, 768 / MT) mc_frames_kernel(McJobs J) {
     int k = 0;
     while (k + 1 < J.n && J.cta_off[k + 1] <= (int)blockIdx.x) ++k;
     const McFrame &F = J.f[k];
@@ -148,18 +150,8 @@ __global__ void __launch_bounds__(MT, TCB_MC_CTAS) mc_frames_kernel(McJobs J) {
 
 }  // namespace
 
-}  // namespace tcb
-
-extern "C" tc_error_t tcb_mc_frames(const tcb_mc_frame_t *frames, int n, void *stream) {
-    using namespace tcb;
-    if (n < 0 || (n > 0 && !frames)) return TC_ERR_PARAM;
-    for (int i = 0; i < n; ++i) {
-        const tcb_mc_frame_t &f = frames[i];
-        if (f.width <= 0 || f.height <= 0 || (f.width & 1) || (f.height & 1) || f.width > TC_MAX_WIDTH ||
-            f.height > TC_MAX_HEIGHT || f.stride_y < f.width || f.stride_c < f.width / 2 || !f.ref_y ||
-            !f.ref_cb || !f.ref_cr || !f.pred_y || !f.pred_cb || !f.pred_cr || !f.mv)
-            return TC_ERR_PARAM;
-    }
+cudaError_t launch_mc_frames(const tcb_mc_frame_t *frames, int n, cudaStream_t st, int threads) {
+    const int MT = (threads == 64 || threads == 128) ? threads : MC_DEFAULT_THREADS;
     for (int i = 0; i < n;) {
         McJobs J;
         J.n = 0;
@@ -175,8 +167,27 @@ extern "C" tc_error_t tcb_mc_frames(const tcb_mc_frame_t *frames, int n, void *s
             ++i;
         }
         J.cta_off[J.n] = total;
-        mc_frames_kernel<<<total, MT, 0, (cudaStream_t)stream>>>(J);
-        if (cudaGetLastError() != cudaSuccess) return TC_ERR_INTERNAL;
+        if (MT == 64) mc_frames_kernel<64><<<total, 64, 0, st>>>(J);
+        else if (MT == 128) mc_frames_kernel<128><<<total, 128, 0, st>>>(J);
+        else mc_frames_kernel<256><<<total, 256, 0, st>>>(J);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
     }
-    return TC_OK;
+    return cudaSuccess;
+}
+
+}  // namespace tcb
+
+extern "C" tc_error_t tcb_mc_frames(const tcb_mc_frame_t *frames, int n, void *stream) {
+    using namespace tcb;
+    if (n < 0 || (n > 0 && !frames)) return TC_ERR_PARAM;
+    for (int i = 0; i < n; ++i) {
+        const tcb_mc_frame_t &f = frames[i];
+        if (f.width <= 0 || f.height <= 0 || (f.width & 1) || (f.height & 1) || f.width > TC_MAX_WIDTH ||
+            f.height > TC_MAX_HEIGHT || f.stride_y < f.width || f.stride_c < f.width / 2 || !f.ref_y ||
+            !f.ref_cb || !f.ref_cr || !f.pred_y || !f.pred_cb || !f.pred_cr || !f.mv)
+            return TC_ERR_PARAM;
+    }
+    const int threads = n ? tuned_threads(TCB_KERNEL_MC, frames[0].width, frames[0].height) : 0;
+    return launch_mc_frames(frames, n, (cudaStream_t)stream, threads) == cudaSuccess ? TC_OK : TC_ERR_INTERNAL;
 }

@@ -48,9 +48,13 @@ __host__ __device__ __forceinline__ uint32_t pair_fshr(uint32_t lo, uint32_t hi,
     return (uint32_t)((((uint64_t)hi << 32) | lo) >> (sh & 31));
 #endif
 }
+// Lane-wise unsigned 16-bit max / min: one PTX max.u16x2 / min.u16x2
+// (sm_90 and later).
 __host__ __device__ __forceinline__ uint32_t pair_max(uint32_t a, uint32_t b) {
 #ifdef __CUDA_ARCH__
-    return __vmaxu2(a, b);
+    uint32_t r;
+    asm("max.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
 #else
     uint32_t lo = (a & 0xFFFF) > (b & 0xFFFF) ? (a & 0xFFFF) : (b & 0xFFFF);
     uint32_t hi = (a >> 16) > (b >> 16) ? (a >> 16) : (b >> 16);
@@ -59,7 +63,9 @@ __host__ __device__ __forceinline__ uint32_t pair_max(uint32_t a, uint32_t b) {
 }
 __host__ __device__ __forceinline__ uint32_t pair_min(uint32_t a, uint32_t b) {
 #ifdef __CUDA_ARCH__
-    return __vminu2(a, b);
+    uint32_t r;
+    asm("min.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
 #else
     uint32_t lo = (a & 0xFFFF) < (b & 0xFFFF) ? (a & 0xFFFF) : (b & 0xFFFF);
     uint32_t hi = (a >> 16) < (b >> 16) ? (a >> 16) : (b >> 16);

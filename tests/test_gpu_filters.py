@@ -52,7 +52,20 @@ def to_dev(a, pad):
     return torch.from_numpy(buf).cuda()
 
 
-def run(lib, fn, cases):
+def run(lib, fn, cases, kernel=None, threads=0):
+    """One call of fn over the cases; with threads != 0 the call runs the
+    CTA-size variant `threads` (recorded for the first frame's size, the
+    size a launch is tuned by, and removed afterwards)."""
+    if threads:
+        assert lib.tcb_autotune_set_threads(kernel, cases[0]["w"], cases[0]["h"], threads) == 0
+    try:
+        return _run(lib, fn, cases)
+    finally:
+        if threads:
+            lib.tcb_autotune_set_threads(kernel, cases[0]["w"], cases[0]["h"], 0)
+
+
+def _run(lib, fn, cases):
     import torch
     frames = (FilterFrame * len(cases))()
     keep = []
@@ -100,17 +113,21 @@ def oracle_sao(c):
     return y, np.array(params, np.int16)
 
 
-def test_deblock_frames_match_oracle(lib):
+@pytest.mark.parametrize("threads", [0, 64, 128, 256])
+def test_deblock_frames_match_oracle(lib, threads):
+    from tcodec_b200 import api
     rng = np.random.default_rng(5)
     cases = [make_case(rng, *c) for c in CASES]
-    got = run(lib, lib.tcb_deblock_frames, cases)
+    got = run(lib, lib.tcb_deblock_frames, cases, api.KERNEL_DEBLOCK, threads)
     for c, g in zip(cases, got):
         y, cb, cr = oracle_deblock(c)
         assert np.array_equal(g["y"], y), (c["w"], c["h"], c["qp"])
         assert np.array_equal(g["cb"], cb) and np.array_equal(g["cr"], cr), (c["w"], c["h"], c["qp"])
 
 
-def test_sao_frames_match_oracle(lib):
+@pytest.mark.parametrize("threads", [0, 64, 128])
+def test_sao_frames_match_oracle(lib, threads):
+    from tcodec_b200 import api
     rng = np.random.default_rng(6)
     cases = [make_case(rng, *c) for c in CASES]
     # extreme values so bands 0 and 31 (where the offset clips) occur
@@ -118,7 +135,7 @@ def test_sao_frames_match_oracle(lib):
     cases[1]["src"][:40, :40] = 0
     cases[4]["y"][64:100, 64:128] = rng.integers(249, 256, (36, 64))
     cases[4]["src"][64:100, 64:128] = 255
-    got = run(lib, lib.tcb_sao_frames, cases)
+    got = run(lib, lib.tcb_sao_frames, cases, api.KERNEL_SAO, threads)
     n_sao = 0
     for c, g in zip(cases, got):
         y, params = oracle_sao(c)
@@ -146,3 +163,36 @@ def test_filters_random_content(lib):
     for c, g in zip(cases, got):
         y, params = oracle_sao(c)
         assert np.array_equal(g["params"], params) and np.array_equal(g["y"], y)
+
+
+def test_autotuner_picks_a_variant_per_kernel(lib):
+    from tcodec_b200 import api
+    w, h = 320, 192
+    assert lib.tcb_autotune_frame_kernels(w, h, 2) == 0
+    assert lib.tcb_autotune_threads(api.KERNEL_DEBLOCK, w, h) in (64, 128, 256)
+    assert lib.tcb_autotune_threads(api.KERNEL_SAO, w, h) in (64, 128)
+    assert lib.tcb_autotune_threads(api.KERNEL_MC, w, h) in (64, 128, 256)
+    assert lib.tcb_autotune_threads(api.KERNEL_MC, w + 2, h) == 0        # other sizes untouched
+    assert lib.tcb_autotune_set_threads(api.KERNEL_SAO, w, h, 256) != 0  # not a SAO variant
+    for k in (api.KERNEL_DEBLOCK, api.KERNEL_SAO, api.KERNEL_MC):
+        assert lib.tcb_autotune_set_threads(k, w, h, 0) == 0
+        assert lib.tcb_autotune_threads(k, w, h) == 0
+
+
+@pytest.mark.parametrize("threads", [64, 128, 256])
+def test_deblock_tma_staging_matches_oracle(lib, threads):
+    """The TMA-staged deblocking kernel (TCB_STAGING_TMA: 2D tile copies in
+    and out of shared memory) on frames whose planes meet the tensor-map
+    alignment (16-byte bases and strides), against the oracle; no bounded
+    wait may have given up."""
+    from tcodec_b200 import api
+    rng = np.random.default_rng(12)
+    cases = [make_case(rng, w, h, qp, 0) for w, h, qp in ((1920, 1080, 32), (256, 192, 42), (320, 240, 27),
+                                                          (640, 384, 37))]
+    assert lib.tcb_frame_kernels_errors() == 0
+    got = run(lib, lib.tcb_deblock_frames, cases, api.KERNEL_DEBLOCK, threads | api.STAGING_TMA)
+    assert lib.tcb_frame_kernels_errors() == 0
+    for c, g in zip(cases, got):
+        y, cb, cr = oracle_deblock(c)
+        assert np.array_equal(g["y"], y), (c["w"], c["h"], c["qp"])
+        assert np.array_equal(g["cb"], cb) and np.array_equal(g["cr"], cr), (c["w"], c["h"], c["qp"])

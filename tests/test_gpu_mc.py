@@ -86,12 +86,20 @@ CASES = [(1920, 1080, 0, "global"), (200, 136, 0, "random"), (130, 70, 6, "rando
          (96, 80, 2, "random")]
 
 
-def test_mc_frames_match_oracle():
+@pytest.mark.parametrize("threads", [0, 64, 128, 256])
+def test_mc_frames_match_oracle(threads):
+    """Every CTA-size variant (recorded for the first frame's size, the
+    size a launch is tuned by) against the oracle."""
     from tcodec_b200 import api
     lib = bind(api.load_library())
     rng = np.random.default_rng(9)
     cases = [make_case(rng, *c) for c in CASES]
-    got = run_gpu(lib, cases)
+    if threads:
+        assert lib.tcb_autotune_set_threads(api.KERNEL_MC, cases[0]["w"], cases[0]["h"], threads) == 0
+    try:
+        got = run_gpu(lib, cases)
+    finally:
+        lib.tcb_autotune_set_threads(api.KERNEL_MC, cases[0]["w"], cases[0]["h"], 0)
     for c, g in zip(cases, got):
         want = run_oracle(c)
         w, h = c["w"], c["h"]
