@@ -51,11 +51,17 @@ __device__ unsigned long long tcb_phase_cycles[16];
 #define ME_T0() long long _me_t = clock64()
 #define ME_MARK(k) do { if (g == 0 && gt == 0) { const long long _n = clock64(); \
     atomicAdd(&tcb_phase_cycles[k], (unsigned long long)(_n - _me_t)); _me_t = _n; } } while (0)
+// Work counts (thread 0 of the calling group, one atomic per call):
+// [0] integer-search SAD pixel differences, [1] quarter-pel SAD pixels,
+// [2] 8x8 and [3] 4x4 transform units coded (luma and chroma).
+__device__ unsigned long long tcb_op_counts[4];
+#define OPCOUNT(k, v) atomicAdd(&tcb_op_counts[k], (unsigned long long)(v))
 #else
 #define PHASE_T0() do {} while (0)
 #define PHASE(k) do {} while (0)
 #define ME_T0() do {} while (0)
 #define ME_MARK(k) do {} while (0)
+#define OPCOUNT(k, v) do {} while (0)
 #endif
 
 __device__ __forceinline__ void group_bar(int g) {
@@ -118,6 +124,7 @@ __device__ void group_int_sads(Smem &S, int g, int gt, const uint8_t *ref, int s
                                const uint8_t *cur, int blk, int pat, int p0, int K,
                                int bx, int by, int scale) {
     const int wpr = blk >> 2, words = blk * wpr, total = K * words;
+    if (gt == 0) OPCOUNT(0, K * blk * blk);
     int acc[7] = {0, 0, 0, 0, 0, 0, 0};
     for (int i = gt; i < total; i += GT) {
         const int k = i / words, w = i - k * words, r = w / wpr, c4 = (w - r * wpr) * 4;
@@ -197,6 +204,7 @@ __device__ int group_subpel_sad(Smem &S, int g, int gt, const uint8_t *ref, int 
     const int fx = qx >> 2, fy = qy >> 2, dx = qx & 3, dy = qy & 3;
     int acc = 0;
     const int total = blk * blk;
+    if (gt == 0) OPCOUNT(1, total);
     for (int i = gt; i < total; i += GT) {
         const int yy = i / blk, xx = i - yy * blk;
         int p;
@@ -316,6 +324,7 @@ __device__ __forceinline__ int lpred(const Smem &S, int cu, int slot, int dc, in
 __device__ void luma_jobs8(Smem &S, const Leaf &L, const int *cl, int ncl, const QuantParams &qp,
                            bool accum, bool wrec, int16_t *emit, int woff = 0) {
     const int cu = L.cu, ntu = cu >> 3, ntu2 = ntu * ntu, J = ncl * ntu2;
+    if (threadIdx.x == 0) OPCOUNT(2, J);
     const int hw = threadIdx.x >> 5, lane = threadIdx.x & 31, oct = lane >> 3, l8 = lane & 7;
     const int warp = (hw + NW - woff % NW) % NW;   // job rank of this warp
     int *scr = S.scratch[hw] + oct * 64;
@@ -361,6 +370,7 @@ __device__ void luma_jobs8(Smem &S, const Leaf &L, const int *cl, int ncl, const
 __device__ void luma_jobs4(Smem &S, const Leaf &L, const int *cl, int ncl, const QuantParams &qp,
                            bool accum, bool wrec, int16_t *emit, int woff = 0) {
     const int cu = L.cu, ntu = cu >> 3, ntu2 = ntu * ntu, per = ntu2 * 4, J = ncl * per;
+    if (threadIdx.x == 0) OPCOUNT(3, J);
     const int hw = threadIdx.x >> 5, lane = threadIdx.x & 31, qd = lane >> 2, l4 = lane & 3;
     const int warp = (hw + NW - woff % NW) % NW;   // job rank of this warp
     int *scr = S.scratch[hw] + qd * 16;
@@ -408,6 +418,7 @@ __device__ void luma_jobs4(Smem &S, const Leaf &L, const int *cl, int ncl, const
 __device__ void chroma_jobs(Smem &S, const Leaf &L, int nopt, int cbase, const QuantParams &qp,
                             bool accum, bool wrec, int16_t *emit, int woff = 0) {
     const int cs = L.cu >> 1, nt = cs >> 2, nt2 = nt * nt, per = 2 * nt2, J = nopt * per;
+    if (threadIdx.x == 0) OPCOUNT(3, J);
     const int lxc = L.lx >> 1, lyc = L.ly >> 1;
     const int hw = threadIdx.x >> 5, lane = threadIdx.x & 31, qd = lane >> 2, l4 = lane & 3;
     const int warp = (hw + NW - woff % NW) % NW;   // job rank of this warp
@@ -2029,6 +2040,12 @@ cudaError_t launch_decode_items(const FrameParams *d_params, const int *d_items,
 
 #ifdef TCB_PHASE_PROFILE
 // Profiling builds only: read and reset the phase cycle counters.
+extern "C" __attribute__((visibility("default"))) int tcb_debug_op_counts(unsigned long long *out4) {
+    cudaDeviceSynchronize();
+    if (cudaMemcpyFromSymbol(out4, tcb::tcb_op_counts, 4 * sizeof(unsigned long long)) != cudaSuccess) return -1;
+    unsigned long long z[4] = {0};
+    return cudaMemcpyToSymbol(tcb::tcb_op_counts, z, sizeof(z)) == cudaSuccess ? 0 : -1;
+}
 extern "C" __attribute__((visibility("default"))) int tcb_debug_phase_cycles(unsigned long long *out16) {
     cudaDeviceSynchronize();
     if (cudaMemcpyFromSymbol(out16, tcb::tcb_phase_cycles, 16 * sizeof(unsigned long long)) != cudaSuccess) return -1;

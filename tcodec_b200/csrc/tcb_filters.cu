@@ -48,10 +48,16 @@ namespace {
 // same SM filter.
 constexpr int FILTER_DEFAULT_THREADS = 128;
 
+// The frame whose CTA range [off[k], off[k+1]) holds CTA g (binary search
+// over the n <= 32 frames of a launch; off[0] = 0 <= g).
 __device__ __forceinline__ int find_frame(const int *off, int n, int g) {
-    int k = 0;
-    while (k + 1 < n && off[k + 1] <= g) ++k;
-    return k;
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
 }
 
 __device__ __forceinline__ bool aligned16(const void *p, int stride) {

@@ -79,8 +79,12 @@ __device__ __forceinline__ void luma_six_tap_fixed(const uint8_t *ref, int s, in
 
 template <int MT>
 __global__ void __launch_bounds__(MT, 768 / MT) mc_frames_kernel(McJobs J) {
-    int k = 0;
-    while (k + 1 < J.n && J.cta_off[k + 1] <= (int)blockIdx.x) ++k;
+    int k = 0, hi = J.n - 1;                      // binary search for the frame of this CTA
+    while (k < hi) {
+        const int mid = (k + hi + 1) >> 1;
+        if (J.cta_off[mid] <= (int)blockIdx.x) k = mid;
+        else hi = mid - 1;
+    }
     const McFrame &F = J.f[k];
     const int gw = (F.W + 7) >> 3, gh = (F.H + 7) >> 3;
     const int g = ((int)blockIdx.x - J.cta_off[k]) * MT + (int)threadIdx.x;
