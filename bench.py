@@ -65,7 +65,8 @@ METRIC = "1080p v2 encode frames/s (bit-exact), batched/served vs plain GPU; p50
 UNIT = "frames/s"
 GOLDEN = os.path.join(ROOT, "tests", "golden", "bench_1080p_gop4b.json")
 GRAPHS = False   # --graphs: batched / served steps replayed as CUDA graphs
-TRAFFIC = os.path.join(ROOT, "profiles", "ctu_engine_traffic.txt")   # JSON body
+TRAFFIC = os.path.join(ROOT, "profiles", "ctu_engine_traffic.txt")
+OPS = os.path.join(ROOT, "profiles", "ctu_engine_ops.txt")   # work counts per frame (profiling build)   # JSON body
 MIXED_GOLDEN = os.path.join(ROOT, "tests", "golden", "mixed_streams.json")
 SERVED_BUDGET = 150 * 10**9          # HBM budget of the served form (bytes)
 
@@ -672,6 +673,26 @@ def main():
         t = json.load(open(TRAFFIC))["measured"]
         per_ctu = (t["dram_read_bytes"] + t["dram_write_bytes"]) / t["ctus"]
         traffic = per_ctu * dev_run["ctu_count"] / launches
+    # Integer work of the engine (the bound the byte roofline does not show):
+    # the profiling build's per-frame counts of integer-search SAD pixel
+    # differences and coded transform units, which are the same in this
+    # build (the encode is deterministic), over this run's engine time.
+    integer_work = None
+    if os.path.exists(OPS):
+        o = json.load(open(OPS))
+        pf = o["per_frame"]
+        fr_s = frames_in_launches / (dev_run["ctu_ms"] / 1000.0)          # frames per engine-second
+        sad = pf["int_sad_px"] * fr_s
+        macs = (2048.0 * pf["tu8"] + 256.0 * pf["tu4"]) * fr_s
+        sms = torch.cuda.get_device_properties(0).multi_processor_count
+        clk = (clocks.get("sm_mhz") or 1965.0) * 1e6
+        lane_peak = sms * o["int32_lanes_per_sm_clock"] * clk
+        integer_work = {
+            "sad_pixel_diffs_per_s": sad, "transform_macs_per_s": macs,
+            "int32_lane_peak_ops_per_s": lane_peak,
+            "sad_frac_of_packed_peak": sad / (4.0 * lane_peak),   # four byte differences per lane op (vsadu4)
+            "transform_mac_frac": macs / lane_peak,
+            "counts": OPS, "peak_note": o["peak_note"]}
     lat = sorted(dev_run["lat"])
     p50 = lat[len(lat) // 2] * 1000 if lat else None
     p99 = lat[min(len(lat) - 1, int(0.99 * len(lat)))] * 1000 if lat else None
@@ -692,7 +713,7 @@ def main():
                      "note": "algorithmic bytes 10*W*H per frame (MC 3WH + deblock 3WH + SAO 4WH) over the "
                              "step's persistent launch; the engine is latency / integer-pipe bound, not HBM bound"},
         "ctu_engine": {"ms_per_step": dev_run["ctu_ms"] / steps, "launches_per_step": launches / steps,
-                       "ctus_per_launch": dev_run["ctu_count"] / launches},
+                       "ctus_per_launch": dev_run["ctu_count"] / launches, "integer_work": integer_work},
         "host_ms_per_step": {k: v / steps for k, v in zip(("plan_launch", "wait_device", "entropy"),
                                                           dev_run["host"])},
         "batch": {"streams_per_gpu": args.streams, "form": "batched: every stream's CTUs in one persistent "

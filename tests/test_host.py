@@ -80,3 +80,27 @@ def test_synthetic_sources_deterministic():
         for pa, pb in zip(fa, fb):
             assert np.array_equal(pa, pb)
     assert a[0][0].shape == (96, 160) and a[0][1].shape == (48, 80)
+
+
+def test_autotune_choice_table():
+    """The frame-kernel autotuner's choice table (no GPU needed to read or
+    record choices): valid variants per kernel, TMA staging for deblocking
+    only, 0 clears, other sizes untouched; invalid variants are refused."""
+    from tcodec_b200 import api
+    L = api.bind_b200(api.load_library())
+    w, h = 1234, 566
+    assert L.tcb_autotune_threads(api.KERNEL_DEBLOCK, w, h) == 0
+    for k, good, bad in ((api.KERNEL_DEBLOCK, [64, 128, 256, 64 | api.STAGING_TMA, 256 | api.STAGING_TMA], [32, 512]),
+                         (api.KERNEL_SAO, [64, 128], [256, 128 | api.STAGING_TMA]),
+                         (api.KERNEL_MC, [64, 128, 256], [96, 64 | api.STAGING_TMA])):
+        for t in good:
+            assert L.tcb_autotune_set_threads(k, w, h, t) == 0
+            assert L.tcb_autotune_threads(k, w, h) == t
+            assert L.tcb_autotune_threads(k, w + 2, h) == 0
+        for t in bad:
+            assert L.tcb_autotune_set_threads(k, w, h, t) == api.TC_ERR_PARAM
+        assert L.tcb_autotune_set_threads(k, w, h, 0) == 0
+        assert L.tcb_autotune_threads(k, w, h) == 0
+    assert L.tcb_autotune_set_threads(7, w, h, 128) == api.TC_ERR_PARAM
+    assert L.tcb_autotune_frame_kernels(w + 1, h, 4) == api.TC_ERR_PARAM     # odd width
+    assert L.tcb_autotune_frame_kernels(w, h, 0) == api.TC_ERR_PARAM         # no frames
