@@ -65,6 +65,7 @@ METRIC = "1080p v2 encode frames/s (bit-exact), batched/served vs plain GPU; p50
 UNIT = "frames/s"
 GOLDEN = os.path.join(ROOT, "tests", "golden", "bench_1080p_gop4b.json")
 GRAPHS = False   # --graphs: batched / served steps replayed as CUDA graphs
+PIPELINE = True   # batched steps entropy-code the previous step during the device step (--no-pipeline: off)
 TRAFFIC = os.path.join(ROOT, "profiles", "ctu_engine_traffic.txt")
 OPS = os.path.join(ROOT, "profiles", "ctu_engine_ops.txt")   # work counts per frame (profiling build)   # JSON body
 MIXED_GOLDEN = os.path.join(ROOT, "tests", "golden", "mixed_streams.json")
@@ -241,6 +242,8 @@ def run_mixed_batch(lib, specs, clips):
               for c in clips]
     batch = api.BatchEncoder(lib, cfgs)
     batch.set_graphs(GRAPHS)
+    if PIPELINE:
+        batch.set_pipelined(True)
     lib.tcb_batch_set_timing(batch.h, 1)
     n = len(specs)
     nf = max(len(c) for c in clips)
@@ -439,7 +442,10 @@ def run_b200(args, rank, world):
     dplanes = [tuple(torch.from_numpy(np.ascontiguousarray(p)).to(dev) for p in f) for f in clip]
     torch.cuda.synchronize()
 
-    def timed(stream_ptr, fn_step, after_warmup=None):
+    def timed(stream_ptr, fn_step, after_warmup=None, finish=None):
+        # finish (pipelined batches): the packets still pending after the
+        # last step, coded inside the timed region, so the region holds
+        # exactly the device steps and the entropy coding of its frames
         stream = torch.cuda.ExternalStream(stream_ptr)
         for t in range(Wm):
             fn_step(t)
@@ -457,6 +463,10 @@ def run_b200(args, rank, world):
             lat.append(time.perf_counter() - t0)
             frames += n
             nbytes += b
+        if finish:
+            n, b = finish()
+            frames += n
+            nbytes += b
         ev1.record(stream)
         torch.cuda.synchronize()
         if world > 1:
@@ -466,6 +476,8 @@ def run_b200(args, rank, world):
     def batch_pass(on_device):
         batch = api.BatchEncoder(lib, [make_cfg(lib) for _ in range(S)])
         batch.set_graphs(GRAPHS)
+        if PIPELINE:
+            batch.set_pipelined(True)
         lib.tcb_batch_set_timing(batch.h, 1)
         pinned = None
         if not on_device:
@@ -491,7 +503,21 @@ def run_b200(args, rank, world):
             lib.tcb_batch_get_timing(batch.h, *[ctypes.byref(x) for x in st])
             lib.tcb_batch_get_host_timing(batch.h, *[ctypes.byref(x) for x in hs])
 
-        res = timed(lib.tcb_batch_stream(batch.h), step, reset)
+        def drain():
+            pk = batch.drain()
+            if pk[0] is not None:
+                first.append(pk[0])
+            got = [p for p in pk if p is not None]
+            return len(got), sum(len(p) for p in got)
+
+        def after_warmup():
+            if PIPELINE:       # nothing pending when the timed region starts
+                pk = batch.drain()
+                if pk[0] is not None:
+                    first.append(pk[0])
+            reset()
+
+        res = timed(lib.tcb_batch_stream(batch.h), step, after_warmup, drain if PIPELINE else None)
         reset()
         tail = batch.flush()
         batch.close()
@@ -571,13 +597,17 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the mixed-batch and served forms")
     ap.add_argument("--served-sessions", type=int, default=64)
     ap.add_argument("--no-kernels", action="store_true", help="skip the standalone-kernel roofline section")
+    ap.add_argument("--no-pipeline", action="store_true",
+                    help="unpipelined batch steps (default: each call entropy-codes the previous call's frames "
+                         "during its own device step)")
     ap.add_argument("--graphs", action="store_true",
                     help="replay every batched / served step's device work as one CUDA graph")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only time the standalone frame kernels (deblock, SAO, motion compensation)")
     args = ap.parse_args()
-    global GRAPHS
+    global GRAPHS, PIPELINE
     GRAPHS = args.graphs
+    PIPELINE = not args.no_pipeline
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -717,7 +747,7 @@ def main():
         "host_ms_per_step": {k: v / steps for k, v in zip(("plan_launch", "wait_device", "entropy"),
                                                           dev_run["host"])},
         "batch": {"streams_per_gpu": args.streams, "form": "batched: every stream's CTUs in one persistent "
-                  "wavefront launch per step (tcb_batch_encode)", "cuda_graphs": GRAPHS},
+                  "wavefront launch per step (tcb_batch_encode)", "cuda_graphs": GRAPHS, "pipelined": PIPELINE},
         "plain_gpu": (None if plain is None else {"value": plain["frames"] / (plain["ms"] / 1000.0), "unit": UNIT,
                       "what": "one stream alone through the same kernels (tcb_encoder_encode_device)"}),
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(import_rec),

@@ -90,6 +90,20 @@ void tcb_batch_get_host_timing(tcb_batch_t *batch, double *plan_ms, double *wait
  * 0, or, for the last in-place update the runtime refused since the
  * previous read, 1000 * (cudaGraphNodeType + 1) + the node's position. */
 void tcb_batch_set_graphs(tcb_batch_t *batch, int enabled);
+/* Pipelined steps (default off; constant-QP streams only): each call
+ * entropy-codes the previous call's frames on host threads while its own
+ * frames run on the device, so packets arrive one call later (status
+ * TC_OK with the previous frame's packet, TC_ERR_NEED_MORE otherwise);
+ * tcb_batch_flush returns the last ones.  Packets are byte-identical to
+ * the unpipelined batch, and tc_encoder_t.recon holds the latest device
+ * step.  Set it before the first frame or after a full flush; TC_ERR_PARAM
+ * if a stream uses rate control or frames are still pending. */
+tc_error_t tcb_batch_set_pipelined(tcb_batch_t *batch, int enabled);
+/* Pipelined batch: entropy-code the frames still pending from the last call
+ * and return their packets (TC_OK), without planning or running new frames
+ * (tcb_batch_flush would also run the B-frame tails); TC_ERR_EOF when
+ * nothing is pending. */
+tc_error_t tcb_batch_drain(tcb_batch_t *batch, tc_packet_t *packets, int *status);
 int tcb_batch_get_graph_stats(tcb_batch_t *batch, int64_t *graph_launches, int64_t *graph_builds);
 
 /* ---------------------------------------------------------------------

@@ -332,6 +332,10 @@ def bind_b200(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.tcb_batch_get_timing.argtypes = [vp] + [vp] * 5
     lib.tcb_batch_get_host_timing.argtypes = [vp] + [vp] * 3
     lib.tcb_batch_set_graphs.argtypes = [vp, ctypes.c_int]
+    lib.tcb_batch_set_pipelined.argtypes = [vp, ctypes.c_int]
+    lib.tcb_batch_set_pipelined.restype = ctypes.c_int
+    lib.tcb_batch_drain.argtypes = [vp, ctypes.POINTER(Packet), ip]
+    lib.tcb_batch_drain.restype = ctypes.c_int
     lib.tcb_batch_get_graph_stats.argtypes = [vp, vp, vp]
     lib.tcb_batch_get_graph_stats.restype = ctypes.c_int
     lib.tcb_ctu_record_bytes.restype = ctypes.c_size_t
@@ -376,6 +380,25 @@ class BatchEncoder:
     def set_graphs(self, on: bool = True):
         """Replay each step's device work as one CUDA graph (tcb_batch_set_graphs)."""
         self.lib.tcb_batch_set_graphs(self.h, 1 if on else 0)
+
+    def set_pipelined(self, on: bool = True):
+        """Entropy-code each call's frames during the next call's device step
+        (tcb_batch_set_pipelined): packets arrive one call later, `flush`
+        returns the last ones."""
+        r = self.lib.tcb_batch_set_pipelined(self.h, 1 if on else 0)
+        if r != TC_OK:
+            raise RuntimeError(f"tcb_batch_set_pipelined -> {r}")
+
+    def drain(self):
+        """Pipelined batch: the packets still pending from the last call (per
+        stream, None where none), without running new frames."""
+        pk = (Packet * self.n)()
+        st = (ctypes.c_int * self.n)()
+        r = self.lib.tcb_batch_drain(self.h, pk, st)
+        if r not in (TC_OK, TC_ERR_EOF):
+            raise RuntimeError(f"tcb_batch_drain -> {r}")
+        return [ctypes.string_at(pk[i].data, pk[i].size) if r == TC_OK and st[i] == TC_OK else None
+                for i in range(self.n)]
 
     def graph_stats(self):
         """(graph launches, graph instantiations, last refused-update result)

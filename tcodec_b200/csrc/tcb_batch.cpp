@@ -44,6 +44,10 @@ struct tcb_batch {
     // CUDA-graph replay of the step's device work: executable graphs keyed
     // by the captured node sequence (P and B steps differ in topology).
     bool graphs = false;
+    // Pipelined steps (tcb_batch_set_pipelined): the streams whose frames
+    // await entropy coding from the previous step.
+    bool pipelined = false;
+    std::vector<int> prev_part;
     struct GraphSlot {
         uint64_t sig;
         cudaGraph_t tmpl;                    // the graph exec was instantiated from
@@ -245,9 +249,26 @@ tc_error_t enqueue_step(tcb_batch *b, const std::vector<int> &part, const std::v
     return TC_OK;
 }
 
-// Run stage_a..stage_d for the streams whose plan produced a frame.
-tc_error_t run_step(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkts, int *status) {
+// Entropy coding of the committed frames of `part`, one host thread per
+// stream; status[s] is the stream's result.
+tc_error_t entropy_code(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkts, int *status) {
     const int n = (int)b->encs.size();
+    std::vector<std::thread> th;
+    std::vector<tc_error_t> rs(n, TC_OK);
+    for (int s : part)
+        th.emplace_back([&, s]() { rs[s] = b->encs[s]->impl->stage_d(&pkts[s]); });
+    for (auto &t : th) t.join();
+    tc_error_t worst = TC_OK;
+    for (int s : part) {
+        status[s] = rs[s];
+        if (rs[s] != TC_OK) worst = rs[s];
+    }
+    return worst;
+}
+
+// Run stage_a..stage_d for the streams whose plan produced a frame (in a
+// pipelined batch, stage_d of the previous step's frames).
+tc_error_t run_step(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkts, int *status) {
     auto t0 = std::chrono::steady_clock::now();
     for (int s : part) {
         EncImpl &e = *b->encs[s]->impl;
@@ -306,6 +327,14 @@ tc_error_t run_step(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkt
     }
     const bool persistent = b->encs[part[0]]->impl->persistent;
     if (b->timing) { b->host_plan_ms += ms_since(t0); t0 = std::chrono::steady_clock::now(); }
+    tc_error_t worst = TC_OK;
+    // Pipelined: the previous step's frames are entropy coded now, while this
+    // step runs on the device; their packets are this call's result.
+    if (b->pipelined && !b->prev_part.empty()) {
+        const tc_error_t r = entropy_code(b, b->prev_part, pkts, status);
+        if (r != TC_OK) worst = r;
+        if (b->timing) { b->host_entropy_ms += ms_since(t0); t0 = std::chrono::steady_clock::now(); }
+    }
     if (cudaStreamSynchronize(b->st) != cudaSuccess) return TC_ERR_INTERNAL;
     if (b->timing) { b->host_wait_ms += ms_since(t0); t0 = std::chrono::steady_clock::now(); }
     if (b->timing) {
@@ -316,21 +345,29 @@ tc_error_t run_step(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkt
         b->steps++;
         b->ctu_count += (long long)b->h_items.size();
     }
-    // Entropy coding in parallel, one host thread per stream.
-    std::vector<std::thread> th;
-    std::vector<tc_error_t> rs(n, TC_OK);
-    for (int s : part)
-        th.emplace_back([&, s]() { rs[s] = b->encs[s]->impl->stage_d(&pkts[s]); });
-    for (auto &t : th) t.join();
-    if (b->timing) b->host_entropy_ms += ms_since(t0);
-    tc_error_t worst = TC_OK;
     for (int s : part) {
-        status[s] = rs[s];
+        const tc_error_t r = b->encs[s]->impl->commit_frame();
+        if (r != TC_OK) { status[s] = r; return r; }
         b->kernel_launches += b->encs[s]->impl->kernel_launches;
         b->encs[s]->impl->kernel_launches = 0;
-        if (rs[s] != TC_OK) worst = rs[s];
     }
-    return worst;
+    if (b->pipelined) {
+        b->prev_part = part;
+        return worst;
+    }
+    const tc_error_t r = entropy_code(b, part, pkts, status);
+    if (b->timing) b->host_entropy_ms += ms_since(t0);
+    return r;
+}
+
+// A call without a device step: a pipelined batch codes the frames still
+// awaiting entropy coding and returns their packets (TC_OK); otherwise
+// `none` (TC_OK from encode, TC_ERR_EOF from flush).
+tc_error_t drain(tcb_batch *b, tc_packet_t *pkts, int *status, tc_error_t none) {
+    if (b->prev_part.empty()) return none;
+    const std::vector<int> part = b->prev_part;
+    b->prev_part.clear();
+    return entropy_code(b, part, pkts, status);
 }
 
 }  // namespace
@@ -450,7 +487,7 @@ tc_error_t tcb_batch_encode(tcb_batch_t *b, const tc_pixel_t *const *y, const in
         if (r == TC_OK) part.push_back(s);
         else if (r != TC_ERR_NEED_MORE) { status[s] = r; return r; }
     }
-    if (part.empty()) return TC_OK;
+    if (part.empty()) return drain(b, packets, status, TC_OK);
     return run_step(b, part, packets, status);
 }
 
@@ -466,8 +503,31 @@ tc_error_t tcb_batch_flush(tcb_batch_t *b, tc_packet_t *packets, int *status) {
         if (r == TC_OK) part.push_back(s);
         else if (r != TC_ERR_EOF) { status[s] = r; return r; }
     }
-    if (part.empty()) return TC_ERR_EOF;
+    if (part.empty()) return drain(b, packets, status, TC_ERR_EOF);
     return run_step(b, part, packets, status);
+}
+
+tc_error_t tcb_batch_drain(tcb_batch_t *b, tc_packet_t *packets, int *status) {
+    if (!b || !packets || !status) return TC_ERR_PARAM;
+    for (size_t s = 0; s < b->encs.size(); ++s) {
+        status[s] = TC_ERR_NEED_MORE;
+        memset(&packets[s], 0, sizeof(tc_packet_t));
+    }
+    return drain(b, packets, status, TC_ERR_EOF);
+}
+
+tc_error_t tcb_batch_set_pipelined(tcb_batch_t *b, int enabled) {
+    if (!b) return TC_ERR_PARAM;
+    if (!b->prev_part.empty()) return TC_ERR_PARAM;   // frames still await entropy coding
+    for (tc_encoder_t *e : b->encs)
+        if (e && !e->impl->set_pipelined(enabled != 0)) {
+            for (tc_encoder_t *f : b->encs)
+                if (f) f->impl->set_pipelined(false);
+            b->pipelined = false;
+            return TC_ERR_PARAM;
+        }
+    b->pipelined = enabled != 0;
+    return TC_OK;
 }
 
 void tcb_batch_set_timing(tcb_batch_t *b, int enabled) {

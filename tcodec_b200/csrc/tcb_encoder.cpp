@@ -14,6 +14,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -213,6 +214,8 @@ void EncImpl::release() {
     if (ev1) cudaEventDestroy(ev1);
     if (own_st) cudaStreamDestroy(own_st);
     free(out_buf);
+    free(out_buf_alt);
+    cudaFreeHost(h_out_alt);
 }
 
 int EncImpl::free_pool_slot() const {
@@ -302,10 +305,9 @@ tc_error_t EncImpl::stage_b() {
     int qp = rc_qp;
     if (frame_type == 2) qp = clampi(qp + b_layer_qp_off, 0, 63);
 
-    // ---- header (reference src/encoder.c:2713-2819, 2365-2399) ---------
-    memset(out_buf, 0, out_buf_size);
-    fbw.init(out_buf, out_buf_size);
-    BitWriter &bw = fbw;
+    // ---- header fields (reference src/encoder.c:2713-2819, 2365-2399); the
+    // header is written with the frame's entropy coding (stage_d), since its
+    // entry-point flag depends on the previous frame's coded size
     int profile = cfg.profile, level = cfg.level_idx;
     if (profile > TC_PROFILE_MAX) profile = TC_PROFILE_BASELINE_MOBILE;
     if (level > TC_LEVEL_MAX) level = TC_LEVEL_AUTO;
@@ -319,19 +321,10 @@ tc_error_t EncImpl::stage_b() {
     if (frame_type == 2) tools |= TC_TOOL_BIPRED;
     tools |= TC_TOOL_SAO;
     if (cfg.preset >= TC_PRESET_MEDIUM) tools |= TC_TOOL_FRESH_SKIP;
-    const int use_ep = !prev_v2_valid || prev_v2_rowbytes >= 256;
-    if (use_ep) tools |= TC_TOOL_ENTRY_POINTS;
     if (bf_b_mode) flags |= TC_FLAG_EXT_HEADER;
-    bw.put_bits(TC_MAGIC_0, 8); bw.put_bits(TC_MAGIC_1, 8); bw.put_bits(TC_MAGIC_2, 8);
-    bw.put_bits(TC_VERSION_V2, 8);
-    bw.put_bits((uint32_t)(uint16_t)W, 16); bw.put_bits((uint32_t)(uint16_t)H, 16);
-    bw.put_bits(flags, 8);
-    bw.put_bits((uint8_t)(int8_t)(qp - TC_QP_DEFAULT), 8);
-    bw.put_bits((uint8_t)(poc & 0xFF), 8);
-    bw.put_bits((uint8_t)((profile << 4) | (level & 0x0F)), 8);
-    bw.put_bits(tools, 16);
-    if (bf_b_mode) bw.put_bits(frame_type == 0 ? 0 : (frame_type == 2 ? 2 : 1), 8);
-    bw.align();
+    pend.hdr_flags = flags;
+    pend.hdr_tools = tools;
+    pend.hdr_pl = (profile << 4) | (level & 0x0F);
 
     if (is_key && poc > 0)
         for (int i = 0; i < TC_REF_FRAMES; ++i) { dpb_slot[i] = -1; dpb_poc[i] = -1; }
@@ -389,7 +382,6 @@ tc_error_t EncImpl::stage_b() {
     pend.is_key = is_key;
     pend.frame_type = frame_type;
     pend.qp = qp;
-    pend.use_ep = use_ep;
     pend.rs = rs;
     pend.multiref = P.multiref;
     return TC_OK;
@@ -437,13 +429,79 @@ tc_error_t EncImpl::readback_recon() {
     return TC_OK;
 }
 
-// Entropy coding of the CTU records and sequence bookkeeping; the stream
-// must be synchronised (host copies complete).
-tc_error_t EncImpl::stage_d(tc_packet_t *pkt) {
+// Second record / packet buffers for pipelined batches (constant QP only:
+// with rate control a frame's QP depends on the previous frame's bits).
+bool EncImpl::set_pipelined(bool on) {
+    if (on && rc_method != TC_RC_CQP) return false;
+    if (on && !h_out_alt) {
+        if (cudaMallocHost(&h_out_alt, sizeof(CtuOut) * (size_t)ctu_cols * ctu_rows) != cudaSuccess) {
+            h_out_alt = nullptr;
+            return false;
+        }
+        out_buf_alt = (uint8_t *)calloc(out_buf_size, 1);
+        if (!out_buf_alt) return false;
+    }
+    pipelined = on;
+    return true;
+}
+
+// After the frame's device step has completed: the device's error word,
+// then the sequence bookkeeping the next frame's planning depends on (DPB
+// shift, temporal MV grid, frame count, reorder buffer), and the frame's
+// entropy-coding job (its pending state, records and SSE) for stage_d.  A
+// pipelined encoder switches to its second record and packet buffers here,
+// so the next device step can land while this frame is entropy coded.
+tc_error_t EncImpl::commit_frame() {
     if (persistent && h_ctrl[1]) return TC_ERR_INTERNAL;   // a bounded wait expired on the device
-    const int poc = pend.poc, is_key = pend.is_key, frame_type = pend.frame_type, qp = pend.qp;
-    const int use_ep = pend.use_ep, rs = pend.rs, multiref = pend.multiref;
+    ent.p = pend;
+    ent.sse = *h_sse;
+    ent.rec = h_out;
+    ent.buf = out_buf;
+    ent_ready = true;
+    // DPB shift: slot 3 falls out, the new reconstruction enters slot 0
+    // (reference src/encoder.c:3085-3097).
+    for (int i = TC_REF_FRAMES - 1; i > 0; --i) { dpb_slot[i] = dpb_slot[i - 1]; dpb_poc[i] = dpb_poc[i - 1]; }
+    dpb_slot[0] = pend.rs;
+    dpb_poc[0] = pend.poc;
+    frame_count++;
+    grid_cur = 1 - grid_cur;   // this frame's grid becomes the temporal predictor
+    prev_mv_valid = 1;
+    if (pend.bf_idx >= 0) {
+        bf_free.push_back(bf_frames[pend.bf_idx]);   // back to the reorder pool
+        bf_frames.erase(bf_frames.begin() + pend.bf_idx);
+        bf_pocs.erase(bf_pocs.begin() + pend.bf_idx);
+        pend.bf_idx = -1;
+    }
+    if (pipelined) {
+        std::swap(h_out, h_out_alt);
+        std::swap(out_buf, out_buf_alt);
+    }
+    return TC_OK;
+}
+
+// Header, entropy coding of the committed frame's CTU records, CRC and the
+// packet (reference src/encoder.c:2713-2819, 2906-2965).
+tc_error_t EncImpl::stage_d(tc_packet_t *pkt) {
+    if (!ent_ready) return TC_ERR_INTERNAL;
+    ent_ready = false;
+    const Pending &pd = ent.p;
+    const int poc = pd.poc, is_key = pd.is_key, frame_type = pd.frame_type, qp = pd.qp, multiref = pd.multiref;
+    const CtuOut *rec_out = ent.rec;
+    uint8_t *const buf = ent.buf;
+    const int use_ep = !prev_v2_valid || prev_v2_rowbytes >= 256;
+    memset(buf, 0, out_buf_size);
+    fbw.init(buf, out_buf_size);
     BitWriter &bw = fbw;
+    bw.put_bits(TC_MAGIC_0, 8); bw.put_bits(TC_MAGIC_1, 8); bw.put_bits(TC_MAGIC_2, 8);
+    bw.put_bits(TC_VERSION_V2, 8);
+    bw.put_bits((uint32_t)(uint16_t)W, 16); bw.put_bits((uint32_t)(uint16_t)H, 16);
+    bw.put_bits(pd.hdr_flags, 8);
+    bw.put_bits((uint8_t)(int8_t)(qp - TC_QP_DEFAULT), 8);
+    bw.put_bits((uint8_t)(poc & 0xFF), 8);
+    bw.put_bits((uint8_t)pd.hdr_pl, 8);
+    bw.put_bits((uint16_t)(pd.hdr_tools | (use_ep ? TC_TOOL_ENTRY_POINTS : 0)), 16);
+    if (bf_b_mode) bw.put_bits(frame_type == 0 ? 0 : (frame_type == 2 ? 2 : 1), 8);
+    bw.align();
     const int entropy = cfg.enable_entropy_coded ? 1 : 0;
     if (use_ep) {
         // Entry-point rows (reference src/encoder.c:2906-2965).
@@ -467,7 +525,7 @@ tc_error_t EncImpl::stage_d(tc_packet_t *pkt) {
             SyntaxSink sink{&rw, entropy ? &rc : nullptr, ctx};
             for (int c = 0; c < ctu_cols; ++c) {
                 const CtuGeom g{c * 64, r * 64, W, H, frame_type, multiref};
-                write_ctu_syntax(sink, h_out[r * ctu_cols + c], g);
+                write_ctu_syntax(sink, rec_out[r * ctu_cols + c], g);
             }
             if (entropy) rc.flush();
             rw.align();
@@ -475,11 +533,11 @@ tc_error_t EncImpl::stage_d(tc_packet_t *pkt) {
             const size_t rb = rw.bytes();
             if (rb > per_row || bw.byte_pos + rb > out_buf_size) return TC_ERR_MEMORY;
             row_off[r] = (uint32_t)(bw.byte_pos - ep_payload);
-            memcpy(out_buf + bw.byte_pos, row_buf.data(), rb);
+            memcpy(buf + bw.byte_pos, row_buf.data(), rb);
             bw.byte_pos += rb;
         }
         for (int i = 0; i < nrows; ++i) {
-            uint8_t *p = out_buf + ep_table + (size_t)i * 4;
+            uint8_t *p = buf + ep_table + (size_t)i * 4;
             p[0] = (uint8_t)(row_off[i] >> 24); p[1] = (uint8_t)(row_off[i] >> 16);
             p[2] = (uint8_t)(row_off[i] >> 8);  p[3] = (uint8_t)row_off[i];
         }
@@ -492,13 +550,13 @@ tc_error_t EncImpl::stage_d(tc_packet_t *pkt) {
         for (int r = 0; r < ctu_rows; ++r)
             for (int c = 0; c < ctu_cols; ++c) {
                 const CtuGeom g{c * 64, r * 64, W, H, frame_type, multiref};
-                write_ctu_syntax(sink, h_out[r * ctu_cols + c], g);
+                write_ctu_syntax(sink, rec_out[r * ctu_cols + c], g);
             }
         if (entropy) rc.flush();
         bw.align();
     }
     if (cfg.enable_crc) {
-        const uint16_t crc = crc16_ccitt(out_buf, bw.bytes());
+        const uint16_t crc = crc16_ccitt(buf, bw.bytes());
         bw.put_bits(crc >> 8, 8);
         bw.put_bits(crc & 0xFF, 8);
     }
@@ -508,36 +566,19 @@ tc_error_t EncImpl::stage_d(tc_packet_t *pkt) {
     if (ctu_rows > 0) { prev_v2_rowbytes = frame_bytes / (size_t)ctu_rows; prev_v2_valid = 1; }
 
     // PSNR statistic (reference src/tcodec.c:34-54) from the device SSE.
-    const unsigned long long sse = *h_sse;
+    const unsigned long long sse = ent.sse;
     double psnr = 100.0;
     if (sse) {
         const double mse = (double)sse / ((double)W * (double)H);
         psnr = 10.0 * log10(255.0 * 255.0 / mse);
     }
     sum_psnr += psnr;
-
-    // DPB shift: slot 3 falls out, the new reconstruction enters slot 0
-    // (reference src/encoder.c:3085-3097).
-    for (int i = TC_REF_FRAMES - 1; i > 0; --i) { dpb_slot[i] = dpb_slot[i - 1]; dpb_poc[i] = dpb_poc[i - 1]; }
-    dpb_slot[0] = rs;
-    dpb_poc[0] = poc;
-    (void)qp;
-
-    pkt->data = out_buf;
+    pkt->data = buf;
     pkt->size = frame_bytes;
     pkt->pts = poc;
     pkt->key_frame = is_key;
     total_bytes += (long long)frame_bytes;
     total_frames++;
-    frame_count++;
-    grid_cur = 1 - grid_cur;   // this frame's grid becomes the temporal predictor
-    prev_mv_valid = 1;
-    if (pend.bf_idx >= 0) {
-        bf_free.push_back(bf_frames[pend.bf_idx]);   // back to the reorder pool
-        bf_frames.erase(bf_frames.begin() + pend.bf_idx);
-        bf_pocs.erase(bf_pocs.begin() + pend.bf_idx);
-        pend.bf_idx = -1;
-    }
     return TC_OK;
 }
 
@@ -557,6 +598,7 @@ tc_error_t EncImpl::encode_planned(tc_packet_t *pkt) {
         ctu_count += (long long)ctu_cols * ctu_rows;
         frames_timed++;
     }
+    if ((r = commit_frame()) != TC_OK) return r;
     return stage_d(pkt);
 }
 

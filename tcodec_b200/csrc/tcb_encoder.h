@@ -105,10 +105,26 @@ struct EncImpl {
     bool dcopy(const DevFrame &dst, const DevFrame &src);
     // staged frame driver
     struct Pending {
-        int poc = 0, qp_off = 0, need_hist = 0, is_key = 0, frame_type = 0, qp = 0, use_ep = 0,
+        int poc = 0, qp_off = 0, need_hist = 0, is_key = 0, frame_type = 0, qp = 0,
             rs = -1, multiref = 0, bf_idx = -1, glob = 0;
+        int hdr_flags = 0, hdr_tools = 0, hdr_pl = 0;   // frame header fields (entry-point bit added at coding)
         const uint8_t *glob_ref = nullptr;
     } pend;
+    // The frame committed after its device step, awaiting entropy coding.
+    struct EntropyJob {
+        Pending p;
+        unsigned long long sse = 0;
+        const CtuOut *rec = nullptr;   // its decision records (host copy)
+        uint8_t *buf = nullptr;        // its packet buffer
+    } ent;
+    bool ent_ready = false;
+    // Pipelined batches (constant QP only): second record and packet
+    // buffers, swapped at every commit, so one frame is entropy coded while
+    // the next one's device step runs.
+    bool pipelined = false;
+    CtuOut *h_out_alt = nullptr;
+    uint8_t *out_buf_alt = nullptr;
+    bool set_pipelined(bool on);
     // Batched streams leave the global-motion walk to the batch, which runs
     // every stream's walk in one launch on the batch's parameter copies.
     bool defer_glob = false;
@@ -121,6 +137,7 @@ struct EncImpl {
     tc_error_t launch_own();
     tc_error_t stage_c(bool with_recon = true);   // copy-back; the host recon copy unless with_recon is false
     tc_error_t readback_recon();
+    tc_error_t commit_frame();
     tc_error_t stage_d(tc_packet_t *pkt);
     tc_error_t encode_planned(tc_packet_t *pkt);
     tc_error_t bf_plan_scheduled();

@@ -46,7 +46,6 @@ namespace {
 // times each per frame size, 128 without tuning.  Small
 // CTAs let many CTUs' loads be in flight per SM while other CTUs of the
 // same SM filter.
-constexpr int FILTER_DEFAULT_THREADS = 128;
 
 // The frame whose CTA range [off[k], off[k+1]) holds CTA g (binary search
 // over the n <= 32 frames of a launch; off[0] = 0 <= g).
