@@ -57,14 +57,18 @@ struct Scratch {
     }
 };
 
-// Median time of `reps` calls of fn after one warm-up call.
+// Median over `reps` samples of the time of `inner` back-to-back calls of
+// fn, after one warm-up call.  A single call of a 32-frame launch lasts
+// about 50 us, too short against event-timing noise to separate variants
+// that differ by 10 %; several calls per sample are not.
 template <class F>
-float time_ms(F fn, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1, int reps, bool *ok) {
+float time_ms(F fn, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1, int reps, int inner, bool *ok) {
     std::vector<float> t;
     if (fn() != cudaSuccess) { *ok = false; return 0.f; }
     for (int r = 0; r < reps; ++r) {
         cudaEventRecord(e0, st);
-        if (fn() != cudaSuccess) { *ok = false; return 0.f; }
+        for (int i = 0; i < inner; ++i)
+            if (fn() != cudaSuccess) { *ok = false; return 0.f; }
         cudaEventRecord(e1, st);
         if (cudaEventSynchronize(e1) != cudaSuccess) { *ok = false; return 0.f; }
         float ms = 0.f;
@@ -148,7 +152,7 @@ tc_error_t tcb_autotune_frame_kernels(int width, int height, int frames) {
                         if (v.kernel == TCB_KERNEL_SAO) return launch_sao_frames(sao.data(), frames, st, th);
                         return launch_mc_frames(mc.data(), frames, st, th);
                     },
-                    st, e0, e1, 5, &ok);
+                    st, e0, e1, 7, 4, &ok);
                 if (!ok) { r = TC_ERR_INTERNAL; break; }
                 if (!best || ms < best_ms) { best = th; best_ms = ms; }
             }
