@@ -9,9 +9,10 @@
 // neighbouring blocks, so its loads and stores are contiguous runs): thread
 // h produces luma columns 4h..4h+3 of the block and chroma plane h (Cb, Cr).
 // The six-tap and bilinear paths run on packed sample pairs
-// (tcb_mc_pairs.cuh); blocks near the frame edge take the per-sample
-// arithmetic of the CTU engine (tcb_pixel.cuh), so predictions equal the
-// encoder's.
+// (tcb_mc_pairs.cuh) for planes whose stride is a multiple of 4 bytes;
+// blocks near the frame edge, and planes with other strides, take the
+// per-sample arithmetic of the CTU engine (tcb_pixel.cuh), so predictions
+// equal the encoder's.
 #include <cuda_runtime.h>
 
 #include "../../include/tcodec_b200.h"
@@ -100,7 +101,7 @@ __global__ void __launch_bounds__(MT, 768 / MT) mc_frames_kernel(McJobs J) {
         if (dx == 0 && dy == 0 && fx >= 0 && fy >= 0 && fx + 8 <= F.W && fy + 8 <= F.H) {
 #pragma unroll
             for (int y = 0; y < 8; ++y) out[y] = mc_load4(F.ry + (size_t)(fy + y) * F.sy + fx + 4 * h);
-        } else if ((dx | dy) != 0 && fx >= 2 && fx + 10 < F.W && fy >= 2 && fy + 10 < F.H) {
+        } else if ((dx | dy) != 0 && fx >= 2 && fx + 10 < F.W && fy >= 2 && fy + 10 < F.H && (F.sy & 3) == 0) {
             // Blocks of one warp that share the phase (coherent motion) take
             // the path specialised for it; mixed phases take the selecting one.
             const int phase = dx * 4 + dy;
@@ -134,7 +135,7 @@ __global__ void __launch_bounds__(MT, 768 / MT) mc_frames_kernel(McJobs J) {
         const uint8_t *ref = h ? F.rcr : F.rcb;
         const int xi = mvx >> 3, yi = mvy >> 3;
         uint32_t out[4];
-        if (xi >= 0 && xi + 4 < Wc && yi >= 0 && yi + 4 < Hc) {
+        if (xi >= 0 && xi + 4 < Wc && yi >= 0 && yi + 4 < Hc && (F.sc & 3) == 0) {
             mc_chroma_bilinear(ref, F.sc, xi, yi, mvx & 7, mvy & 7, out);
         } else {
             for (int y = 0; y < 4; ++y) {

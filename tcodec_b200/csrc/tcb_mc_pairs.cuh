@@ -34,26 +34,27 @@ __host__ __device__ __forceinline__ uint32_t mc_ld32(const uint32_t *p) {
 #endif
 }
 
-// The bytes p[0..7] as u0, u1 and p[8] as the low byte of u2, from the
-// three aligned words that hold them (each holds at least one of the
-// bytes asked for, so no word lies outside the pages the caller may read).
-__host__ __device__ __forceinline__ void mc_load9(const uint8_t *p, uint32_t &u0, uint32_t &u1, uint32_t &u2) {
-    const uintptr_t a = (uintptr_t)p;
-    const uint32_t *w = (const uint32_t *)(a & ~(uintptr_t)3);
-    const uint32_t sh = (uint32_t)(a & 3) * 8;
+// The same nine / five bytes from words already aligned: w is the aligned
+// word holding the first byte and sh its byte offset times 8.  With a row
+// stride that is a multiple of 4 every row has the same offset, so a block's
+// rows step w by the stride in words and compute the alignment once.
+__host__ __device__ __forceinline__ void mc_load9w(const uint32_t *w, uint32_t sh, uint32_t &u0, uint32_t &u1,
+                                                 uint32_t &u2) {
     const uint32_t w0 = mc_ld32(w), w1 = mc_ld32(w + 1), w2 = mc_ld32(w + 2);
     u0 = pair_fshr(w0, w1, sh);
     u1 = pair_fshr(w1, w2, sh);
     u2 = w2 >> sh;
 }
-// The bytes p[0..3] as u0 and p[4] as the low byte of u1.
-__host__ __device__ __forceinline__ void mc_load5(const uint8_t *p, uint32_t &u0, uint32_t &u1) {
-    const uintptr_t a = (uintptr_t)p;
-    const uint32_t *w = (const uint32_t *)(a & ~(uintptr_t)3);
-    const uint32_t sh = (uint32_t)(a & 3) * 8;
+__host__ __device__ __forceinline__ void mc_load5w(const uint32_t *w, uint32_t sh, uint32_t &u0, uint32_t &u1) {
     const uint32_t w0 = mc_ld32(w), w1 = mc_ld32(w + 1);
     u0 = pair_fshr(w0, w1, sh);
     u1 = w1 >> sh;
+}
+// The aligned word holding byte p, and p's offset in it times 8.
+__host__ __device__ __forceinline__ const uint32_t *mc_align(const uint8_t *p, uint32_t &sh) {
+    const uintptr_t a = (uintptr_t)p;
+    sh = (uint32_t)(a & 3) * 8;
+    return (const uint32_t *)(a & ~(uintptr_t)3);
 }
 // The bytes p[0..3] (as one little-endian word).
 __host__ __device__ __forceinline__ uint32_t mc_load4(const uint8_t *p) {
@@ -65,8 +66,8 @@ __host__ __device__ __forceinline__ uint32_t mc_load4(const uint8_t *p) {
 
 // Columns 4h..4h+3 of the 8x8 luma prediction at integer position (fx, fy),
 // quarter phase ph (PairPhase or PairPhaseFixed); the caller guarantees
-// fx >= 2, fx + 10 < W, fy >= 2, fy + 10 < H.  out[y] holds row y's four
-// samples.
+// fx >= 2, fx + 10 < W, fy >= 2, fy + 10 < H and a stride s that is a
+// multiple of 4.  out[y] holds row y's four samples.
 template <class Phase>
 __host__ __device__ __forceinline__ void mc_luma_six_tap(const uint8_t *ref, int s, int fx, int fy, int h,
                                                        const Phase &ph, uint32_t out[8]) {
@@ -75,11 +76,13 @@ __host__ __device__ __forceinline__ void mc_luma_six_tap(const uint8_t *ref, int
     // (4h+1, 4h+2), (4h+3, 4h+4); horizontal halves H0, H1 at the two even
     // pairs (biased).
     uint32_t E1[13], E2[13], E3[13], O1[13], O2[13], H0[13], H1[13];
-    const uint8_t *p = ref + (ptrdiff_t)(fy - 2) * s + fx + 4 * h - 2;
+    uint32_t sh;
+    const uint32_t *w = mc_align(ref + (ptrdiff_t)(fy - 2) * s + fx + 4 * h - 2, sh);
+    const int sw = s >> 2;
 #pragma unroll
-    for (int r = 0; r < 13; ++r, p += s) {
+    for (int r = 0; r < 13; ++r, w += sw) {
         uint32_t u0, u1, u2;
-        mc_load9(p, u0, u1, u2);                          // columns 4h-2 .. 4h+6
+        mc_load9w(w, sh, u0, u1, u2);                     // columns 4h-2 .. 4h+6
         const uint32_t x0 = pair_lo(u0), x1 = pair_hi(u0), x2 = pair_lo(u1), x3 = pair_hi(u1), x4 = pair_lo(u2);
         const uint32_t o0 = pair_mid(x0, x1), o1 = pair_mid(x1, x2), o2 = pair_mid(x2, x3), o3 = pair_mid(x3, x4);
         E1[r] = x1; E2[r] = x2; E3[r] = x3; O1[r] = o1; O2[r] = o2;
@@ -108,16 +111,19 @@ __host__ __device__ __forceinline__ void mc_luma_six_tap(const uint8_t *ref, int
 
 // The 4x4 chroma prediction at 1/8-sample position (xi + fx/8, yi + fy/8);
 // the caller guarantees xi >= 0, xi + 4 < W, yi >= 0, yi + 4 < H (no
-// coordinate clamps).  out[y] holds row y's four samples.
+// coordinate clamps) and a stride s that is a multiple of 4.  out[y] holds
+// row y's four samples.
 __host__ __device__ __forceinline__ void mc_chroma_bilinear(const uint8_t *ref, int s, int xi, int yi, int fx,
                                                           int fy, uint32_t out[4]) {
     const uint32_t w00 = (8 - fx) * (8 - fy), w01 = fx * (8 - fy), w10 = (8 - fx) * fy, w11 = fx * fy;
     uint32_t A0[5], A1[5], B0[5], B1[5];   // pairs at columns (0,1), (2,3) and (1,2), (3,4)
-    const uint8_t *p = ref + (ptrdiff_t)yi * s + xi;
+    uint32_t sh;
+    const uint32_t *w = mc_align(ref + (ptrdiff_t)yi * s + xi, sh);
+    const int sw = s >> 2;
 #pragma unroll
-    for (int r = 0; r < 5; ++r, p += s) {
+    for (int r = 0; r < 5; ++r, w += sw) {
         uint32_t u0, u1;
-        mc_load5(p, u0, u1);
+        mc_load5w(w, sh, u0, u1);
         const uint32_t x0 = pair_lo(u0), x1 = pair_hi(u0), x2 = pair_lo(u1);
         A0[r] = x0; A1[r] = x1; B0[r] = pair_mid(x0, x1); B1[r] = pair_mid(x1, x2);
     }
