@@ -1,11 +1,13 @@
 // tcb_batch.cpp — batched form of the v2 encoder: N independent streams
 // (any mix of resolutions, QPs, presets) advance one frame per call and
-// share every CTU-engine launch.  Step d of the call launches, in ONE
-// kernel, the CTUs on anti-diagonal d of every participating stream, so a
-// 1080p stream's ~11 CTUs per diagonal are joined by everyone else's and
-// the 148 SMs fill up.  Per-stream host work (frame type, header, entropy
-// coding) runs on host threads in parallel; all device work is ordered on
-// the batch's CUDA stream.
+// share one CTU-engine launch per call: a persistent kernel drains a queue
+// holding every participating stream's CTUs in anti-diagonal order, so a
+// 1080p stream's at most 9 CTUs per diagonal are joined by everyone else's
+// and the 148 SMs fill up.  Per-stream entropy coding runs on host
+// threads in parallel; all device work is ordered on the batch's CUDA
+// stream, optionally replayed as a CUDA graph, and optionally pipelined
+// (each call entropy-codes the previous call's frames during its own
+// device step).
 #include <string.h>
 
 #include <algorithm>

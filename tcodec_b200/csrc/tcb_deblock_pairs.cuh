@@ -43,19 +43,22 @@ __host__ __device__ __forceinline__ uint32_t deblock_keep(uint32_t p0, uint32_t 
 // with A = 9 (q0 - p0) - 3 (q1 - p1), p0 + clamp((A + 8) >> 4, +-tc) and
 // q0 - clamp((A + 7) >> 4, +-tc) (the reference's (8 - A) >> 4 for the q
 // side, negated), both clamped to 0..255, in the lanes not kept.
-// A is carried with a bias of 3072 (lanes 20..6140), the deltas with 192.
+// A is carried with a bias of 4096 (lanes 1044..7164) and the deltas and
+// results with 256: a result clamped to 256..511 holds the sample in its
+// low byte, and only the low bytes of p0 and q0 are used afterwards (bit 8
+// of a filtered lane stays set).
 __host__ __device__ __forceinline__ void deblock_luma_pair(uint32_t p1, uint32_t &p0, uint32_t &q0, uint32_t q1,
                                                          uint32_t t3, uint32_t tc) {
     const uint32_t one = 0x00010001u;
-    const uint32_t s1 = q0 * 9u + p1 * 3u + (3072u + 8u) * one;
+    const uint32_t s1 = q0 * 9u + p1 * 3u + (4096u + 8u) * one;
     const uint32_t s2 = p0 * 9u + q1 * 3u;
-    const uint32_t a8 = s1 - s2;                                 // A + 8 + 3072
-    const uint32_t lo = (192u - tc) * one, hi = (192u + tc) * one;
+    const uint32_t a8 = s1 - s2;                                 // A + 8 + 4096
+    const uint32_t lo = (256u - tc) * one, hi = (256u + tc) * one;
     const uint32_t dp = pair_min(pair_max((a8 >> 4) & 0x0FFF0FFFu, lo), hi);
     const uint32_t dq = pair_min(pair_max(((a8 - one) >> 4) & 0x0FFF0FFFu, lo), hi);
-    const uint32_t b0 = 192u * one, b255 = (192u + 255u) * one;
-    const uint32_t np = pair_min(pair_max(p0 + dp, b0), b255) - b0;
-    const uint32_t nq = pair_min(pair_max(q0 + 2u * b0 - dq, b0), b255) - b0;
+    const uint32_t b0 = 256u * one, b255 = 511u * one;
+    const uint32_t np = pair_min(pair_max(p0 + dp, b0), b255);
+    const uint32_t nq = pair_min(pair_max(q0 + 2u * b0 - dq, b0), b255);
     const uint32_t keep = deblock_keep(p0, q0, t3);
     p0 = (p0 & keep) | (np & ~keep);
     q0 = (q0 & keep) | (nq & ~keep);
@@ -63,13 +66,14 @@ __host__ __device__ __forceinline__ void deblock_luma_pair(uint32_t p1, uint32_t
 
 // Chroma filter (reference src/filter.c:196-234): delta =
 // clamp((q0 - p0 + 1) >> 1, +-tc), p0 + delta and q0 - delta clamped to
-// 0..255, in the lanes not kept.  The delta is carried with a bias of 128.
+// 0..255, in the lanes not kept.  The delta and the results carry a bias of
+// 256 as in the luma filter (sample in the low byte).
 __host__ __device__ __forceinline__ void deblock_chroma_pair(uint32_t &p0, uint32_t &q0, uint32_t keep, uint32_t tc) {
-    const uint32_t one = 0x00010001u, b0 = 128u * one, b255 = (128u + 255u) * one;
-    const uint32_t d = ((q0 + 257u * one - p0) >> 1) & 0x7FFF7FFFu;
-    const uint32_t dc = pair_min(pair_max(d, (128u - tc) * one), (128u + tc) * one);
-    const uint32_t np = pair_min(pair_max(p0 + dc, b0), b255) - b0;
-    const uint32_t nq = pair_min(pair_max(q0 + 2u * b0 - dc, b0), b255) - b0;
+    const uint32_t one = 0x00010001u, b0 = 256u * one, b255 = 511u * one;
+    const uint32_t d = ((q0 + 513u * one - p0) >> 1) & 0x7FFF7FFFu;
+    const uint32_t dc = pair_min(pair_max(d, (256u - tc) * one), (256u + tc) * one);
+    const uint32_t np = pair_min(pair_max(p0 + dc, b0), b255);
+    const uint32_t nq = pair_min(pair_max(q0 + 2u * b0 - dc, b0), b255);
     p0 = (p0 & keep) | (np & ~keep);
     q0 = (q0 & keep) | (nq & ~keep);
 }

@@ -246,10 +246,13 @@ bool EncImpl::dcopy(const DevFrame &dst, const DevFrame &src) {
 // ---------------------------------------------------------------------------
 // Frame driver, in stages so that many streams can share each CTU-engine
 // launch (batched form): plan (B-frame schedule) -> stage_a (scene-cut
-// histogram) -> stage_b (frame type, header, device parameters, global
-// motion hint) -> wavefront launches -> stage_c (copy-back) -> stage_d
-// (entropy coding, DPB update).  Single-stream encodes run the same stages
-// back to back (reference src/encoder.c:2625-3121 encode_poc_frame).
+// histogram) -> stage_b (frame type, header fields, device parameters,
+// global motion hint) -> wavefront launches -> stage_c (copy-back) ->
+// commit_frame (DPB update and the other bookkeeping the next frame needs)
+// -> stage_d (header, entropy coding, packet).  Single-stream encodes run
+// the same stages back to back (reference src/encoder.c:2625-3121
+// encode_poc_frame); a pipelined batch runs stage_d of one frame during the
+// next frame's device step.
 // ---------------------------------------------------------------------------
 tc_error_t EncImpl::stage_a(int poc, int b_layer_qp_off) {
     pend.poc = poc;
