@@ -34,12 +34,15 @@ __global__ void fill_bytes(uint8_t *p, size_t n, uint32_t seed) {
     }
 }
 
-// Quarter-sample vectors within +-24 samples.
-__global__ void fill_mv(int16_t *mv, int n, uint32_t seed) {
+// Quarter-sample vectors within +-24 samples (random), or one fractional
+// vector (+2.5, +0.75) samples for every block (coherent motion, where
+// blocks of a warp share their phase).  The two load the MC kernel
+// differently, so the scratch frames alternate between them.
+__global__ void fill_mv(int16_t *mv, int n, uint32_t seed, int coherent) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t x = (uint32_t)i * 2654435761u ^ seed;
         x ^= x >> 15; x *= 2246822519u; x ^= x >> 13;
-        mv[i] = (int16_t)((int)(x % 193u) - 96);
+        mv[i] = coherent ? (int16_t)((i & 1) ? 3 : 10) : (int16_t)((int)(x % 193u) - 96);
     }
 }
 
@@ -125,7 +128,7 @@ tc_error_t tcb_autotune_frame_kernels(int width, int height, int frames) {
         fill_bytes<<<256, 256, 0, st>>>(cb, (size_t)sc * hc, 17u * f + 2);
         fill_bytes<<<256, 256, 0, st>>>(cr, (size_t)sc * hc, 17u * f + 3);
         fill_bytes<<<256, 256, 0, st>>>(src, (size_t)sy * height, 17u * f + 4);
-        fill_mv<<<64, 256, 0, st>>>(mv, gw * gh * 2, 17u * f + 5);
+        fill_mv<<<64, 256, 0, st>>>(mv, gw * gh * 2, 17u * f + 5, f & 1);
         db[f] = {y, cb, cr, width, height, sy, sc, 32};
         sao[f] = {y, src, width, height, sy, sy, (int)tc_lambda_host(32), params};
         mc[f].width = width; mc[f].height = height; mc[f].stride_y = sy; mc[f].stride_c = sc;

@@ -12,7 +12,8 @@
 // (tcb_mc_pairs.cuh) for planes whose stride is a multiple of 4 bytes;
 // blocks near the frame edge, and planes with other strides, take the
 // per-sample arithmetic of the CTU engine (tcb_pixel.cuh), so predictions
-// equal the encoder's.
+// equal the encoder's; a CTA queues those blocks and all of its threads
+// share their samples after its packed blocks (McEdge below).
 #include <cuda_runtime.h>
 
 #include "../../include/tcodec_b200.h"
@@ -78,8 +79,57 @@ __device__ __forceinline__ void luma_six_tap_fixed(const uint8_t *ref, int s, in
     }
 }
 
+// The per-sample edge-safe path costs 30-40 times the packed one.  A block
+// that needs it would hold its whole warp (16 blocks) for that long, so its
+// threads only queue it in shared memory; once the CTA's packed blocks are
+// done, all MT threads share the queued blocks' samples, one sample each.
+// (Sharing within the warp instead, without the CTA barrier, measured 5 %
+// slower on random vectors.)
+struct McEdge {
+    int h, X, Y, mvx, mvy;
+    __device__ __forceinline__ McEdge(const McFrame &F, int g) {
+        const int gw = (F.W + 7) >> 3, blk = g >> 1;
+        h = g & 1;
+        const int by = blk / gw, bx = blk - by * gw;
+        X = bx * 8;
+        Y = by * 8;
+        mvx = X * 4 + F.mv[2 * blk];
+        mvy = Y * 4 + F.mv[2 * blk + 1];
+    }
+};
+
+// The queued half blocks (entries: thread indices within the CTA, whose
+// first element is g0), one sample per thread: luma 32 per entry (4 columns
+// x 8 rows), chroma 16 (the 4x4 block of plane h).  Not inlined, so that
+// its registers do not add to the packed path's; the frame comes by value,
+// as an address into the kernel parameter would copy every frame to the
+// stack.
+template <int MT>
+__device__ __noinline__ void mc_edge_samples(const McFrame F, int g0, const uint16_t *q_luma, int n_luma,
+                                             const uint16_t *q_chroma, int n_chroma) {
+    const int nl = n_luma * 32, nc = n_chroma * 16;
+    for (int i = threadIdx.x; i < nl; i += MT) {
+        const McEdge B(F, g0 + q_luma[i >> 5]);
+        const int c = i & 3, y = (i >> 2) & 7, x = B.X + 4 * B.h + c;
+        if (x < F.W && B.Y + y < F.H)
+            F.py[(size_t)(B.Y + y) * F.sy + x] = (uint8_t)interp_luma_safe(
+                F.ry, F.sy, F.W, F.H, (B.mvx >> 2) + 4 * B.h + c, (B.mvy >> 2) + y, B.mvx & 3, B.mvy & 3);
+    }
+    for (int i = threadIdx.x; i < nc; i += MT) {
+        const McEdge B(F, g0 + q_chroma[i >> 4]);
+        const int Wc = F.W >> 1, Hc = F.H >> 1, c = i & 3, y = (i >> 2) & 3;
+        const int x = (B.X >> 1) + c, yy = (B.Y >> 1) + y;
+        if (x < Wc && yy < Hc)
+            (B.h ? F.pcr : F.pcb)[(size_t)yy * F.sc + x] =
+                (uint8_t)chroma_mc_at(B.h ? F.rcr : F.rcb, F.sc, Wc, Hc, B.mvx, B.mvy, c, y);
+    }
+}
+
 template <int MT>
 __global__ void __launch_bounds__(MT, 768 / MT) mc_frames_kernel(McJobs J) {
+    __shared__ uint16_t q_luma[MT], q_chroma[MT];   // threads whose block takes the per-sample path
+    __shared__ int n_luma, n_chroma;
+    if (threadIdx.x == 0) n_luma = n_chroma = 0;
     int k = 0, hi = J.n - 1;                      // binary search for the frame of this CTA
     while (k < hi) {
         const int mid = (k + hi + 1) >> 1;
@@ -88,16 +138,15 @@ __global__ void __launch_bounds__(MT, 768 / MT) mc_frames_kernel(McJobs J) {
     }
     const McFrame &F = J.f[k];
     const int gw = (F.W + 7) >> 3, gh = (F.H + 7) >> 3;
-    const int g = ((int)blockIdx.x - J.cta_off[k]) * MT + (int)threadIdx.x;
-    const int blk = g >> 1, h = g & 1;
-    if (blk >= gw * gh) return;
-    const int by = blk / gw, bx = blk - by * gw;
-    const int X = bx * 8, Y = by * 8;
-    const int mvx = X * 4 + F.mv[2 * blk], mvy = Y * 4 + F.mv[2 * blk + 1];
-    // ---- luma: columns 4h..4h+3
-    {
+    const int g0 = ((int)blockIdx.x - J.cta_off[k]) * MT;
+    __syncthreads();
+    if (((g0 + (int)threadIdx.x) >> 1) < gw * gh) {
+        const McEdge B(F, g0 + (int)threadIdx.x);
+        const int h = B.h, X = B.X, Y = B.Y, mvx = B.mvx, mvy = B.mvy;
+        // ---- luma: columns 4h..4h+3
         const int fx = mvx >> 2, fy = mvy >> 2, dx = mvx & 3, dy = mvy & 3;
         uint32_t out[8];
+        bool packed = true;
         if (dx == 0 && dy == 0 && fx >= 0 && fy >= 0 && fx + 8 <= F.W && fy + 8 <= F.H) {
 #pragma unroll
             for (int y = 0; y < 8; ++y) out[y] = mc_load4(F.ry + (size_t)(fy + y) * F.sy + fx + 4 * h);
@@ -114,43 +163,33 @@ __global__ void __launch_bounds__(MT, 768 / MT) mc_frames_kernel(McJobs J) {
                 mc_luma_six_tap(F.ry, F.sy, fx, fy, h, ph, out);
             }
         } else {
-            for (int y = 0; y < 8; ++y) {
-                uint32_t v = 0;
-                for (int c = 0; c < 4; ++c)
-                    v |= (uint32_t)interp_luma_safe(F.ry, F.sy, F.W, F.H, fx + 4 * h + c, fy + y, dx, dy) << (8 * c);
-                out[y] = v;
-            }
+            q_luma[atomicAdd(&n_luma, 1)] = (uint16_t)threadIdx.x;
+            packed = false;
         }
         const int x0 = X + 4 * h, wl = min(4, F.W - x0), hl = min(8, F.H - Y);
-        if (wl > 0) {
+        if (packed && wl > 0) {
             uint8_t *dst = F.py + (size_t)Y * F.sy + x0;
 #pragma unroll
             for (int y = 0; y < 8; ++y)
                 if (y < hl) store4(dst + (size_t)y * F.sy, out[y], wl);
         }
-    }
-    // ---- chroma: plane h, the 4x4 block at (X/2, Y/2)
-    {
+        // ---- chroma: plane h, the 4x4 block at (X/2, Y/2)
         const int Wc = F.W >> 1, Hc = F.H >> 1, cx = X >> 1, cy = Y >> 1;
-        const uint8_t *ref = h ? F.rcr : F.rcb;
         const int xi = mvx >> 3, yi = mvy >> 3;
-        uint32_t out[4];
         if (xi >= 0 && xi + 4 < Wc && yi >= 0 && yi + 4 < Hc && (F.sc & 3) == 0) {
-            mc_chroma_bilinear(ref, F.sc, xi, yi, mvx & 7, mvy & 7, out);
-        } else {
-            for (int y = 0; y < 4; ++y) {
-                uint32_t v = 0;
-                for (int c = 0; c < 4; ++c)
-                    v |= (uint32_t)chroma_mc_at(ref, F.sc, Wc, Hc, mvx, mvy, c, y) << (8 * c);
-                out[y] = v;
-            }
-        }
-        const int wc = min(4, Wc - cx), hc = min(4, Hc - cy);
-        uint8_t *dst = (h ? F.pcr : F.pcb) + (size_t)cy * F.sc + cx;
+            uint32_t cout[4];
+            mc_chroma_bilinear(h ? F.rcr : F.rcb, F.sc, xi, yi, mvx & 7, mvy & 7, cout);
+            const int wc = min(4, Wc - cx), hc = min(4, Hc - cy);
+            uint8_t *dst = (h ? F.pcr : F.pcb) + (size_t)cy * F.sc + cx;
 #pragma unroll
-        for (int y = 0; y < 4; ++y)
-            if (y < hc) store4(dst + (size_t)y * F.sc, out[y], wc);
+            for (int y = 0; y < 4; ++y)
+                if (y < hc) store4(dst + (size_t)y * F.sc, cout[y], wc);
+        } else {
+            q_chroma[atomicAdd(&n_chroma, 1)] = (uint16_t)threadIdx.x;
+        }
     }
+    __syncthreads();
+    if (n_luma | n_chroma) mc_edge_samples<MT>(F, g0, q_luma, n_luma, q_chroma, n_chroma);
 }
 
 }  // namespace

@@ -74,8 +74,12 @@ __host__ __device__ __forceinline__ void mc_luma_six_tap(const uint8_t *ref, int
     // Per row r (frame row fy - 2 + r): even pairs E1..E3 at columns
     // (4h, 4h+1), (4h+2, 4h+3), (4h+4, 4h+5); odd pairs O1, O2 at
     // (4h+1, 4h+2), (4h+3, 4h+4); horizontal halves H0, H1 at the two even
-    // pairs (biased).
-    uint32_t E1[13], E2[13], E3[13], O1[13], O2[13], H0[13], H1[13];
+    // pairs (biased).  The value along x on integer row y (0..8, frame row
+    // fy + y) serves output row y as its top and row y - 1 as its bottom
+    // (T0, T1).  Output row y reads rows y..y+5 only, so it is formed as
+    // soon as row y + 5 is in: a rolling window of six rows stays live, not
+    // all thirteen.
+    uint32_t E1[13], E2[13], E3[13], H0[13], H1[13], T0[9], T1[9];
     uint32_t sh;
     const uint32_t *w = mc_align(ref + (ptrdiff_t)(fy - 2) * s + fx + 4 * h - 2, sh);
     const int sw = s >> 2;
@@ -85,27 +89,23 @@ __host__ __device__ __forceinline__ void mc_luma_six_tap(const uint8_t *ref, int
         mc_load9w(w, sh, u0, u1, u2);                     // columns 4h-2 .. 4h+6
         const uint32_t x0 = pair_lo(u0), x1 = pair_hi(u0), x2 = pair_lo(u1), x3 = pair_hi(u1), x4 = pair_lo(u2);
         const uint32_t o0 = pair_mid(x0, x1), o1 = pair_mid(x1, x2), o2 = pair_mid(x2, x3), o3 = pair_mid(x3, x4);
-        E1[r] = x1; E2[r] = x2; E3[r] = x3; O1[r] = o1; O2[r] = o2;
+        E1[r] = x1; E2[r] = x2; E3[r] = x3;
         H0[r] = pair_six_tap(x0, o0, x1, o1, x2, o2, PAIR_K_RAW);
         H1[r] = pair_six_tap(x1, o1, x2, o2, x3, o3, PAIR_K_RAW);
-    }
-    // The value along x on integer row y (0..8) serves output row y as its
-    // top and row y - 1 as its bottom.
-    uint32_t T0[9], T1[9];
-#pragma unroll
-    for (int y = 0; y < 9; ++y) {
-        T0[y] = ph.along_x(E1[y + 2] + PAIR_B, H0[y + 2], O1[y + 2] + PAIR_B);
-        T1[y] = ph.along_x(E2[y + 2] + PAIR_B, H1[y + 2], O2[y + 2] + PAIR_B);
-    }
-#pragma unroll
-    for (int y = 0; y < 8; ++y) {
-        const uint32_t c0 = pair_six_tap(E1[y], E1[y + 1], E1[y + 2], E1[y + 3], E1[y + 4], E1[y + 5], PAIR_K_RAW);
-        const uint32_t c1 = pair_six_tap(E2[y], E2[y + 1], E2[y + 2], E2[y + 3], E2[y + 4], E2[y + 5], PAIR_K_RAW);
-        const uint32_t c2 = pair_six_tap(E3[y], E3[y + 1], E3[y + 2], E3[y + 3], E3[y + 4], E3[y + 5], PAIR_K_RAW);
-        const uint32_t d0 = pair_six_tap(H0[y], H0[y + 1], H0[y + 2], H0[y + 3], H0[y + 4], H0[y + 5], PAIR_K_HALF);
-        const uint32_t d1 = pair_six_tap(H1[y], H1[y + 1], H1[y + 2], H1[y + 3], H1[y + 4], H1[y + 5], PAIR_K_HALF);
-        const uint32_t m0 = ph.along_x(c0, d0, pair_mid(c0, c1)), m1 = ph.along_x(c1, d1, pair_mid(c1, c2));
-        out[y] = pair_pack(ph.finish(T0[y], m0, T0[y + 1]), ph.finish(T1[y], m1, T1[y + 1]));
+        if (r >= 2 && r <= 10) {
+            T0[r - 2] = ph.along_x(x1 + PAIR_B, H0[r], o1 + PAIR_B);
+            T1[r - 2] = ph.along_x(x2 + PAIR_B, H1[r], o2 + PAIR_B);
+        }
+        if (r >= 5) {
+            const int y = r - 5;
+            const uint32_t c0 = pair_six_tap(E1[y], E1[y + 1], E1[y + 2], E1[y + 3], E1[y + 4], E1[y + 5], PAIR_K_RAW);
+            const uint32_t c1 = pair_six_tap(E2[y], E2[y + 1], E2[y + 2], E2[y + 3], E2[y + 4], E2[y + 5], PAIR_K_RAW);
+            const uint32_t c2 = pair_six_tap(E3[y], E3[y + 1], E3[y + 2], E3[y + 3], E3[y + 4], E3[y + 5], PAIR_K_RAW);
+            const uint32_t d0 = pair_six_tap(H0[y], H0[y + 1], H0[y + 2], H0[y + 3], H0[y + 4], H0[y + 5], PAIR_K_HALF);
+            const uint32_t d1 = pair_six_tap(H1[y], H1[y + 1], H1[y + 2], H1[y + 3], H1[y + 4], H1[y + 5], PAIR_K_HALF);
+            const uint32_t m0 = ph.along_x(c0, d0, pair_mid(c0, c1)), m1 = ph.along_x(c1, d1, pair_mid(c1, c2));
+            out[y] = pair_pack(ph.finish(T0[y], m0, T0[y + 1]), ph.finish(T1[y], m1, T1[y + 1]));
+        }
     }
 }
 
