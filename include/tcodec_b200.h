@@ -225,6 +225,32 @@ tc_error_t tcb_ctu_encode_frame(const tcb_frame_desc_t *desc, void *scratch, siz
 #define TCB_CTU_STATIC_MAX_CTUS 2048
 tc_error_t tcb_ctu_encode_frame_static(const tcb_frame_desc_t *desc, void *stream);
 
+/* Result of the last frame launched with this scratch (or with the static
+ * scratch): waits for `stream`, then returns TC_OK, or TC_ERR_INTERNAL
+ * when a CTU's wait for its left / above neighbour ran out (the frame's
+ * output is then not valid) or the device reported an error.  The two
+ * frame entry points above return once the work is queued; this is how a
+ * caller learns that it completed.  No reference counterpart (the
+ * reference's per-CTU loop cannot stall). */
+tc_error_t tcb_ctu_frame_result(const void *scratch, void *stream);
+tc_error_t tcb_ctu_frame_result_static(void *stream);
+
+/* Bound of a CTU's wait for a neighbour's publish flag, in back-off
+ * iterations of at most 2,048 ns each; default 2^22 (about 8.6 s).  Set
+ * for the current device; applies to every CTU-engine launch on it
+ * (frame entry points, encoders, batches, served sessions) that starts
+ * afterwards.  spins < 1 returns TC_ERR_PARAM. */
+tc_error_t tcb_set_neighbor_wait_limit(long long spins);
+tc_error_t tcb_get_neighbor_wait_limit(long long *spins);
+
+/* Test hook: tcb_ctu_encode_frame with the first CTU of the wavefront
+ * queue left out.  Its publish flag is never set, so the waits of its
+ * right and lower neighbours run out (bounded, see above) and
+ * tcb_ctu_frame_result reports TC_ERR_INTERNAL; the device context stays
+ * usable.  Frames of at least 2 CTUs. */
+tc_error_t tcb_debug_ctu_encode_frame_without_first(const tcb_frame_desc_t *desc, void *scratch,
+                                                    size_t scratch_bytes, void *stream);
+
 /* One frame for standalone motion compensation.  Device pointers; the
  * reference and prediction planes share stride_y / stride_c. */
 typedef struct tcb_mc_frame {

@@ -346,6 +346,16 @@ def bind_b200(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.tcb_ctu_encode_frame.restype = ctypes.c_int
     lib.tcb_ctu_encode_frame_static.argtypes = [ctypes.POINTER(FrameDesc), vp]
     lib.tcb_ctu_encode_frame_static.restype = ctypes.c_int
+    lib.tcb_ctu_frame_result.argtypes = [vp, vp]
+    lib.tcb_ctu_frame_result.restype = ctypes.c_int
+    lib.tcb_ctu_frame_result_static.argtypes = [vp]
+    lib.tcb_ctu_frame_result_static.restype = ctypes.c_int
+    lib.tcb_set_neighbor_wait_limit.argtypes = [ctypes.c_longlong]
+    lib.tcb_set_neighbor_wait_limit.restype = ctypes.c_int
+    lib.tcb_get_neighbor_wait_limit.argtypes = [ctypes.POINTER(ctypes.c_longlong)]
+    lib.tcb_get_neighbor_wait_limit.restype = ctypes.c_int
+    lib.tcb_debug_ctu_encode_frame_without_first.argtypes = [ctypes.POINTER(FrameDesc), vp, ctypes.c_size_t, vp]
+    lib.tcb_debug_ctu_encode_frame_without_first.restype = ctypes.c_int
     for fn in (lib.tcb_deblock_frames, lib.tcb_sao_frames):
         fn.argtypes = [ctypes.POINTER(FilterFrame), ctypes.c_int, vp]
         fn.restype = ctypes.c_int

@@ -1513,6 +1513,12 @@ __device__ __forceinline__ void st_release(int *p, int v) {
     asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Bound of a neighbour wait, in back-off iterations (sleeps of 32 ns
+// doubling to 2,048 ns): the default 2^22 is about 8.6 s, far above a
+// CTU's encode time even when the GPU is time-shared.  Per device; set by
+// tcb_set_neighbor_wait_limit.
+__device__ long long g_neighbor_wait_limit = 1ll << 22;
+
 // Persistent wavefront: a resident grid pulls CTUs from a queue laid out in
 // topological (anti-diagonal) order and starts each one as soon as its
 // left and above neighbours are published.  A CTU only ever waits for
@@ -1550,13 +1556,14 @@ ctu_persistent_kernel(const FrameParams *__restrict__ params, const int *__restr
             const int *du = row > 0 ? P.done + (row - 1) * P.ctu_cols + col : nullptr;
             unsigned ns = 32;
             long long spins = 0;
+            const long long limit = g_neighbor_wait_limit;
 #ifdef TCB_PHASE_PROFILE
             const long long w0 = clock64();
 #endif
             while ((dl && ld_acquire(dl) != epoch) || (du && ld_acquire(du) != epoch)) {
                 __nanosleep(ns);
                 if (ns < 2048) ns <<= 1;
-                if (++spins > (1ll << 22)) { atomicExch(&ctrl[1], 1); break; }
+                if (++spins > limit) { atomicExch(&ctrl[1], 1); break; }
             }
 #ifdef TCB_PHASE_PROFILE
             atomicAdd(&tcb_phase_cycles[13], (unsigned long long)(clock64() - w0));
@@ -1616,8 +1623,10 @@ __global__ void frame_setup_kernel(FrameParams P, uint8_t *__restrict__ scratch)
 
 // Shared host half of the frame entry points: one set-up launch fills
 // `scratch`, one persistent launch drains its queue.  Nothing is allocated
-// and nothing is copied from host memory.
-cudaError_t encode_frame_with_scratch(const FrameParams &P0, uint8_t *scratch, cudaStream_t st) {
+// and nothing is copied from host memory.  `first` > 0 leaves the queue's
+// first items out (the wait-expiry test hook: their publish flags are
+// never set, so their neighbours' bounded waits run out).
+cudaError_t encode_frame_with_scratch(const FrameParams &P0, uint8_t *scratch, cudaStream_t st, int first) {
     FrameParams P = P0;
     const int nctu = P.ctu_cols * P.ctu_rows;
     int *ctrl = (int *)(scratch + SCR_CTRL), *done = (int *)(scratch + SCR_DONE), *items = done + nctu;
@@ -1630,7 +1639,8 @@ cudaError_t encode_frame_with_scratch(const FrameParams &P0, uint8_t *scratch, c
     int dev = 0, sms = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    return launch_ctu_persistent((const FrameParams *)(scratch + SCR_PARAMS), items, nctu, ctrl, sms, st);
+    return launch_ctu_persistent((const FrameParams *)(scratch + SCR_PARAMS), items + first, nctu - first, ctrl,
+                                 sms, st);
 }
 
 // Constant tables and kernel attributes, once per device.
@@ -1723,7 +1733,7 @@ tc_error_t tcb_ctu_encode_frame(const tcb_frame_desc_t *desc, void *scratch, siz
     if (!desc || !scratch || !tcb::frame_params_from_desc(*desc, P)) return TC_ERR_PARAM;
     if (scratch_bytes < tcb::scratch_bytes_for(P.ctu_cols * P.ctu_rows)) return TC_ERR_PARAM;
     if (tcb::ensure_device_tables() != cudaSuccess) return TC_ERR_INTERNAL;
-    return tcb::encode_frame_with_scratch(P, (uint8_t *)scratch, (cudaStream_t)stream) == cudaSuccess
+    return tcb::encode_frame_with_scratch(P, (uint8_t *)scratch, (cudaStream_t)stream, 0) == cudaSuccess
                ? TC_OK : TC_ERR_INTERNAL;
 }
 
@@ -1734,8 +1744,53 @@ tc_error_t tcb_ctu_encode_frame_static(const tcb_frame_desc_t *desc, void *strea
     if (tcb::ensure_device_tables() != cudaSuccess) return TC_ERR_INTERNAL;
     uint8_t *scratch = nullptr;
     if (tcb::static_scratch_address(&scratch) != cudaSuccess) return TC_ERR_INTERNAL;
-    return tcb::encode_frame_with_scratch(P, scratch, (cudaStream_t)stream) == cudaSuccess ? TC_OK
-                                                                                           : TC_ERR_INTERNAL;
+    return tcb::encode_frame_with_scratch(P, scratch, (cudaStream_t)stream, 0) == cudaSuccess ? TC_OK
+                                                                                              : TC_ERR_INTERNAL;
+}
+
+// The frame's error word (set when a neighbour wait ran out), read once the
+// frame's work on `stream` has finished.
+static tc_error_t frame_result(const uint8_t *scratch, void *stream) {
+    int err = 0;
+    if (cudaMemcpyAsync(&err, scratch + tcb::SCR_CTRL + sizeof(int), sizeof(int), cudaMemcpyDeviceToHost,
+                        (cudaStream_t)stream) != cudaSuccess ||
+        cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess)
+        return TC_ERR_INTERNAL;
+    return err ? TC_ERR_INTERNAL : TC_OK;
+}
+
+tc_error_t tcb_ctu_frame_result(const void *scratch, void *stream) {
+    if (!scratch) return TC_ERR_PARAM;
+    return frame_result((const uint8_t *)scratch, stream);
+}
+
+tc_error_t tcb_ctu_frame_result_static(void *stream) {
+    uint8_t *scratch = nullptr;
+    if (tcb::static_scratch_address(&scratch) != cudaSuccess) return TC_ERR_INTERNAL;
+    return frame_result(scratch, stream);
+}
+
+tc_error_t tcb_set_neighbor_wait_limit(long long spins) {
+    if (spins < 1) return TC_ERR_PARAM;
+    return cudaMemcpyToSymbol(tcb::g_neighbor_wait_limit, &spins, sizeof(spins)) == cudaSuccess ? TC_OK
+                                                                                                : TC_ERR_INTERNAL;
+}
+
+tc_error_t tcb_get_neighbor_wait_limit(long long *spins) {
+    if (!spins) return TC_ERR_PARAM;
+    return cudaMemcpyFromSymbol(spins, tcb::g_neighbor_wait_limit, sizeof(*spins)) == cudaSuccess
+               ? TC_OK : TC_ERR_INTERNAL;
+}
+
+tc_error_t tcb_debug_ctu_encode_frame_without_first(const tcb_frame_desc_t *desc, void *scratch,
+                                                    size_t scratch_bytes, void *stream) {
+    tcb::FrameParams P;
+    if (!desc || !scratch || !tcb::frame_params_from_desc(*desc, P)) return TC_ERR_PARAM;
+    if (P.ctu_cols * P.ctu_rows < 2 || scratch_bytes < tcb::scratch_bytes_for(P.ctu_cols * P.ctu_rows))
+        return TC_ERR_PARAM;
+    if (tcb::ensure_device_tables() != cudaSuccess) return TC_ERR_INTERNAL;
+    return tcb::encode_frame_with_scratch(P, (uint8_t *)scratch, (cudaStream_t)stream, 1) == cudaSuccess
+               ? TC_OK : TC_ERR_INTERNAL;
 }
 
 }  // extern "C"
