@@ -251,6 +251,14 @@ tc_error_t tcb_get_neighbor_wait_limit(long long *spins);
 tc_error_t tcb_debug_ctu_encode_frame_without_first(const tcb_frame_desc_t *desc, void *scratch,
                                                     size_t scratch_bytes, void *stream);
 
+/* Test hook: the next n device or pinned-host allocations of the library
+ * succeed and the one after fails, once (n < 0: none).  Returns the count
+ * that was still pending (negative when the armed failure has happened or
+ * none was armed).  A failure surfaces as NULL from the create calls or
+ * TC_ERR_MEMORY from encode / decode / batch calls, with the object still
+ * usable or destroyable. */
+long long tcb_debug_fail_allocations_after(long long n);
+
 /* One frame for standalone motion compensation.  Device pointers; the
  * reference and prediction planes share stride_y / stride_c. */
 typedef struct tcb_mc_frame {

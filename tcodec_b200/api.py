@@ -356,6 +356,8 @@ def bind_b200(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.tcb_get_neighbor_wait_limit.restype = ctypes.c_int
     lib.tcb_debug_ctu_encode_frame_without_first.argtypes = [ctypes.POINTER(FrameDesc), vp, ctypes.c_size_t, vp]
     lib.tcb_debug_ctu_encode_frame_without_first.restype = ctypes.c_int
+    lib.tcb_debug_fail_allocations_after.argtypes = [ctypes.c_longlong]
+    lib.tcb_debug_fail_allocations_after.restype = ctypes.c_longlong
     for fn in (lib.tcb_deblock_frames, lib.tcb_sao_frames):
         fn.argtypes = [ctypes.POINTER(FilterFrame), ctypes.c_int, vp]
         fn.restype = ctypes.c_int

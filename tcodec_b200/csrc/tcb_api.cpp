@@ -9,7 +9,19 @@
 #include "../../include/tcodec.h"
 #include "tcb_encoder.h"
 
+namespace tcb {
+std::atomic<long long> g_alloc_countdown{-1};
+}  // namespace tcb
+
 extern "C" {
+
+// Arms the allocation fault injector (tcb_alloc.h): the next n device or
+// pinned-host allocations of the library succeed and the one after fails
+// (once); n < 0 disarms it.  Returns the count that was left, negative when
+// nothing was pending, so a caller can tell whether the failure happened.
+long long tcb_debug_fail_allocations_after(long long n) {
+    return tcb::g_alloc_countdown.exchange(n < 0 ? -1 : n);
+}
 
 // Host frame with 64-byte aligned strides (reference src/frame.c:19-43).
 // Pinned frames are used for the per-frame reconstruction copy.
@@ -24,8 +36,8 @@ tc_frame_buf_t *tcb_host_frame_alloc(int width, int height, int pinned) {
     f->owned = pinned ? 2 : 1;
     const size_t ys = (size_t)f->stride_y * height, cs = (size_t)f->stride_c * (height / 2);
     if (pinned) {
-        if (cudaMallocHost(&f->y, ys ? ys : 1) != cudaSuccess || cudaMallocHost(&f->cb, cs ? cs : 1) != cudaSuccess ||
-            cudaMallocHost(&f->cr, cs ? cs : 1) != cudaSuccess) {
+        if (tcb::pinned_alloc(&f->y, ys ? ys : 1) != cudaSuccess || tcb::pinned_alloc(&f->cb, cs ? cs : 1) != cudaSuccess ||
+            tcb::pinned_alloc(&f->cr, cs ? cs : 1) != cudaSuccess) {
             tcb_host_frame_free(f);
             return nullptr;
         }

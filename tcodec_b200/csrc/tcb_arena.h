@@ -17,6 +17,8 @@
 
 #include <cuda_runtime.h>
 
+#include "tcb_alloc.h"
+
 namespace tcb {
 
 class DeviceArena {
@@ -26,7 +28,7 @@ public:
 
     cudaError_t init(size_t bytes) {
         cap_ = round_up(bytes);
-        cudaError_t e = cudaMalloc(&base_, cap_);
+        cudaError_t e = dev_alloc(&base_, cap_);
         if (e != cudaSuccess) { base_ = nullptr; cap_ = 0; return e; }
         free_.clear();
         live_.clear();

@@ -54,7 +54,7 @@ struct Scratch {
     template <class T>
     T *alloc(size_t n) {
         void *p = nullptr;
-        if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+        if (dev_alloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
         bufs.push_back(p);
         return (T *)p;
     }

@@ -296,14 +296,14 @@ tc_error_t run_step(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkt
         cudaFree(b->d_items);
         b->d_items = nullptr;
         b->items_cap = 0;
-        if (cudaMalloc(&b->d_items, sizeof(int) * b->h_items.size()) != cudaSuccess) return TC_ERR_MEMORY;
+        if (tcb::dev_alloc(&b->d_items, sizeof(int) * b->h_items.size()) != cudaSuccess) return TC_ERR_MEMORY;
         b->items_cap = b->h_items.size();
     }
     if (b->h_items.size() > b->h_items_pin_cap) {
         cudaFreeHost(b->h_items_pin);
         b->h_items_pin = nullptr;
         b->h_items_pin_cap = 0;
-        if (cudaMallocHost(&b->h_items_pin, sizeof(int) * b->h_items.size()) != cudaSuccess) return TC_ERR_MEMORY;
+        if (tcb::pinned_alloc(&b->h_items_pin, sizeof(int) * b->h_items.size()) != cudaSuccess) return TC_ERR_MEMORY;
         b->h_items_pin_cap = b->h_items.size();
     }
     memcpy(b->h_items_pin, b->h_items.data(), sizeof(int) * b->h_items.size());
@@ -380,8 +380,8 @@ tcb_batch *tcb::batch_new(int cap) {
     if (!b) return nullptr;
     if (cudaGetDevice(&b->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
-        cudaMalloc(&b->d_params, sizeof(FrameParams) * cap) != cudaSuccess ||
-        cudaMalloc(&b->d_ctrl, 2 * sizeof(int)) != cudaSuccess ||
+        tcb::dev_alloc(&b->d_params, sizeof(FrameParams) * cap) != cudaSuccess ||
+        tcb::dev_alloc(&b->d_ctrl, 2 * sizeof(int)) != cudaSuccess ||
         cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess) {
         release(b);
         return nullptr;

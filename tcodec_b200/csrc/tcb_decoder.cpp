@@ -386,11 +386,14 @@ struct DecImpl {
     int crc_valid = 1, entropy = 0, threads = 4, profile = 0;
     uint64_t prof[7] = {0, 0, 0, 0, 0, 0, 0};
 
+    // All three planes or none: a partly allocated frame is freed again.
     bool alloc_frame(DevFrame &f) {
         const size_t yb = (size_t)sy * fh + 64, cb = (size_t)sc * (fh / 2) + 64;
-        if (cudaMalloc(&f.y, yb) != cudaSuccess || cudaMalloc(&f.cb, cb) != cudaSuccess ||
-            cudaMalloc(&f.cr, cb) != cudaSuccess)
+        if (dev_alloc(&f.y, yb) != cudaSuccess || dev_alloc(&f.cb, cb) != cudaSuccess ||
+            dev_alloc(&f.cr, cb) != cudaSuccess) {
+            free_frame(f);
             return false;
+        }
         cudaMemset(f.y, 0, yb); cudaMemset(f.cb, 0, cb); cudaMemset(f.cr, 0, cb);
         return true;
     }
@@ -407,7 +410,16 @@ struct DecImpl {
         tcb_host_frame_free(out);
         out = nullptr;
     }
+    // Geometry-dependent buffers for w x h.  On failure everything is
+    // released and the size forgotten, so the next frame starts over
+    // instead of decoding into a partly allocated set.
     bool setup(int w, int h) {
+        if (setup_buffers(w, h)) return true;
+        release_geometry();
+        fw = fh = 0;
+        return false;
+    }
+    bool setup_buffers(int w, int h) {
         release_geometry();
         fw = w; fh = h;
         sy = ((w + 63) / 64) * 64;
@@ -415,8 +427,8 @@ struct DecImpl {
         cols = (w + 63) / 64;
         rows = (h + 63) / 64;
         if (!alloc_frame(cur)) return false;
-        if (cudaMalloc(&d_rec, sizeof(CtuOut) * cols * rows) != cudaSuccess) return false;
-        if (cudaMallocHost(&h_rec, sizeof(CtuOut) * cols * rows) != cudaSuccess) return false;
+        if (dev_alloc(&d_rec, sizeof(CtuOut) * cols * rows) != cudaSuccess) return false;
+        if (pinned_alloc(&h_rec, sizeof(CtuOut) * cols * rows) != cudaSuccess) return false;
         std::vector<int> items;
         diag_off.clear(); diag_cnt.clear();
         for (int d = 0; d < rows + cols - 1; ++d) {
@@ -427,7 +439,7 @@ struct DecImpl {
             }
             diag_cnt.push_back((int)items.size() - diag_off.back());
         }
-        if (cudaMalloc(&d_items, sizeof(int) * items.size()) != cudaSuccess) return false;
+        if (dev_alloc(&d_items, sizeof(int) * items.size()) != cudaSuccess) return false;
         cudaMemcpy(d_items, items.data(), sizeof(int) * items.size(), cudaMemcpyHostToDevice);
         out = tcb_host_frame_alloc(w, h, 1);
         return out != nullptr;
@@ -589,7 +601,7 @@ tc_error_t DecImpl::decode(const uint8_t *data, size_t size, const tc_pixel_t **
         P.eff_l[b] = maxi((qs[P.qp] * jw[b] + 4) >> 3, 1);
         P.eff_c[b] = maxi((qs[P.qp_c] * jw[b] + 4) >> 3, 1);
     }
-    if (!d_params && cudaMalloc(&d_params, sizeof(FrameParams)) != cudaSuccess) return TC_ERR_MEMORY;
+    if (!d_params && dev_alloc(&d_params, sizeof(FrameParams)) != cudaSuccess) return TC_ERR_MEMORY;
     const int nctu = rows * cols;
     if (cudaMemcpyAsync(d_params, &P, sizeof(P), cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaMemcpyAsync(d_rec, h_rec, sizeof(CtuOut) * nctu, cudaMemcpyHostToDevice, st) != cudaSuccess)
@@ -597,11 +609,18 @@ tc_error_t DecImpl::decode(const uint8_t *data, size_t size, const tc_pixel_t **
     for (size_t d = 0; d < diag_off.size(); ++d)
         if (launch_decode_items(d_params, d_items + diag_off[d], diag_cnt[d], st) != cudaSuccess)
             return TC_ERR_INTERNAL;
-    // DPB: slot 3 falls out, a copy of the reconstruction enters slot 0.
-    if (dpb_ok[TC_REF_FRAMES - 1]) spare.push_back(dpb[TC_REF_FRAMES - 1]);
+    // DPB: slot 3 falls out and its buffer takes a copy of the
+    // reconstruction into slot 0 (another buffer when slot 3 is empty, taken
+    // before anything moves, so a failed allocation leaves the DPB as it
+    // was).  The copy follows this frame's kernels on the stream.
+    DevFrame nf;
+    if (dpb_ok[TC_REF_FRAMES - 1]) {
+        nf = dpb[TC_REF_FRAMES - 1];
+    } else {
+        nf = take_frame();
+        if (!nf.y) return TC_ERR_MEMORY;
+    }
     for (int i = TC_REF_FRAMES - 1; i > 0; --i) { dpb[i] = dpb[i - 1]; dpb_ok[i] = dpb_ok[i - 1]; dpb_poc[i] = dpb_poc[i - 1]; }
-    DevFrame nf = take_frame();
-    if (!nf.y) return TC_ERR_MEMORY;
     if (cudaMemcpyAsync(nf.y, cur.y, (size_t)sy * fh, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
         cudaMemcpyAsync(nf.cb, cur.cb, (size_t)sc * (fh / 2), cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
         cudaMemcpyAsync(nf.cr, cur.cr, (size_t)sc * (fh / 2), cudaMemcpyDeviceToDevice, st) != cudaSuccess)

@@ -147,19 +147,19 @@ bool EncImpl::init(const tc_config_t &c) {
     }
     const int nctu = ctu_cols * ctu_rows;
     CK(dmalloc(&d_out, sizeof(CtuOut) * nctu));
-    CK(cudaMallocHost(&h_out, sizeof(CtuOut) * nctu));
+    CK(pinned_alloc(&h_out, sizeof(CtuOut) * nctu));
     CK(dmalloc(&d_params, sizeof(FrameParams)));
     CK(dmalloc(&d_hist, 16 * sizeof(int)));
-    CK(cudaMallocHost(&h_hist, 16 * sizeof(int)));
+    CK(pinned_alloc(&h_hist, 16 * sizeof(int)));
     CK(dmalloc(&d_sse, sizeof(unsigned long long)));
-    CK(cudaMallocHost(&h_sse, sizeof(unsigned long long)));
+    CK(pinned_alloc(&h_sse, sizeof(unsigned long long)));
     CK(dmalloc(&d_err, sizeof(int)));
     CK(cudaMemset(d_err, 0, sizeof(int)));
     CK(dmalloc(&d_done, sizeof(int) * ctu_cols * ctu_rows));
     CK(cudaMemset(d_done, 0, sizeof(int) * ctu_cols * ctu_rows));
     CK(dmalloc(&d_ctrl, 2 * sizeof(int)));
-    CK(cudaMallocHost(&h_ctrl, 2 * sizeof(int)));
-    CK(cudaMallocHost(&h_params_pin, sizeof(FrameParams)));
+    CK(pinned_alloc(&h_ctrl, 2 * sizeof(int)));
+    CK(pinned_alloc(&h_params_pin, sizeof(FrameParams)));
     CK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
     {
         const char *wf = getenv("TCB_WAVEFRONT");
@@ -185,13 +185,15 @@ bool EncImpl::init(const tc_config_t &c) {
     bf_b_mode = c.enable_b_frames ? 1 : 0;
     // B-frame reorder buffers, allocated once: the reorder path then makes
     // no device allocation (and no implicit device synchronisation) per frame.
+    // Each frame joins bf_free before its planes are allocated, so a failed
+    // allocation leaves nothing that release() does not free.
     if (bf_b_mode)
         for (size_t i = 0; i < BF_MAX; ++i) {
-            DevFrame f;
+            bf_free.emplace_back();
+            DevFrame &f = bf_free.back();
             CK(dmalloc(&f.y, ybytes));
             CK(dmalloc(&f.cb, cbytes));
             CK(dmalloc(&f.cr, cbytes));
-            bf_free.push_back(f);
         }
     return true;
 }
@@ -437,7 +439,7 @@ tc_error_t EncImpl::readback_recon() {
 bool EncImpl::set_pipelined(bool on) {
     if (on && rc_method != TC_RC_CQP) return false;
     if (on && !h_out_alt) {
-        if (cudaMallocHost(&h_out_alt, sizeof(CtuOut) * (size_t)ctu_cols * ctu_rows) != cudaSuccess) {
+        if (pinned_alloc(&h_out_alt, sizeof(CtuOut) * (size_t)ctu_cols * ctu_rows) != cudaSuccess) {
             h_out_alt = nullptr;
             return false;
         }

@@ -84,7 +84,8 @@ struct EncImpl {
     // from cudaMalloc.
     DeviceArena *arena = nullptr;
     template <typename T> cudaError_t dmalloc(T **p, size_t n) {
-        if (!arena) return cudaMalloc((void **)p, n);
+        if (!arena) return dev_alloc(p, n);
+        if (alloc_fault_now()) { *p = nullptr; return cudaErrorMemoryAllocation; }
         *p = (T *)arena->alloc(n);
         return *p ? cudaSuccess : cudaErrorMemoryAllocation;
     }
