@@ -65,3 +65,45 @@ def test_served_sessions_match_alone_and_respect_budget():
     for i in range(len(specs)):
         want = api.encode_sequence(lib, cfgs[i], clips[i])
         assert got[i] == want, i
+
+
+def test_failed_admission_is_retried():
+    """A session whose admission fails (its first device allocation fails,
+    injected on the host) stays queued and is admitted at a later step; no
+    session is lost and packets stay bit-exact."""
+    from tcodec_b200 import api, synth
+    lib = api.bind_b200(api.load_library())
+    specs = [(128, 72, 30), (96, 80, 34)]
+    clips = [synth.stream_clip(dict(w=w, h=h, seed=700 + i, frames=4)) for i, (w, h, _) in enumerate(specs)]
+    cfgs = [api.make_config(lib, w, h, qp=q, preset=2, profile=1, keyframe_interval=1000) for w, h, q in specs]
+    srv = api.Server(lib, hbm_budget_bytes=1 << 30, max_active=4)
+    sids = [srv.open(c) for c in cfgs]
+    fed = [0, 0]
+    got = [[], []]
+    try:
+        for step in range(40):
+            for i, s in enumerate(sids):
+                while fed[i] < len(clips[i]) and srv.push(s, clips[i][fed[i]]):
+                    fed[i] += 1
+                    if fed[i] == len(clips[i]):
+                        srv.finish(s)
+            if step == 0:
+                assert lib.tcb_debug_fail_allocations_after(0) < 0
+            out = srv.step()
+            if step == 0:
+                assert lib.tcb_debug_fail_allocations_after(-1) < 0   # the failure fired
+                st = srv.stats()
+                assert st["waiting"] == 2 and st["active"] == 0 and st["bytes_in_use"] == 0
+            for s, status, pkt in out:
+                assert status in (api.TC_OK, api.TC_ERR_NEED_MORE), (s, status)
+                if pkt is not None:
+                    got[sids.index(s)].append(pkt)
+            if all(srv.state(s) == api.SESSION_DONE for s in sids):
+                break
+        else:
+            raise AssertionError("sessions did not drain")
+    finally:
+        lib.tcb_debug_fail_allocations_after(-1)
+        srv.close()
+    for i in range(2):
+        assert got[i] == api.encode_sequence(lib, cfgs[i], clips[i]), i
