@@ -147,3 +147,18 @@ def test_preset_entropy_matrix_matches_reference(lib, ref_lib, size):
                 for pa, pb, pd in zip(a, b, d):
                     assert np.array_equal(pa, pb), (size, kw)
                     assert np.array_equal(pd, pb), (size, kw)
+
+
+@pytest.mark.parametrize("name", ["cfg0", "cfg1"])
+def test_single_stream_configs_known_answers(lib, name):
+    """The two single-stream workloads at full length through tc_encoder_*:
+    320x240 x 30 frames (1 searched reference) and 1280x720 x 60 frames
+    (2 searched references, rectangles moving over global motion).  Every
+    packet and the final reconstruction equal the reference encoder's
+    (tests/golden/configs_v2.json, from tests/golden/make_config_golden.py)."""
+    from tests.golden import make_config_golden as cg
+    want = json.load(open(os.path.join(HERE, "golden", "configs_v2.json")))[name]
+    got = cg.run(lib, name)
+    assert got["sizes"] == want["sizes"]
+    assert got["packets"] == want["packets"]
+    assert got["final_recon"] == want["final_recon"]
