@@ -100,6 +100,22 @@ void tc_fdct4x4_res(const tc_coeff_t *in, int stride, tc_coeff_t *out);
 void tc_idct4x4_res(const tc_coeff_t *in, tc_coeff_t *out, int stride);
 void tc_fdct8x8_res(const tc_coeff_t *in, int stride, tc_coeff_t *out);
 void tc_idct8x8_res(const tc_coeff_t *in, tc_coeff_t *out, int stride);
+
+/* Every output sample of tc_idct4x4_res / tc_idct8x8_res when only the DC
+ * coefficient is non-zero (reference include/tcodec_common.h:150-163, the
+ * decoder's DC-only path): both rounded 14-bit passes with the DC basis
+ * value round(2^14 * sqrt(1/N)), 8192 for N = 4 and 5793 for N = 8. */
+static inline int tc_idct_dc4_res(int dc) {
+    const int basis = 8192, half = 1 << 13;
+    const int row = (dc * basis + half) >> 14;
+    return (row * basis + half) >> 14;
+}
+static inline int tc_idct_dc8_res(int dc) {
+    const int basis = 5793, half = 1 << 13;
+    const int row = (dc * basis + half) >> 14;
+    return (row * basis + half) >> 14;
+}
+
 void tc_fwht4x4(const tc_coeff_t *in, int stride, tc_coeff_t *out);
 void tc_iwht4x4(const tc_coeff_t *in, tc_coeff_t *out, int stride);
 void tc_fwht8x8(const tc_coeff_t *in, int stride, tc_coeff_t *out);

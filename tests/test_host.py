@@ -16,7 +16,8 @@ LIB = os.path.join(ROOT, "tcodec_b200", "libtcodec_b200.so")
 def _declared(header):
     text = open(os.path.join(ROOT, "include", header)).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(tcb?_[a-z0-9_]+)\s*\(", text)))
+    inline = set(re.findall(r"static\s+inline\s+[\w\s\*]*?\b(tcb?_[a-z0-9_]+)\s*\(", text))   # defined in the header
+    return sorted(set(re.findall(r"\b(tcb?_[a-z0-9_]+)\s*\(", text)) - inline)
 
 
 def _exported():
@@ -104,3 +105,23 @@ def test_autotune_choice_table():
     assert L.tcb_autotune_set_threads(7, w, h, 128) == api.TC_ERR_PARAM
     assert L.tcb_autotune_frame_kernels(w + 1, h, 4) == api.TC_ERR_PARAM     # odd width
     assert L.tcb_autotune_frame_kernels(w, h, 0) == api.TC_ERR_PARAM         # no frames
+
+
+def test_transform_dc_paths(tmp_path):
+    """The reference's transform checks (test/test_tcodec.c:3074-3149) on
+    the library's residual transforms and the DC-only helpers of
+    include/tcodec_b200_common.h: DC gains, the +-2 round-trip bound, and
+    exact DC-only parity for every DC in [-2000, 2000]."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not cc:
+        pytest.skip("no C compiler")
+    libdir = os.path.join(ROOT, "tcodec_b200")
+    exe = str(tmp_path / "transform_dc_check")
+    subprocess.run([cc, "-std=c99", "-O2", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "transform_dc_check.c"), "-L", libdir, "-ltcodec_b200",
+                    "-Wl,-rpath," + libdir, "-o", exe], check=True, timeout=120)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
