@@ -429,6 +429,69 @@ def run_standalone_kernels(lib, peak, iters=8, frames=64):
     return out
 
 
+# ---------------------------------------------------------------- engine phase profile
+PHASES = ["refs/mvp", "ME", "MC", "resid jobs", "skip chk", "scan", "CfL", "replay", "decide(total)",
+          "write pass", "deblock+sao", "me0:int", "me0:subpel"]
+
+
+def run_phase_profile(streams, steps, ops_out=None):
+    """Counters of the CTU engine on the batched 1080p GOP4-B workload, read
+    from the profiling build (`make -C tcodec_b200 prof`: the same kernels
+    compiled with -DTCB_PHASE_PROFILE):
+
+    * per-phase cycles of each CTU (thread 0's clock64 deltas summed over CTUs);
+    * each CTA's residency and the cycles it waited for a left or above
+      neighbour's publish flag;
+    * work counts: integer-search SAD pixel differences, quarter-sample SAD
+      pixels, and 8x8 / 4x4 transform units coded.  The encode is
+      deterministic, so these counts hold for the production build too.
+
+    The counters slow the engine: its timings are for shares, not for
+    throughput."""
+    from tcodec_b200 import api, synth
+    lib = api.load_library(os.path.join(ROOT, "tcodec_b200", "libtcodec_b200_prof.so"))
+    lib = api.bind_b200(lib)
+    lib.tcb_debug_phase_cycles.argtypes = [ctypes.c_void_p]
+    lib.tcb_debug_op_counts.argtypes = [ctypes.c_void_p]
+    S = streams
+    clip = synth.workload("rects_lines", frames=12)
+    batch = api.BatchEncoder(lib, [make_cfg(lib) for _ in range(S)])
+    cyc, ops = (ctypes.c_ulonglong * 16)(), (ctypes.c_ulonglong * 4)()
+    tot, steady = [0, 0, 0, 0], 0
+    for t in range(steps):
+        t0 = time.time()
+        pk = batch.encode([clip[(t + s) % len(clip)] for s in range(S)])
+        dt = time.time() - t0
+        lib.tcb_debug_phase_cycles(cyc)
+        lib.tcb_debug_op_counts(ops)
+        coded = sum(p is not None for p in pk)
+        enc = cyc[8] + cyc[9] + cyc[10]
+        print(f"step {t} {dt * 1000:.0f} ms, {coded} frames: residency {cyc[14] / 1e9:.2f} Gcyc, encode "
+              f"{100 * enc / max(1, cyc[14]):.1f} %, neighbour wait {100 * cyc[13] / max(1, cyc[14]):.1f} %; "
+              f"int SAD px {ops[0] / 1e9:.3f} G, qpel SAD px {ops[1] / 1e9:.3f} G, "
+              f"TU8 {ops[2] / 1e6:.2f} M, TU4 {ops[3] / 1e6:.2f} M")
+        if t == steps - 1:
+            for i, n in enumerate(PHASES):
+                print(f"   {n:14s} {cyc[i] / 1e6:10.1f} Mcyc  {100 * cyc[i] / max(1, enc):5.1f} %")
+        if t >= 4 and coded == S:          # steady GOP4-B steps (after the first anchor)
+            steady += 1
+            for i in range(4):
+                tot[i] += ops[i]
+    batch.close()
+    per_frame = {k: tot[i] / max(1, steady * S) for i, k in enumerate(("int_sad_px", "qpel_sad_px", "tu8", "tu4"))}
+    print("per frame:", json.dumps(per_frame))
+    if ops_out:
+        out = {"workload": f"1920x1080 GOP4-B, CQP 32, preset medium, profile 1, {S} streams, "
+                           f"mean over {steady} steady steps",
+               "per_frame": per_frame,
+               "int32_lanes_per_sm_clock": 64,
+               "peak_note": "integer peak taken as 64 INT32 lane operations per SM per clock (half the 128 "
+                            "FP32 lanes), an assumption; a packed SAD (vsadu4) counts 4 byte differences",
+               "command": "python bench.py --phase-profile --streams %d --steps %d --ops-out <file>" % (S, steps)}
+        with open(ops_out, "w") as f:
+            f.write(json.dumps(out, indent=1) + "\n")
+
+
 # ---------------------------------------------------------------- B200 arm
 def run_b200(args, rank, world):
     """Batched pass (device-resident and host inputs) and a plain
@@ -602,6 +665,10 @@ def main():
                          "during its own device step)")
     ap.add_argument("--graphs", action="store_true",
                     help="replay every batched / served step's device work as one CUDA graph")
+    ap.add_argument("--phase-profile", action="store_true",
+                    help="per-phase cycle split and work counts of the CTU engine from the profiling build "
+                         "(make -C tcodec_b200 prof); --ops-out writes the work counts")
+    ap.add_argument("--ops-out", default=None)
     ap.add_argument("--kernels-only", action="store_true",
                     help="only time the standalone frame kernels (deblock, SAO, motion compensation)")
     args = ap.parse_args()
@@ -639,6 +706,9 @@ def main():
         print(json.dumps(line))
         return
 
+    if args.phase_profile:
+        run_phase_profile(args.streams, max(args.steps, 6), args.ops_out)
+        return
     if args.kernels_only:
         peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]) \
             if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
@@ -722,7 +792,7 @@ def main():
             "int32_lane_peak_ops_per_s": lane_peak,
             "sad_frac_of_packed_peak": sad / (4.0 * lane_peak),   # four byte differences per lane op (vsadu4)
             "transform_mac_frac": macs / lane_peak,
-            "counts": OPS, "peak_note": o["peak_note"]}
+            "counts": os.path.relpath(OPS, ROOT), "peak_note": o["peak_note"]}
     lat = sorted(dev_run["lat"])
     p50 = lat[len(lat) // 2] * 1000 if lat else None
     p99 = lat[min(len(lat) - 1, int(0.99 * len(lat)))] * 1000 if lat else None

@@ -1,9 +1,11 @@
 """B200-native TCodec v2 pixel pipeline.
 
-`tcodec_b200.api` binds the include/tcodec.h C ABI of libtcodec_b200.so
-(hand-written sm_100a kernels behind the reference's encoder API);
-`tcodec_b200.kernels` binds the batched standalone kernels of
-include/tcodec_b200.h; `tcodec_b200.synth` makes the seeded synthetic
+`tcodec_b200.api` binds the C ABI of libtcodec_b200.so: the reference's
+include/tcodec.h encoder / decoder entry points and the additions of
+include/tcodec_b200.h (batched and served forms, the standalone CTU-engine
+frame entry points and the frame kernels), all backed by hand-written sm_100a
+kernels.  `tcodec_b200.serving` replays a served-session schedule through
+the server entry points, and `tcodec_b200.synth` makes the seeded synthetic
 benchmark sources.
 """
 from .api import LIB_PATH, load_library  # noqa: F401

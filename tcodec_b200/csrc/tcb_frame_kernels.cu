@@ -115,9 +115,7 @@ __global__ void frame_sse_kernel(const uint8_t *__restrict__ a, const uint8_t *_
 cudaError_t init_device_tables() {
     cudaError_t e = init_engine_tables();
     if (e != cudaSuccess) return e;
-    e = init_decode_tables();
-    if (e != cudaSuccess) return e;
-    return init_unit_tables();
+    return init_decode_tables();
 }
 
 cudaError_t launch_glob_mv(const uint8_t *cur, const uint8_t *ref, int W, int H, int s,

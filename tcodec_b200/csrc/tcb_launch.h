@@ -9,7 +9,6 @@ namespace tcb {
 
 cudaError_t init_device_tables();
 cudaError_t init_engine_tables();
-cudaError_t init_unit_tables();
 size_t ctu_smem_bytes();
 cudaError_t init_decode_tables();
 cudaError_t launch_decode_items(const FrameParams *d_params, const int *d_items, int n, cudaStream_t st);

@@ -9,15 +9,28 @@ tree.  `clip()` regenerates each one-frame test pattern with the same
 per-pixel rules as the reference generator (gradient, checkerboard,
 per-pixel-seeded noise from Python's `random`, line patterns; chroma 128).
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:  python tests/golden/make_golden.py [REFERENCE_TREE | MANIFEST]
+(default: the tree oracle/Makefile reads, `make -s -C oracle refdir`).
 """
 import os
 import random
+import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "golden_v2.sha256")
-REF_MANIFEST = "/root/reference/golden/MANIFEST.sha256"
+
+
+def reference_manifest() -> str:
+    if len(sys.argv) > 1:
+        if os.path.isfile(sys.argv[1]):      # a manifest file given directly
+            return sys.argv[1]
+        ref = sys.argv[1]
+    else:
+        root = os.path.dirname(os.path.dirname(HERE))
+        ref = subprocess.run(["make", "-s", "-C", os.path.join(root, "oracle"), "refdir"], check=True,
+                             capture_output=True, text=True).stdout.strip()
+    return os.path.join(ref, "golden", "MANIFEST.sha256")
 
 PATTERNS = {"gradient", "checkerboard", "noise", "hlines", "vlines", "diagonal"}
 # tcenc flags of each variant (reference tools/gen_golden.sh:111-147).
@@ -74,7 +87,7 @@ def load():
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else REF_MANIFEST
+    src = reference_manifest()
     lines = []
     with open(src) as f:
         for line in f:
