@@ -327,7 +327,7 @@ __device__ void luma_jobs8(Smem &S, const Leaf &L, const int *cl, int ncl, const
     if (threadIdx.x == 0) OPCOUNT(2, J);
     const int hw = threadIdx.x >> 5, lane = threadIdx.x & 31, oct = lane >> 3, l8 = lane & 7;
     const int warp = (hw + NW - woff % NW) % NW;   // job rank of this warp
-    int *scr = S.scratch[hw] + oct * 64;
+    int *scr = S.scratch[hw] + oct * 72;
     const int dc = S.dc;
     for (int base = 0; base < J; base += NW * 4) {
         const int j = base + warp * 4 + oct;
@@ -373,7 +373,7 @@ __device__ void luma_jobs4(Smem &S, const Leaf &L, const int *cl, int ncl, const
     if (threadIdx.x == 0) OPCOUNT(3, J);
     const int hw = threadIdx.x >> 5, lane = threadIdx.x & 31, qd = lane >> 2, l4 = lane & 3;
     const int warp = (hw + NW - woff % NW) % NW;   // job rank of this warp
-    int *scr = S.scratch[hw] + qd * 16;
+    int *scr = S.scratch[hw] + qd * 20;
     const int dc = S.dc;
     for (int base = 0; base < J; base += NW * 8) {
         const int j = base + warp * 8 + qd;
@@ -422,7 +422,7 @@ __device__ void chroma_jobs(Smem &S, const Leaf &L, int nopt, int cbase, const Q
     const int lxc = L.lx >> 1, lyc = L.ly >> 1;
     const int hw = threadIdx.x >> 5, lane = threadIdx.x & 31, qd = lane >> 2, l4 = lane & 3;
     const int warp = (hw + NW - woff % NW) % NW;   // job rank of this warp
-    int *scr = S.scratch[hw] + qd * 16;
+    int *scr = S.scratch[hw] + qd * 20;
     for (int base = 0; base < J; base += NW * 8) {
         const int j = base + warp * 8 + qd;
         const bool act = j < J;

@@ -62,7 +62,7 @@ struct Smem {
     uint8_t ra[2 * 64 + 4], rl[2 * 64 + 4];     // index i+1 holds ref[i], i in -1..2N
     uint8_t ipred[18][IPRED_MAX * IPRED_MAX];    // intra predictions of the current leaf (<= IPRED_MAX)
     uint32_t ipred_ok;                           // modes held in ipred
-    int scratch[NW][256];
+    int scratch[NW][288];     // per warp: 4 octets x 72 or 8 quads x 20 ints (padded rows)
     MeGroup me[NGROUP];
     QuantParams qparam[2];     // luma, chroma quantiser of the current CTU
     // Luma reconstruction of every scored candidate of the current leaf

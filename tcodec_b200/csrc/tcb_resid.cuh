@@ -7,8 +7,11 @@
 //           row pass and column r afterwards.
 //   4x4 TU: a "quad" of 4 consecutive lanes, same ownership.
 //
-// The row<->column exchange goes through a 64-int (octet) / 16-int (quad)
-// shared-memory scratch private to the lane group.  All 32 lanes of the
+// The row<->column exchange goes through a shared-memory scratch private to
+// the lane group: 8 rows of 9 ints per octet (72), 4 rows of 5 ints per quad
+// (20).  The padded rows put the 32 lanes of a warp (four octets at 72-int
+// or eight quads at 20-int offsets) on 32 different banks for both the row
+// writes and the column reads.  All 32 lanes of the
 // warp must call these routines together (they use full-mask shuffles of
 // width 8 / 4); inactive groups pass dummy data and discard the results.
 //
@@ -141,11 +144,11 @@ __device__ __forceinline__ int tu8_code(int l8, const int res_row[8], int *scr,
         t[k] = (acc + 8192) >> 14;
     }
 #pragma unroll
-    for (int k = 0; k < 8; ++k) scr[l8 * 8 + k] = t[k];
+    for (int k = 0; k < 8; ++k) scr[l8 * 9 + k] = t[k];
     __syncwarp();
     int col[8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) col[i] = scr[i * 8 + l8];
+    for (int i = 0; i < 8; ++i) col[i] = scr[i * 9 + l8];
     __syncwarp();
     int nz = 0, last = -1;
 #pragma unroll
@@ -170,24 +173,23 @@ __device__ __forceinline__ int tu8_code(int l8, const int res_row[8], int *scr,
     // Dequantise and hand columns back as rows for the inverse row pass.
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-        const int pos = k * 8 + l8;
-        scr[pos] = (int16_t)dequant_band(q_col[k], band_rc<8>(k, l8), qp);
+        scr[k * 9 + l8] = (int16_t)dequant_band(q_col[k], band_rc<8>(k, l8), qp);
     }
     __syncwarp();
     int row[8];
 #pragma unroll
-    for (int n = 0; n < 8; ++n) row[n] = scr[l8 * 8 + n];
+    for (int n = 0; n < 8; ++n) row[n] = scr[l8 * 9 + n];
     __syncwarp();
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         int acc = 0;
 #pragma unroll
         for (int n = 0; n < 8; ++n) acc += c_dct8[n][k] * row[n];
-        scr[l8 * 8 + k] = (acc + 8192) >> 14;
+        scr[l8 * 9 + k] = (acc + 8192) >> 14;
     }
     __syncwarp();
 #pragma unroll
-    for (int n = 0; n < 8; ++n) col[n] = scr[n * 8 + l8];
+    for (int n = 0; n < 8; ++n) col[n] = scr[n * 9 + l8];
     __syncwarp();
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
@@ -212,11 +214,11 @@ __device__ __forceinline__ int tu4_code(int l4, const int res_row[4], int *scr,
         t[k] = (acc + 8192) >> 14;
     }
 #pragma unroll
-    for (int k = 0; k < 4; ++k) scr[l4 * 4 + k] = t[k];
+    for (int k = 0; k < 4; ++k) scr[l4 * 5 + k] = t[k];
     __syncwarp();
     int col[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) col[i] = scr[i * 4 + l4];
+    for (int i = 0; i < 4; ++i) col[i] = scr[i * 5 + l4];
     __syncwarp();
     int nz = 0, last = -1;
 #pragma unroll
@@ -240,24 +242,23 @@ __device__ __forceinline__ int tu4_code(int l4, const int res_row[4], int *scr,
     const int bits = 1 + 2 * nz + lb + lastpos_cost(last);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const int pos = k * 4 + l4;
-        scr[pos] = (int16_t)dequant_band(q_col[k], band_rc<4>(k, l4), qp);
+        scr[k * 5 + l4] = (int16_t)dequant_band(q_col[k], band_rc<4>(k, l4), qp);
     }
     __syncwarp();
     int row[4];
 #pragma unroll
-    for (int n = 0; n < 4; ++n) row[n] = scr[l4 * 4 + n];
+    for (int n = 0; n < 4; ++n) row[n] = scr[l4 * 5 + n];
     __syncwarp();
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         int acc = 0;
 #pragma unroll
         for (int n = 0; n < 4; ++n) acc += c_dct4[n][k] * row[n];
-        scr[l4 * 4 + k] = (acc + 8192) >> 14;
+        scr[l4 * 5 + k] = (acc + 8192) >> 14;
     }
     __syncwarp();
 #pragma unroll
-    for (int n = 0; n < 4; ++n) col[n] = scr[n * 4 + l4];
+    for (int n = 0; n < 4; ++n) col[n] = scr[n * 5 + l4];
     __syncwarp();
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
