@@ -42,15 +42,32 @@ __constant__ int8_t c_qpel[9][2] = {{0, 0}, {1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1
 // Optional per-phase cycle counters (build with -DTCB_PHASE_PROFILE); thread
 // 0 of each CTA accumulates clock64() deltas into tcb_phase_cycles[].
 #ifdef TCB_PHASE_PROFILE
-__device__ unsigned long long tcb_phase_cycles[16];
+// Slots 0..15 as listed by the profiling reader; 16 + 8 * depth + k: leaf
+// phase k (0..7) of leaves at that quadtree depth; 48 + depth: leaf
+// decisions at that depth; 52 + 2 * depth + {0, 1}: integer stages and
+// quarter-pel refinement of group 0's searches at that depth; 60..63:
+// thread 0's time inside one 8x8 residual job (setup and residual,
+// transform chain, reconstruction and sums) and the intra prediction fill
+// of build_refs.
+constexpr int PHASE_SLOTS = 64;
+__device__ unsigned long long tcb_phase_cycles[PHASE_SLOTS];
 #define PHASE_T0() long long _ph_t = clock64()
 #define PHASE(k) do { if (threadIdx.x == 0) { const long long _n = clock64(); \
     atomicAdd(&tcb_phase_cycles[k], (unsigned long long)(_n - _ph_t)); _ph_t = _n; } } while (0)
+#define PHASE_D(k, d) do { if (threadIdx.x == 0) { const long long _n = clock64(); \
+    atomicAdd(&tcb_phase_cycles[k], (unsigned long long)(_n - _ph_t)); \
+    atomicAdd(&tcb_phase_cycles[16 + 8 * (d) + (k)], (unsigned long long)(_n - _ph_t)); _ph_t = _n; } } while (0)
+#define COUNT_D(d) do { if (threadIdx.x == 0) atomicAdd(&tcb_phase_cycles[48 + (d)], 1ull); } while (0)
+#define PROBE_T0() long long _pb_t = clock64()
+#define PROBE(k) do { if (threadIdx.x == 0) { const long long _n = clock64(); \
+    atomicAdd(&tcb_phase_cycles[k], (unsigned long long)(_n - _pb_t)); _pb_t = _n; } } while (0)
 // Inside a motion search, thread 0 of group 0 splits its time into the
 // integer stages (slot 11) and the quarter-pel refinement (slot 12).
 #define ME_T0() long long _me_t = clock64()
 #define ME_MARK(k) do { if (g == 0 && gt == 0) { const long long _n = clock64(); \
-    atomicAdd(&tcb_phase_cycles[k], (unsigned long long)(_n - _me_t)); _me_t = _n; } } while (0)
+    const int _d = blk == 64 ? 0 : blk == 32 ? 1 : blk == 16 ? 2 : 3; \
+    atomicAdd(&tcb_phase_cycles[k], (unsigned long long)(_n - _me_t)); \
+    atomicAdd(&tcb_phase_cycles[52 + 2 * _d + (k) - 11], (unsigned long long)(_n - _me_t)); _me_t = _n; } } while (0)
 // Work counts (thread 0 of the calling group, one atomic per call):
 // [0] integer-search SAD pixel differences, [1] quarter-pel SAD pixels,
 // [2] 8x8 and [3] 4x4 transform units coded (luma and chroma).
@@ -59,6 +76,10 @@ __device__ unsigned long long tcb_op_counts[4];
 #else
 #define PHASE_T0() do {} while (0)
 #define PHASE(k) do {} while (0)
+#define PHASE_D(k, d) do {} while (0)
+#define COUNT_D(d) do {} while (0)
+#define PROBE_T0() do {} while (0)
+#define PROBE(k) do {} while (0)
 #define ME_T0() do {} while (0)
 #define ME_MARK(k) do {} while (0)
 #define OPCOUNT(k, v) do {} while (0)
@@ -85,6 +106,19 @@ __device__ __forceinline__ uint8_t &RY(Smem &S, int x, int y) {
 __device__ __forceinline__ uint8_t &RC(Smem &S, int c, int x, int y) {
     return S.rec_c[c][(y + RC_OY) * RC_W + x + RC_OX];
 }
+
+// The CTU state lives in the kernels' one dynamic shared buffer, and the
+// frame parameters of the CTU being encoded or decoded in g_fp (every
+// kernel that calls the helpers below fills g_fp first).  Functions compiled
+// once (__noinline__, so the kernel keeps a single copy of each: the whole
+// engine is far larger than the SM's instruction cache) take them from here
+// rather than through their reference parameters, so their accesses stay
+// shared-memory accesses instead of generic ones.
+__device__ __forceinline__ Smem &smem_state() {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    return *reinterpret_cast<Smem *>(smem_raw);
+}
+__shared__ FrameParams g_fp;
 
 struct Leaf {
     int depth, cx, cy, cu, lx, ly, px, py;
@@ -118,57 +152,116 @@ __device__ void mvp_at(const MvCell *grid, int cx, int cy, int &mx, int &my) {
 // Motion search on one warp group (reference src/motion.c:384-485).
 // ====================================================================
 
-// SADs of up to 7 integer candidates base + pat[p0 + k] * scale, k < K.
-// Out-of-frame candidates cost 0x7FFFFFFF (reference sad_at).
-__device__ void group_int_sads(Smem &S, int g, int gt, const uint8_t *ref, int s, int W, int H,
-                               const uint8_t *cur, int blk, int pat, int p0, int K,
-                               int bx, int by, int scale) {
-    const int wpr = blk >> 2, words = blk * wpr, total = K * words;
+__device__ __forceinline__ void pat_point(int pat, int p, int &dx, int &dy) {
+    if (pat == 0) { dx = c_hex_large[p][0]; dy = c_hex_large[p][1]; }
+    else if (pat == 1) { dx = c_hex_small[p][0]; dy = c_hex_small[p][1]; }
+    else if (pat == 2) { dx = c_diamond[p][0]; dy = c_diamond[p][1]; }
+    else { dx = 0; dy = 0; }
+}
+
+__device__ __forceinline__ int lg2i(int v) { return 31 - __clz(v); }
+
+// SADs of the K <= 7 integer candidates base + pat[p0 + k] * scale, k < K,
+// on the 128 threads of group g; every thread ends with all K values in
+// sad[] (out-of-frame candidates: 0x7FFFFFFF, reference sad_at).  Each warp
+// reduces its lanes' partial sums into S.me[g].part[par]; after the one
+// group barrier every thread adds the partials up itself, and `par` flips so
+// the next call writes the other buffer (a thread can only get to that
+// call's barrier after all threads have read this one's).
+//
+// Work split (4-byte words of the block, blk = 8 << n):
+//   blk >= 32  every thread covers words gt, gt + 128, ... of all K candidates;
+//   blk == 16  64 words: warps 0-1 take candidates 0, 2, 4, 6 and warps 2-3
+//              candidates 1, 3, 5, one word of each per thread;
+//   blk == 8   16 words: each half warp takes one candidate (k = gt >> 4).
+__device__ __forceinline__ void group_int_sads(Smem &S, int g, int gt, int &par, const uint8_t *ref, int s, int W, int H,
+                               const uint8_t *cur, int blk, int pat, int p0, int K, int bx, int by, int scale,
+                               int sad[7]) {
+    const int lgb = lg2i(blk), lgwpr = lgb - 2, lgw = 2 * lgb - 2;   // words per row, words
+    const int wig = gt >> 5, lane = gt & 31;
     if (gt == 0) OPCOUNT(0, K * blk * blk);
-    int acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (int i = gt; i < total; i += GT) {
-        const int k = i / words, w = i - k * words, r = w / wpr, c4 = (w - r * wpr) * 4;
-        int dx, dy;
-        if (pat == 0) { dx = c_hex_large[p0 + k][0]; dy = c_hex_large[p0 + k][1]; }
-        else if (pat == 1) { dx = c_hex_small[p0 + k][0]; dy = c_hex_small[p0 + k][1]; }
-        else if (pat == 2) { dx = c_diamond[p0 + k][0]; dy = c_diamond[p0 + k][1]; }
-        else { dx = 0; dy = 0; }
-        const int x = bx + dx * scale, y = by + dy * scale;
+    int *part = S.me[g].part[par];
+    if (blk >= 32) {
+        int cx[7], cy[7];
+        bool in[7];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+            int dx = 0, dy = 0;
+            if (k < K) pat_point(pat, p0 + k, dx, dy);
+            cx[k] = bx + dx * scale; cy[k] = by + dy * scale;
+            in[k] = k < K && cx[k] >= 0 && cy[k] >= 0 && cx[k] + blk <= W && cy[k] + blk <= H;
+        }
+        int acc[7] = {0, 0, 0, 0, 0, 0, 0};
+        for (int w = gt; w < (1 << lgw); w += GT) {
+            const int r = w >> lgwpr, c4 = (w & ((1 << lgwpr) - 1)) << 2;
+            const uint32_t cv = *(const uint32_t *)(cur + r * 64 + c4);
+#pragma unroll
+            for (int k = 0; k < 7; ++k)
+                if (in[k]) acc[k] += (int)__vsadu4(ld4u(ref + (size_t)(cy[k] + r) * s + cx[k] + c4), cv);
+        }
+#pragma unroll
+        for (int k = 0; k < 7; ++k)
+            if (k < K) {
+                const int v = (int)__reduce_add_sync(0xffffffffu, (unsigned)acc[k]);
+                if (lane == 0) part[wig * 8 + k] = v;
+            }
+    } else if (blk == 16) {
+        const int kb = gt >> 6, w = gt & 63, r = w >> 2, c4 = (w & 3) << 2;
+        const uint32_t cv = *(const uint32_t *)(cur + r * 64 + c4);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const int k = kb + 2 * m;
+            int v = 0;
+            if (k < K) {
+                int dx, dy;
+                pat_point(pat, p0 + k, dx, dy);
+                const int x = bx + dx * scale, y = by + dy * scale;
+                if (x >= 0 && y >= 0 && x + 16 <= W && y + 16 <= H)
+                    v = (int)__vsadu4(ld4u(ref + (size_t)(y + r) * s + x + c4), cv);
+            }
+            if (2 * m < K) {     // warp-uniform
+                v = (int)__reduce_add_sync(0xffffffffu, (unsigned)v);
+                if (lane == 0) part[wig * 8 + m] = v;
+            }
+        }
+    } else {   // blk == 8
+        const int k = gt >> 4, w = gt & 15, r = w >> 1, c4 = (w & 1) << 2;
         int v = 0;
-        if (x >= 0 && y >= 0 && x + blk <= W && y + blk <= H)
-            v = (int)__vsadu4(ld4u(ref + (size_t)(y + r) * s + x + c4),
-                              *(const uint32_t *)(cur + r * 64 + c4));
-#pragma unroll
-        for (int kk = 0; kk < 7; ++kk) acc[kk] += (kk == k) ? v : 0;
+        if (k < K) {
+            int dx, dy;
+            pat_point(pat, p0 + k, dx, dy);
+            const int x = bx + dx * scale, y = by + dy * scale;
+            if (x >= 0 && y >= 0 && x + 8 <= W && y + 8 <= H)
+                v = (int)__vsadu4(ld4u(ref + (size_t)(y + r) * s + x + c4),
+                                  *(const uint32_t *)(cur + r * 64 + c4));
+        }
+        v += __shfl_xor_sync(0xffffffffu, v, 8);
+        v += __shfl_xor_sync(0xffffffffu, v, 4);
+        v += __shfl_xor_sync(0xffffffffu, v, 2);
+        v += __shfl_xor_sync(0xffffffffu, v, 1);
+        if ((lane & 15) == 0) part[k] = v;
     }
-    const int wig = (gt >> 5), lane = gt & 31;
+    group_bar(g);
 #pragma unroll
-    for (int kk = 0; kk < 7; ++kk) {
-        if (kk < K) {
-            const int v = __reduce_add_sync(0xffffffffu, acc[kk]);
-            if (lane == 0) S.me[g].part[wig][kk] = v;
+    for (int k = 0; k < 7; ++k) {
+        if (k < K) {
+            int sum;
+            if (blk >= 32) sum = part[k] + part[8 + k] + part[16 + k] + part[24 + k];
+            else if (blk == 16) sum = part[((k & 1) * 2) * 8 + (k >> 1)] + part[((k & 1) * 2 + 1) * 8 + (k >> 1)];
+            else sum = part[k];
+            int dx, dy;
+            pat_point(pat, p0 + k, dx, dy);
+            const int x = bx + dx * scale, y = by + dy * scale;
+            sad[k] = (x >= 0 && y >= 0 && x + blk <= W && y + blk <= H) ? sum : 0x7FFFFFFF;
         }
     }
-    group_bar(g);
-    if (gt < K) {
-        int dx, dy;
-        if (pat == 0) { dx = c_hex_large[p0 + gt][0]; dy = c_hex_large[p0 + gt][1]; }
-        else if (pat == 1) { dx = c_hex_small[p0 + gt][0]; dy = c_hex_small[p0 + gt][1]; }
-        else if (pat == 2) { dx = c_diamond[p0 + gt][0]; dy = c_diamond[p0 + gt][1]; }
-        else { dx = 0; dy = 0; }
-        const int x = bx + dx * scale, y = by + dy * scale;
-        int sum = 0;
-#pragma unroll
-        for (int w = 0; w < GT / 32; ++w) sum += S.me[g].part[w][gt];
-        S.me[g].sad[gt] = (x >= 0 && y >= 0 && x + blk <= W && y + blk <= H) ? sum : 0x7FFFFFFF;
-    }
-    group_bar(g);
+    par ^= 1;
 }
 
 // One integer stage: `iters` passes over pattern points 1..npts, each point
 // taken relative to the running best (sequential commit, first improvement
 // wins; reference src/motion.c:398-448).
-__device__ void int_stage(Smem &S, int g, int gt, const uint8_t *ref, int s, int W, int H,
+__device__ void int_stage(Smem &S, int g, int gt, int &par, const uint8_t *ref, int s, int W, int H,
                           const uint8_t *cur, int blk, int pat, int npts, int iters, int scale,
                           int &bx, int &by, int &bsad) {
     for (int it = 0; it < iters; ++it) {
@@ -176,37 +269,47 @@ __device__ void int_stage(Smem &S, int g, int gt, const uint8_t *ref, int s, int
         int p0 = 1;
         while (p0 <= npts) {
             const int K = npts - p0 + 1;
-            group_int_sads(S, g, gt, ref, s, W, H, cur, blk, pat, p0, K, bx, by, scale);
-            int found = -1;
-            for (int k = 0; k < K; ++k)
-                if (S.me[g].sad[k] < bsad) { found = k; break; }
-            const int fs = found >= 0 ? S.me[g].sad[found] : 0;
-            group_bar(g);
+            int sad[7];
+            group_int_sads(S, g, gt, par, ref, s, W, H, cur, blk, pat, p0, K, bx, by, scale, sad);
+            int found = -1, fs = 0;
+#pragma unroll
+            for (int k = 0; k < 7; ++k)
+                if (found < 0 && k < K && sad[k] < bsad) { found = k; fs = sad[k]; }
             if (found < 0) break;
             int dx, dy;
-            const int p = p0 + found;
-            if (pat == 0) { dx = c_hex_large[p][0]; dy = c_hex_large[p][1]; }
-            else if (pat == 1) { dx = c_hex_small[p][0]; dy = c_hex_small[p][1]; }
-            else { dx = c_diamond[p][0]; dy = c_diamond[p][1]; }
+            pat_point(pat, p0 + found, dx, dy);
             bx += dx * scale; by += dy * scale; bsad = fs;
             improved = true;
-            p0 = p + 1;
+            p0 = p0 + found + 1;
         }
         if (!improved) break;
     }
 }
 
-// Sub-pel SAD of one candidate: six-tap diagonal interpolation where the
-// margins allow, else the bilinear sub-pel SAD (reference
-// src/motion.c:308-341 and 450-481).
-__device__ int group_subpel_sad(Smem &S, int g, int gt, const uint8_t *ref, int s,
+// Sum over group g of one int per thread (one barrier, double-buffered as in
+// group_int_sads).
+__device__ __forceinline__ int group_sum(Smem &S, int g, int gt, int &par, int v) {
+    v = (int)__reduce_add_sync(0xffffffffu, (unsigned)v);
+    int *part = S.me[g].part[par];
+    if ((gt & 31) == 0) part[(gt >> 5) * 8] = v;
+    group_bar(g);
+    const int sum = part[0] + part[8] + part[16] + part[24];
+    par ^= 1;
+    return sum;
+}
+
+// Sub-pel SAD of one candidate straight from the reference frame: six-tap
+// diagonal interpolation where the margins allow, else the bilinear sub-pel
+// SAD (reference src/motion.c:308-341 and 450-481).
+__device__ int group_subpel_sad(Smem &S, int g, int gt, int &par, const uint8_t *ref, int s,
                                 const uint8_t *cur, int blk, int qx, int qy, bool six) {
     const int fx = qx >> 2, fy = qy >> 2, dx = qx & 3, dy = qy & 3;
+    const int lgb = lg2i(blk);
     int acc = 0;
     const int total = blk * blk;
     if (gt == 0) OPCOUNT(1, total);
     for (int i = gt; i < total; i += GT) {
-        const int yy = i / blk, xx = i - yy * blk;
+        const int yy = i >> lgb, xx = i & (blk - 1);
         int p;
         if (six) {
             p = luma_hv(ref, s, fx + xx, fy + yy, dx, dy);
@@ -218,39 +321,146 @@ __device__ int group_subpel_sad(Smem &S, int g, int gt, const uint8_t *ref, int 
         }
         acc += absi((int)cur[yy * 64 + xx] - p);
     }
-    acc = __reduce_add_sync(0xffffffffu, acc);
-    if ((gt & 31) == 0) S.me[g].part[gt >> 5][0] = acc;
-    group_bar(g);
-    int sum = 0;
-#pragma unroll
-    for (int w = 0; w < GT / 32; ++w) sum += S.me[g].part[w][0];
-    group_bar(g);
-    return sum;
+    return group_sum(S, g, gt, par, acc);
 }
 
-__device__ void me_run(Smem &S, int g, int gt, const uint8_t *ref, int s, int W, int H,
+// Quarter-sample anchors of a search of a block up to 16x16 whose eight
+// refinement points all take the six-tap path.  Each point lies within 3
+// quarter samples of the integer best (bx, by) (the eight offsets of c_qpel
+// move the running best by at most one quarter sample each way per point),
+// so its integer part is bx-1..bx, by-1..by, and every sample luma_hv reads
+// for it is one of, relative to (bx-1, by-1):
+//   I   integer samples                  (B+2) x (B+2) bytes
+//   Hh  horizontal half samples f6h      rows by-3 .. by+B+2, columns bx-1 .. bx+B-1
+//   V   vertical half samples f6v        (B+1) rows x (B+2) columns
+//   D   centre half samples f6hv         (B+1) x (B+1)
+// (unclipped six-tap values, reference src/motion.c:70-107), computed once
+// per search by the group into the search's own 4 KB prediction slot, which
+// nothing reads while the searches run.
+template <int B>
+struct QpelAnchors {
+    static constexpr int GI = B + 2, GH = B + 1, GV = B + 2, GD = B + 1;
+    static constexpr int OFF_H = 336, OFF_V = OFF_H + 2 * (B + 6) * GH, OFF_D = OFF_V + 2 * (B + 1) * GV;
+    static constexpr int BYTES = OFF_D + 2 * GD * GD;
+    static_assert(GI * GI <= OFF_H && BYTES <= 64 * 64, "anchor grids overflow the 4 KB slot");
+    uint8_t *I;
+    int16_t *Hh, *V, *D;
+    __device__ explicit QpelAnchors(uint8_t *area)
+        : I(area), Hh((int16_t *)(area + OFF_H)), V((int16_t *)(area + OFF_V)), D((int16_t *)(area + OFF_D)) {}
+
+    __device__ void build(Smem &S, int g, int gt, const uint8_t *ref, int s, int bx, int by) const {
+        const int ox = bx - 1, oy = by - 1;
+        for (int i = gt; i < GI * GI; i += GT) {
+            const int r = i / GI, c = i - r * GI;
+            I[i] = ref[(size_t)(oy + r) * s + ox + c];
+        }
+        for (int i = gt; i < (B + 6) * GH; i += GT) {
+            const int r = i / GH, c = i - r * GH;
+            Hh[i] = (int16_t)f6h(ref + (size_t)(oy - 2 + r) * s, ox + c);
+        }
+        for (int i = gt; i < (B + 1) * GV; i += GT) {
+            const int r = i / GV, c = i - r * GV;
+            V[i] = (int16_t)f6v(ref, s, ox + c, oy + r);
+        }
+        group_bar(g);
+        for (int i = gt; i < GD * GD; i += GT) {
+            const int r = i / GD, c = i - r * GD;
+            const int16_t *h = Hh + r * GH + c;   // half samples of rows oy+r-2 .. oy+r+3
+            D[i] = (int16_t)((h[0] - 5 * h[GH] + 20 * h[2 * GH] + 20 * h[3 * GH] - 5 * h[4 * GH] + h[5 * GH] +
+                              16) >> 5);
+        }
+        group_bar(g);
+    }
+
+    // luma_hv's combination for sample (X, Y) of the grid at phase (dx, dy).
+    __device__ __forceinline__ int sample(int X, int Y, int dx, int dy) const {
+        const uint8_t *ip = I + Y * GI + X;
+        const int a00 = ip[0], a10 = ip[1], a01 = ip[GI], a11 = ip[GI + 1];
+        int b = 0, e = 0, c = 0, f = 0, d = 0;
+        if (dx != 0) { b = Hh[(Y + 2) * GH + X]; e = Hh[(Y + 3) * GH + X]; }
+        if (dy != 0) {
+            c = V[Y * GV + X];
+            if (dx != 0) { f = V[Y * GV + X + 1]; d = D[Y * GD + X]; }
+        }
+        int top, mid, bot;
+        switch (dx) {
+            case 0:  top = a00;               mid = c;               bot = a01; break;
+            case 1:  top = (a00 + b + 1) >> 1; mid = (c + d + 1) >> 1; bot = (a01 + e + 1) >> 1; break;
+            case 2:  top = b;                 mid = d;               bot = e; break;
+            default: top = (b + a10 + 1) >> 1; mid = (d + f + 1) >> 1; bot = (e + a11 + 1) >> 1; break;
+        }
+        int r;
+        switch (dy) {
+            case 0:  r = top; break;
+            case 1:  r = (top + mid + 1) >> 1; break;
+            case 2:  r = mid; break;
+            default: r = (mid + bot + 1) >> 1; break;
+        }
+        return clampi(r, 0, 255);
+    }
+};
+
+// Quarter-pel refinement of a B x B block (B <= 16) from anchors: the eight
+// points of reference src/motion.c:450-481 with their first-improvement
+// commits, one group barrier per point.
+template <int B>
+__device__ void qpel_refine_anchored(Smem &S, int g, int gt, int &par, const uint8_t *ref, int s,
+                                     const uint8_t *cur, int bx, int by, int &mx, int &my, int &bsad) {
+    const QpelAnchors<B> A(S.pred[g]);
+    A.build(S, g, gt, ref, s, bx, by);
+    for (int p = 1; p < 9; ++p) {
+        const int qx = mx + c_qpel[p][0], qy = my + c_qpel[p][1];
+        const int X0 = (qx >> 2) - (bx - 1), Y0 = (qy >> 2) - (by - 1), dx = qx & 3, dy = qy & 3;
+        if (gt == 0) OPCOUNT(1, B * B);
+        int acc = 0;
+#pragma unroll
+        for (int j = 0; j < (B * B + GT - 1) / GT; ++j) {
+            const int i = gt + j * GT;
+            if (i < B * B) {
+                const int x = i % B, y = i / B;
+                acc += absi((int)cur[y * 64 + x] - A.sample(X0 + x, Y0 + y, dx, dy));
+            }
+        }
+        const int sum = group_sum(S, g, gt, par, acc);
+        if (sum < bsad) { bsad = sum; mx = qx; my = qy; }
+    }
+}
+
+__device__ __noinline__ void me_run(Smem &, int g, int gt, const uint8_t *ref, int s, int W, int H,
                        int lx, int ly, int blk, int center_x, int center_y, int sr) {
+    Smem &S = smem_state();
     ME_T0();
     const uint8_t *cur = S.cur_y + ly * 64 + lx;
+    int par = 0;
     int bx = clampi(center_x, 0, W - blk), by = clampi(center_y, 0, H - blk);
-    group_int_sads(S, g, gt, ref, s, W, H, cur, blk, 3, 0, 1, bx, by, 1);
-    int bsad = S.me[g].sad[0];
-    group_bar(g);
+    int sad[7];
+    group_int_sads(S, g, gt, par, ref, s, W, H, cur, blk, 3, 0, 1, bx, by, 1, sad);
+    int bsad = sad[0];
     const int scale = maxi(1, sr / 4);
-    int_stage(S, g, gt, ref, s, W, H, cur, blk, 0, 6, 2, scale, bx, by, bsad);
-    int_stage(S, g, gt, ref, s, W, H, cur, blk, 1, 6, 3, 1, bx, by, bsad);
-    int_stage(S, g, gt, ref, s, W, H, cur, blk, 2, 4, 4, 1, bx, by, bsad);
+    // large hexagon (6 points, 2 passes, scaled), small hexagon (6, 3),
+    // diamond (4, 4); a loop rather than three inlined copies of the stage
+#pragma unroll 1
+    for (int st = 0; st < 3; ++st)
+        int_stage(S, g, gt, par, ref, s, W, H, cur, blk, st, st == 2 ? 4 : 6, st + 2, st == 0 ? scale : 1, bx, by,
+                  bsad);
     ME_MARK(11);
     // Quarter-pel refinement around the running best, first improvement
     // commits (reference src/motion.c:450-481).
     int mx = bx * 4, my = by * 4;
-    for (int p = 1; p < 9; ++p) {
-        const int qx = mx + c_qpel[p][0], qy = my + c_qpel[p][1];
-        const int fx = qx >> 2, fy = qy >> 2;
-        if (fx < 0 || fy < 0 || fx + blk + 1 > W || fy + blk + 1 > H) continue;
-        const bool six = fx >= 2 && fy >= 2 && fx + blk + 2 < W && fy + blk + 2 < H;
-        const int sad = group_subpel_sad(S, g, gt, ref, s, cur, blk, qx, qy, six);
-        if (sad < bsad) { bsad = sad; mx = qx; my = qy; }
+    const bool inner = bx - 1 >= 2 && by - 1 >= 2 && bx + blk + 2 < W && by + blk + 2 < H;
+    if (inner && blk == 16) {
+        qpel_refine_anchored<16>(S, g, gt, par, ref, s, cur, bx, by, mx, my, bsad);
+    } else if (inner && blk == 8) {
+        qpel_refine_anchored<8>(S, g, gt, par, ref, s, cur, bx, by, mx, my, bsad);
+    } else {
+        for (int p = 1; p < 9; ++p) {
+            const int qx = mx + c_qpel[p][0], qy = my + c_qpel[p][1];
+            const int fx = qx >> 2, fy = qy >> 2;
+            if (fx < 0 || fy < 0 || fx + blk + 1 > W || fy + blk + 1 > H) continue;
+            const bool six = fx >= 2 && fy >= 2 && fx + blk + 2 < W && fy + blk + 2 < H;
+            const int sum = group_subpel_sad(S, g, gt, par, ref, s, cur, blk, qx, qy, six);
+            if (sum < bsad) { bsad = sum; mx = qx; my = qy; }
+        }
     }
     ME_MARK(12);
     if (gt == 0) { S.me[g].mvx = mx; S.me[g].mvy = my; S.me[g].best = bsad; }
@@ -265,7 +475,8 @@ __device__ void me_run(Smem &S, int g, int gt, const uint8_t *ref, int s, int W,
 // For leaves up to IPRED_MAX the predictions of the intra modes in `mode_mask`
 // (DC excepted: it is the constant S.dc) are also evaluated once into
 // S.ipred, so residual jobs read them instead of re-deriving every sample.
-__device__ void build_refs(Smem &S, const Leaf &L, uint32_t mode_mask) {
+__device__ __noinline__ void build_refs(Smem &, const Leaf L, uint32_t mode_mask) {
+    Smem &S = smem_state();
     const int N = L.cu;
     const bool ha = L.py > 0, hl = L.px > 0;
     for (int i = threadIdx.x; i <= 2 * N; i += NT) {
@@ -288,6 +499,7 @@ __device__ void build_refs(Smem &S, const Leaf &L, uint32_t mode_mask) {
         S.rl[0] = (uint8_t)tl;
     }
     SYNC();
+    PROBE_T0();
     const uint32_t fill = N <= IPRED_MAX ? (mode_mask & ~2u & ((1u << 18) - 1)) : 0u;
     if (threadIdx.x < 32) {
         // DC value (reference src/predict.c:140-161): samples 1..N of each run.
@@ -310,6 +522,7 @@ __device__ void build_refs(Smem &S, const Leaf &L, uint32_t mode_mask) {
         }
     }
     SYNC();
+    PROBE(63);
 }
 
 __device__ __forceinline__ int lpred(const Smem &S, int cu, int slot, int dc, int x, int y) {
@@ -321,8 +534,10 @@ __device__ __forceinline__ int lpred(const Smem &S, int cu, int slot, int dc, in
 }
 
 // Luma residual jobs, 8x8 TUs: one octet per (candidate, TU).
-__device__ void luma_jobs8(Smem &S, const Leaf &L, const int *cl, int ncl, const QuantParams &qp,
+__device__ __noinline__ void luma_jobs8(Smem &, const Leaf L, const int *cl, int ncl, const QuantParams &,
                            bool accum, bool wrec, int16_t *emit, int woff = 0) {
+    Smem &S = smem_state();
+    const QuantParams &qp = S.qparam[0];
     const int cu = L.cu, ntu = cu >> 3, ntu2 = ntu * ntu, J = ncl * ntu2;
     if (threadIdx.x == 0) OPCOUNT(2, J);
     const int hw = threadIdx.x >> 5, lane = threadIdx.x & 31, oct = lane >> 3, l8 = lane & 7;
@@ -330,6 +545,7 @@ __device__ void luma_jobs8(Smem &S, const Leaf &L, const int *cl, int ncl, const
     int *scr = S.scratch[hw] + oct * 72;
     const int dc = S.dc;
     for (int base = 0; base < J; base += NW * 4) {
+        PROBE_T0();
         const int j = base + warp * 4 + oct;
         const bool act = j < J;
         const int jj = act ? j : 0;
@@ -343,7 +559,9 @@ __device__ void luma_jobs8(Smem &S, const Leaf &L, const int *cl, int ncl, const
             res[n] = clampi((int)S.cur_y[(L.ly + r) * 64 + L.lx + x] - lpred(S, cu, slot, dc, x, r), -512, 511);
         }
         int qc[8], rc[8];
+        PROBE(60);
         const int bits = tu8_code(l8, res, scr, qp, qc, rc);
+        PROBE(61);
         int sse = 0;
         const int x = tx * 8 + l8;
 #pragma unroll
@@ -361,14 +579,17 @@ __device__ void luma_jobs8(Smem &S, const Leaf &L, const int *cl, int ncl, const
             atomicAdd(&S.acc_sse[slot][0], sse);
             atomicAdd(&S.acc_bits[slot][0], bits);
         }
+        PROBE(62);
     }
 }
 
 // Luma residual jobs, 4x4 TUs inside each 8x8 TU: one quad per
 // (candidate, TU, sub-block); the sub-block-0 quad adds the outer flag bit
 // (reference src/encoder.c:508-535).
-__device__ void luma_jobs4(Smem &S, const Leaf &L, const int *cl, int ncl, const QuantParams &qp,
+__device__ __noinline__ void luma_jobs4(Smem &, const Leaf L, const int *cl, int ncl, const QuantParams &,
                            bool accum, bool wrec, int16_t *emit, int woff = 0) {
+    Smem &S = smem_state();
+    const QuantParams &qp = S.qparam[0];
     const int cu = L.cu, ntu = cu >> 3, ntu2 = ntu * ntu, per = ntu2 * 4, J = ncl * per;
     if (threadIdx.x == 0) OPCOUNT(3, J);
     const int hw = threadIdx.x >> 5, lane = threadIdx.x & 31, qd = lane >> 2, l4 = lane & 3;
@@ -415,8 +636,10 @@ __device__ void luma_jobs4(Smem &S, const Leaf &L, const int *cl, int ncl, const
 // Chroma residual jobs (reference src/encoder.c:429-475 qt_code_chroma):
 // 4x4 TUs, one quad per (option, component, TU).  Option o, component c
 // predicts from S.cpred[cbase + 2*o + c]; results accumulate in slot o.
-__device__ void chroma_jobs(Smem &S, const Leaf &L, int nopt, int cbase, const QuantParams &qp,
+__device__ __noinline__ void chroma_jobs(Smem &, const Leaf L, int nopt, int cbase, const QuantParams &,
                             bool accum, bool wrec, int16_t *emit, int woff = 0) {
+    Smem &S = smem_state();
+    const QuantParams &qp = S.qparam[1];
     const int cs = L.cu >> 1, nt = cs >> 2, nt2 = nt * nt, per = 2 * nt2, J = nopt * per;
     if (threadIdx.x == 0) OPCOUNT(3, J);
     const int lxc = L.lx >> 1, lyc = L.ly >> 1;
@@ -459,7 +682,8 @@ __device__ void chroma_jobs(Smem &S, const Leaf &L, int nopt, int cbase, const Q
 }
 
 // Chroma DC predictor (reference src/predict.c:364-379) into cpred[dst+c].
-__device__ void chroma_dc_pred(Smem &S, const Leaf &L, int dst) {
+__device__ __noinline__ void chroma_dc_pred(Smem &, const Leaf L, int dst) {
+    Smem &S = smem_state();
     const int cs = L.cu >> 1, lxc = L.lx >> 1, lyc = L.ly >> 1;
     const bool ha = L.py > 0, hl = L.px > 0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -475,16 +699,18 @@ __device__ void chroma_dc_pred(Smem &S, const Leaf &L, int dst) {
         if (lane == 0) S.sao[c] = n ? (sum + n / 2) / n : 128;
     }
     SYNC();
+    const int lg2 = 2 * lg2i(cs);
     for (int i = threadIdx.x; i < 2 * cs * cs; i += NT) {
-        const int c = i / (cs * cs);
-        S.cpred[dst + c][i - c * cs * cs] = (uint8_t)S.sao[c];
+        const int c = i >> lg2;
+        S.cpred[dst + c][i & ((1 << lg2) - 1)] = (uint8_t)S.sao[c];
     }
     SYNC();
 }
 
 // Chroma-from-luma blend over the DC prediction in cpred[dst+c]
 // (reference src/predict.c:390-462), reading fresh reconstructed luma.
-__device__ void cfl_blend(Smem &S, const Leaf &L, int dst) {
+__device__ __noinline__ void cfl_blend(Smem &, const Leaf L, int dst) {
+    Smem &S = smem_state();
     const int cs = L.cu >> 1, lxc = L.lx >> 1, lyc = L.ly >> 1;
     const bool up = L.py > 0, left = L.px > 0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -531,9 +757,9 @@ __device__ void cfl_blend(Smem &S, const Leaf &L, int dst) {
     }
     SYNC();
     // Per 4x4 chroma tile: mean of the 2x2-averaged collocated luma.
-    const int nt = cs >> 2;
+    const int nt = cs >> 2, lgs = lg2i(cs);
     for (int i = threadIdx.x; i < 2 * cs * cs; i += NT) {
-        const int c = i / (cs * cs), p = i - c * cs * cs, y = p / cs, x = p - y * cs;
+        const int c = i >> (2 * lgs), p = i & ((1 << (2 * lgs)) - 1), y = p >> lgs, x = p & (cs - 1);
         const int ty = (y >> 2) << 2, tx = (x >> 2) << 2;
         int sum = 0;
 #pragma unroll
@@ -555,11 +781,13 @@ __device__ void cfl_blend(Smem &S, const Leaf &L, int dst) {
 
 // Chroma MC of both components into cpred[dst+c] (or straight into the
 // recon tile when to_rec).
-__device__ void chroma_mc(Smem &S, const FrameParams &P, const Leaf &L, int refi, int mvx, int mvy,
+__device__ __noinline__ void chroma_mc(Smem &, const FrameParams &, const Leaf L, int refi, int mvx, int mvy,
                           int dst, bool to_rec) {
-    const int cs = L.cu >> 1, Wc = P.W >> 1, Hc = P.H >> 1;
+    Smem &S = smem_state();
+    const FrameParams &P = g_fp;
+    const int cs = L.cu >> 1, Wc = P.W >> 1, Hc = P.H >> 1, lgs = lg2i(cs);
     for (int i = threadIdx.x; i < 2 * cs * cs; i += NT) {
-        const int c = i / (cs * cs), p = i - c * cs * cs, y = p / cs, x = p - y * cs;
+        const int c = i >> (2 * lgs), p = i & ((1 << (2 * lgs)) - 1), y = p >> lgs, x = p & (cs - 1);
         const uint8_t *ref = c ? P.ref_cr[refi] : P.ref_cb[refi];
         const int v = chroma_mc_at(ref, P.stride_c, Wc, Hc, mvx, mvy, x, y);
         if (to_rec) RC(S, c, (L.lx >> 1) + x, (L.ly >> 1) + y) = (uint8_t)v;
@@ -569,24 +797,31 @@ __device__ void chroma_mc(Smem &S, const FrameParams &P, const Leaf &L, int refi
 }
 
 // Luma MC of the listed (slot, ref, mv) predictions into S.pred[slot].
-__device__ void luma_mc_slots(Smem &S, const FrameParams &P, const Leaf &L, int nslots,
-                              const int *slots) {
-    const int cu = L.cu, n = cu * cu;
+// (to_rec: the one listed slot's prediction goes straight into the
+// reconstruction tile, as a skipped leaf's does.)
+__device__ __noinline__ void luma_mc_slots(Smem &, const FrameParams &, const Leaf L, int nslots,
+                                           const int *slots, bool to_rec) {
+    Smem &S = smem_state();
+    const FrameParams &P = g_fp;
+    const int cu = L.cu, n = cu * cu, lg = lg2i(cu);
     for (int i = threadIdx.x; i < nslots * n; i += NT) {
-        const int k = i / n, p = i - k * n, y = p / cu, x = p - y * cu;
+        const int k = i >> (2 * lg), p = i & (n - 1), y = p >> lg, x = p & (cu - 1);
         const int slot = slots[k];
-        LumaMC m;
-        m.init(P.ref_y[S.cand_ref[slot]], P.stride_y, P.W, P.H, S.cand_mvx[slot], S.cand_mvy[slot], cu);
-        int v = m.at(x, y);
         const int r2 = S.cand_ref2[slot];
-        if (r2 >= 0) {
-            // Bi-average with the mirrored (negated absolute) MV on the
-            // second reference (reference src/encoder.c:642-647, 855-859).
-            LumaMC m2;
-            m2.init(P.ref_y[r2], P.stride_y, P.W, P.H, -S.cand_mvx[slot], -S.cand_mvy[slot], cu);
-            v = (v + m2.at(x, y) + 1) >> 1;
+        int v = 0;
+        // Bi-prediction averages with the mirrored (negated absolute) MV on
+        // the second reference (reference src/encoder.c:642-647, 855-859).
+#pragma unroll 1
+        for (int h = 0; h < (r2 >= 0 ? 2 : 1); ++h) {
+            const int sgn = h ? -1 : 1;
+            LumaMC m;
+            m.init(P.ref_y[h ? r2 : S.cand_ref[slot]], P.stride_y, P.W, P.H, sgn * S.cand_mvx[slot],
+                   sgn * S.cand_mvy[slot], cu);
+            const int u = m.at(x, y);
+            v = h ? (v + u + 1) >> 1 : u;
         }
-        S.pred[slot][p] = (uint8_t)v;
+        if (to_rec) RY(S, L.lx + x, L.ly + y) = (uint8_t)v;
+        else S.pred[slot][p] = (uint8_t)v;
     }
     SYNC();
 }
@@ -607,7 +842,7 @@ __device__ void sad_jobs(Smem &S, const Leaf &L, const int *cl, int ncl) {
         const int slot = cl[k];
         int acc = 0;
         for (int p = threadIdx.x; p < n; p += NT) {
-            const int y = p / cu, x = p - y * cu;
+            const int y = p >> lg2i(cu), x = p & (cu - 1);
             acc += absi((int)S.cur_y[(L.ly + y) * 64 + L.lx + x] - lpred(S, cu, slot, dc, x, y));
         }
         acc = __reduce_add_sync(0xffffffffu, acc);
@@ -636,17 +871,18 @@ __device__ void snap(Smem &S, const Leaf &L, int which, bool save) {
     uint8_t *c0 = D == 0 ? S.snap_c0[which][0] : D == 1 ? S.snap_c1[which][0] : S.snap_c2[which][0];
     uint8_t *c1 = D == 0 ? S.snap_c0[which][1] : D == 1 ? S.snap_c1[which][1] : S.snap_c2[which][1];
     MvCell *gs = S.snap_g[D][which];
+    constexpr int lgu = 6 - D, lgs = 5 - D, lgg = 3 - D;
     for (int i = threadIdx.x; i < cu * cu; i += NT) {
-        const int y = i / cu, x = i - y * cu;
+        const int y = i >> lgu, x = i & (cu - 1);
         if (save) ys[i] = RY(S, L.lx + x, L.ly + y); else RY(S, L.lx + x, L.ly + y) = ys[i];
     }
     for (int i = threadIdx.x; i < cs * cs; i += NT) {
-        const int y = i / cs, x = i - y * cs;
+        const int y = i >> lgs, x = i & (cs - 1);
         if (save) { c0[i] = RC(S, 0, (L.lx >> 1) + x, (L.ly >> 1) + y); c1[i] = RC(S, 1, (L.lx >> 1) + x, (L.ly >> 1) + y); }
         else { RC(S, 0, (L.lx >> 1) + x, (L.ly >> 1) + y) = c0[i]; RC(S, 1, (L.lx >> 1) + x, (L.ly >> 1) + y) = c1[i]; }
     }
     for (int i = threadIdx.x; i < gc * gc; i += NT) {
-        const int y = i / gc, x = i - y * gc;
+        const int y = i >> lgg, x = i & (gc - 1);
         if (save) gs[i] = S.grid[(L.cy + y) * 8 + L.cx + x]; else S.grid[(L.cy + y) * 8 + L.cx + x] = gs[i];
     }
     SYNC();
@@ -654,9 +890,9 @@ __device__ void snap(Smem &S, const Leaf &L, int which, bool save) {
 
 // Grid update after a leaf (reference src/encoder.c:1279-1288 / 760-780).
 __device__ void grid_update(Smem &S, const Leaf &L, const Node &nd, int mvpx, int mvpy) {
-    const int gc = L.cu >> 3;
+    const int gc = L.cu >> 3, lgg = lg2i(gc);
     for (int i = threadIdx.x; i < gc * gc; i += NT) {
-        const int y = i / gc, x = i - y * gc;
+        const int y = i >> lgg, x = i & (gc - 1);
         MvCell &g = S.grid[(L.cy + y) * 8 + L.cx + x];
         if (nd.intra) g.intra = 1;
         else {
@@ -687,10 +923,12 @@ __device__ __forceinline__ int dpb_bwd(const FrameParams &P) {
 
 // Chroma MC of both components, averaged over two references when r2 >= 0
 // (second reference with the mirrored MV; reference src/encoder.c:673-699).
-__device__ void chroma_mc_bi(Smem &S, const FrameParams &P, const Leaf &L, int r1, int r2, int mvx, int mvy) {
-    const int cs = L.cu >> 1, Wc = P.W >> 1, Hc = P.H >> 1;
+__device__ __noinline__ void chroma_mc_bi(Smem &, const FrameParams &, const Leaf L, int r1, int r2, int mvx, int mvy) {
+    Smem &S = smem_state();
+    const FrameParams &P = g_fp;
+    const int cs = L.cu >> 1, Wc = P.W >> 1, Hc = P.H >> 1, lgs = lg2i(cs);
     for (int i = threadIdx.x; i < 2 * cs * cs; i += NT) {
-        const int c = i / (cs * cs), p = i - c * cs * cs, y = p / cs, x = p - y * cs;
+        const int c = i >> (2 * lgs), p = i & ((1 << (2 * lgs)) - 1), y = p >> lgs, x = p & (cs - 1);
         int v = chroma_mc_at(c ? P.ref_cr[r1] : P.ref_cb[r1], P.stride_c, Wc, Hc, mvx, mvy, x, y);
         if (r2 >= 0)
             v = (v + chroma_mc_at(c ? P.ref_cr[r2] : P.ref_cb[r2], P.stride_c, Wc, Hc, -mvx, -mvy, x, y) + 1) >> 1;
@@ -708,14 +946,18 @@ __device__ void chroma_mc_bi(Smem &S, const FrameParams &P, const Leaf &L, int r
 __device__ void luma_from_cache(Smem &S, const Leaf &L, int slot, bool dct8) {
     const int cu = L.cu;
     const uint8_t *src = S.crec[slot][dct8 ? 0 : 1];
+    const int lg = lg2i(cu);
     for (int i = threadIdx.x; i < cu * cu; i += NT) {
-        const int y = i / cu, x = i - y * cu;
+        const int y = i >> lg, x = i & (cu - 1);
         RY(S, L.lx + x, L.ly + y) = src[i];
     }
 }
 
-__device__ void leaf_code(Smem &S, const FrameParams &P, const Leaf &L, const QuantParams &ql,
-                          const QuantParams &qc, bool emit, CtuOut *out, bool use_cache = false) {
+__device__ __noinline__ void leaf_code(Smem &, const FrameParams &, const Leaf L, const QuantParams &,
+                          const QuantParams &, bool emit, CtuOut *out, bool use_cache = false) {
+    Smem &S = smem_state();
+    const FrameParams &P = g_fp;
+    const QuantParams &ql = S.qparam[0], &qc = S.qparam[1];
     const Node nd = S.nodes[qt_index(L.depth, L.cx, L.cy)];
     int mvpx, mvpy;
     mvp_at(S.grid, L.cx, L.cy, mvpx, mvpy);
@@ -794,7 +1036,7 @@ __device__ void leaf_code(Smem &S, const FrameParams &P, const Leaf &L, const Qu
                     SYNC();
                 } else {
                     const int slots[1] = {0};
-                    luma_mc_slots(S, P, L, 1, slots);
+                    luma_mc_slots(S, P, L, 1, slots, false);
                 }
                 const int ntu = cu >> 3;
                 const int wl = nd.dct_size ? mini(NW, (ntu * ntu + 3) / 4) : mini(NW, (ntu * ntu * 4 + 7) / 8);
@@ -804,14 +1046,12 @@ __device__ void leaf_code(Smem &S, const FrameParams &P, const Leaf &L, const Qu
             }
         } else {
             coded = false;
-            const int n = cu * cu;
-            for (int i = threadIdx.x; i < n; i += NT) {
-                const int y = i / cu, x = i - y * cu;
-                LumaMC m;
-                m.init(P.ref_y[0], P.stride_y, P.W, P.H, mvx, mvy, cu);
-                RY(S, L.lx + x, L.ly + y) = (uint8_t)m.at(x, y);
+            if (threadIdx.x == 0) {
+                S.cand_mvx[0] = mvx; S.cand_mvy[0] = mvy; S.cand_ref[0] = 0; S.cand_ref2[0] = -1;
             }
             SYNC();
+            const int slots[1] = {0};
+            luma_mc_slots(S, P, L, 1, slots, true);
             if (P.fresh_skip && P.frame_type == 1 && P.ref_valid[0])
                 chroma_mc(S, P, L, 0, mvx, mvy, 0, true);
         }
@@ -831,8 +1071,11 @@ __device__ void leaf_code(Smem &S, const FrameParams &P, const Leaf &L, const Qu
 // ====================================================================
 // Leaf decision (reference src/encoder.c:784-1277).
 // ====================================================================
-__device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
-                                 const QuantParams &ql, const QuantParams &qc) {
+__device__ __noinline__ long long leaf_decide(Smem &, const FrameParams &, const Leaf L,
+                                 const QuantParams &, const QuantParams &) {
+    Smem &S = smem_state();
+    const FrameParams &P = g_fp;
+    const QuantParams &ql = S.qparam[0], &qc = S.qparam[1];
     const int cu = L.cu, tid = threadIdx.x;
     const bool fast = P.preset <= 1;
     const bool medium = P.preset >= 2;
@@ -840,6 +1083,7 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
     const bool is_p = P.frame_type == 1;
     const bool is_b = P.frame_type == 2;
     PHASE_T0();
+    COUNT_D(L.depth);
     int mvpx, mvpy;
     mvp_at(S.grid, L.cx, L.cy, mvpx, mvpy);
     {
@@ -852,7 +1096,7 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
         build_refs(S, L, mm);
     }
     zero_acc(S);
-    PHASE(0);
+    PHASE_D(0, L.depth);
 
     // ---- candidate set -------------------------------------------------
     bool has_glb = false, has_tmp = false, has_me1 = false;
@@ -885,7 +1129,7 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
             me_run(S, 3, gt, P.ref_y[0], P.stride_y, P.W, P.H, L.lx, L.ly, cu,
                    (L.px * 4 + tdx) >> 2, (L.py * 4 + tdy) >> 2, sr);
         SYNC();
-        PHASE(1);
+        PHASE_D(1, L.depth);
         if (has_glb && S.me[2].mvx == S.me[0].mvx && S.me[2].mvy == S.me[0].mvy) has_glb = false;
         if (has_tmp && S.me[3].mvx == S.me[0].mvx && S.me[3].mvy == S.me[0].mvy) has_tmp = false;
         int slots[5], ns = 0;
@@ -905,8 +1149,8 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
         }
         if (medium) n8only = 1;
         SYNC();
-        luma_mc_slots(S, P, L, ns, slots);
-        PHASE(2);
+        luma_mc_slots(S, P, L, ns, slots, false);
+        PHASE_D(2, L.depth);
     } else if (is_b) {
         // Forward / backward searches (reference src/encoder.c:795-852).
         const int sr = fast ? 16 : 32;
@@ -915,7 +1159,7 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
         else if (g == 1 && rb >= 0)
             me_run(S, 1, gt, P.ref_y[rb], P.stride_y, P.W, P.H, L.lx, L.ly, cu, cx0, cy0, sr);
         SYNC();
-        PHASE(1);
+        PHASE_D(1, L.depth);
         int slots[5], ns = 0;
         if (rf >= 0) slots[ns++] = K_B0 + 0;
         if (rb >= 0) slots[ns++] = K_B0 + 1;
@@ -939,8 +1183,8 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
         }
         n8only = (mrg && rf >= 0 && rb >= 0) + (mrg && rf >= 0) + (mrg && rb >= 0);
         SYNC();
-        luma_mc_slots(S, P, L, ns, slots);
-        PHASE(2);
+        luma_mc_slots(S, P, L, ns, slots, false);
+        PHASE_D(2, L.depth);
     }
 
     // ---- residual coding / SAD proxies for every candidate --------------
@@ -983,13 +1227,13 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
         if (use4) luma_jobs4(S, L, S.cl, ncl, ql, true, false, nullptr, w8);
         if (n8only) luma_jobs8(S, L, S.cl2, n8only, ql, true, false, nullptr, w8 + w4);
         SYNC();
-        PHASE(3);
+        PHASE_D(3, L.depth);
         if (is_p && medium) {
             // Skip pre-check (src/encoder.c:1064-1142): luma SSE of the merge
             // prediction, then fresh chroma SSE when the luma is exact.
             long long acc = 0;
             for (int p = tid; p < cu * cu; p += NT) {
-                const int y = p / cu, x = p - y * cu;
+                const int y = p >> lg2i(cu), x = p & (cu - 1);
                 const int d = (int)S.cur_y[(L.ly + y) * 64 + L.lx + x] - (int)S.pred[K_MRG][p];
                 acc += d * d;
             }
@@ -1001,7 +1245,7 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
                 const int cs = cu >> 1;
                 long long ac = 0;
                 for (int p = tid; p < cs * cs; p += NT) {
-                    const int y = p / cs, x = p - y * cs;
+                    const int y = p >> lg2i(cs), x = p & (cs - 1);
                     const int db = (int)S.cur_c[0][((L.ly >> 1) + y) * 32 + (L.lx >> 1) + x] - (int)S.cpred[0][p];
                     const int dr = (int)S.cur_c[1][((L.ly >> 1) + y) * 32 + (L.lx >> 1) + x] - (int)S.cpred[1][p];
                     ac += db * db + dr * dr;
@@ -1016,7 +1260,7 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
         }
     }
 
-    PHASE(4);
+    PHASE_D(4, L.depth);
     // ---- in-order candidate scan (strict <, first minimum wins) ---------
     // Each lane of warp 0 scores one candidate of the scan order (inter
     // candidates, then the intra modes), then a warp argmin on (cost,
@@ -1053,56 +1297,53 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
         int kind = C_NONE, slot = 0;
         if (lane < nk) kind = kinds[lane];
         else if (lane < n) { kind = C_INTRA; slot = S.cl[ninter + lane - nk]; }
-        long long cost = (long long)1 << 60;   // no candidate: defaults, as the sequential scan
+        // Each kind only sets its parameters (a short divergent switch); the
+        // cost then comes from one common path for all lanes:
+        //   cost = distortion + lambda * (extra + MV bits + level bits)
+        // with distortion / level bits from best_of (explicit inter and
+        // intra), the 8x8-only sums (merges), the SAD proxy (fast presets)
+        // or nothing (skip).
+        int sl = -1, extra = 0, plb = 0, mvsl = -1;
+        bool mvbits = false, merge8 = false, proxy = false;
         int f_intra = 0, f_skip = 0, f_merge = 0, f_bi = 0, f_dct = 1, f_ref = 0, f_mx = 0, f_my = 0, f_mode = 1;
-        auto explicit_inter = [&](int sl, int extra_bits, bool sad_proxy, int lb_proxy) {
-            const int dx = S.cand_mvx[sl] - base_x, dy = S.cand_mvy[sl] - base_y;
-            long long dl;
-            int lb, dct = 1;
-            if (sad_proxy) {
-                const long long sad = S.acc_sse[sl][0];
-                dl = (sad * sad) / (long long)(cu * cu);
-                lb = lb_proxy;
-            } else {
-                dl = best_of(S, sl, use4, lam, lb, dct);
-            }
-            cost = dl + lam * (extra_bits + se_bits(dx) + se_bits(dy) + lb);
-            f_dct = dct; f_mx = dx; f_my = dy;
-        };
         switch (kind) {
-            case C_P_ME0: explicit_inter(K_ME0, 6 + (P.multiref ? 2 : 0), fast, 3); break;
-            case C_P_ME1: explicit_inter(K_ME1, 8, false, 0); f_ref = 1; break;
-            case C_P_GLB: explicit_inter(K_GLB, 6 + (P.multiref ? 1 : 0), false, 0); break;
-            case C_P_TMP: explicit_inter(K_TMP, 6 + (P.multiref ? 2 : 0), false, 0); break;
-            case C_P_MRG:
-                cost = (long long)S.acc_sse[K_MRG][0] + lam * (6 + S.acc_bits[K_MRG][0]);
-                f_merge = 1;
-                f_mx = S.cand_mvx[K_ME0] - base_x; f_my = S.cand_mvy[K_ME0] - base_y;
-                break;
-            case C_P_SKIP: cost = lam * 2; f_skip = 1; break;
-            case C_B_DIR0: explicit_inter(K_B0 + 0, 6, fast, 3); f_ref = 0; break;
-            case C_B_DIR1: explicit_inter(K_B0 + 1, 6, fast, 3); f_ref = 1; break;
-            case C_B_M2: case C_B_M3: case C_B_M4: {
-                const int k = kind == C_B_M2 ? 2 : (kind == C_B_M3 ? 3 : 4), sl = K_B0 + k;
-                cost = (long long)S.acc_sse[sl][0] + lam * (6 + S.acc_bits[sl][0]);
-                f_merge = 1; f_ref = k == 4 ? 1 : 0; f_bi = k == 2 ? 1 : 0;
-                break;
-            }
-            case C_INTRA: {
-                long long dl;
-                int lb, dct = 1;
-                if (fast) {
-                    const long long sad = S.acc_sse[slot][0];
-                    dl = (sad * sad) / (long long)(cu * cu);
-                    lb = 8;
-                } else {
-                    dl = best_of(S, slot, use4, lam, lb, dct);
-                }
-                cost = dl + lam * (8 + lb);
-                f_intra = 1; f_mode = slot - K_INTRA; f_dct = dct;
-                break;
-            }
+            case C_P_ME0: sl = K_ME0; extra = 6 + (P.multiref ? 2 : 0); mvbits = true; proxy = fast; plb = 3; break;
+            case C_P_ME1: sl = K_ME1; extra = 8; mvbits = true; f_ref = 1; break;
+            case C_P_GLB: sl = K_GLB; extra = 6 + (P.multiref ? 1 : 0); mvbits = true; break;
+            case C_P_TMP: sl = K_TMP; extra = 6 + (P.multiref ? 2 : 0); mvbits = true; break;
+            case C_P_MRG: sl = K_MRG; extra = 6; merge8 = true; f_merge = 1; mvsl = K_ME0; break;
+            case C_P_SKIP: extra = 2; f_skip = 1; break;
+            case C_B_DIR0: sl = K_B0; extra = 6; mvbits = true; proxy = fast; plb = 3; break;
+            case C_B_DIR1: sl = K_B0 + 1; extra = 6; mvbits = true; proxy = fast; plb = 3; f_ref = 1; break;
+            case C_B_M2: sl = K_B0 + 2; extra = 6; merge8 = true; f_merge = 1; f_bi = 1; break;
+            case C_B_M3: sl = K_B0 + 3; extra = 6; merge8 = true; f_merge = 1; break;
+            case C_B_M4: sl = K_B0 + 4; extra = 6; merge8 = true; f_merge = 1; f_ref = 1; break;
+            case C_INTRA: sl = slot; extra = 8; proxy = fast; plb = 8; f_intra = 1; f_mode = slot - K_INTRA; break;
             default: break;
+        }
+        if (mvbits) mvsl = sl;
+        long long cost = (long long)1 << 60;   // no candidate: defaults, as the sequential scan
+        if (kind != C_NONE) {
+            long long dl = 0;
+            int lb = 0;
+            if (sl >= 0) {
+                if (proxy) {
+                    const long long sad = S.acc_sse[sl][0];
+                    dl = (sad * sad) >> (2 * lg2i(cu));   // / (cu * cu), sad >= 0
+                    lb = plb;
+                } else if (merge8) {
+                    dl = S.acc_sse[sl][0];
+                    lb = S.acc_bits[sl][0];
+                } else {
+                    dl = best_of(S, sl, use4, lam, lb, f_dct);
+                }
+            }
+            int mb = 0;
+            if (mvsl >= 0) {
+                f_mx = S.cand_mvx[mvsl] - base_x; f_my = S.cand_mvy[mvsl] - base_y;
+                if (mvbits) mb = se_bits(f_mx) + se_bits(f_my);
+            }
+            cost = dl + lam * (extra + mb + lb);
         }
         // first minimum: smallest cost, then smallest scan position
         long long bc = cost;
@@ -1141,7 +1382,7 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
     }
     SYNC();
 
-    PHASE(5);
+    PHASE_D(5, L.depth);
     // ---- intra chroma choice: MC vs CfL-blended DC (src/encoder.c:1194-1221)
     const Node nd0 = S.nodes[qt_index(L.depth, L.cx, L.cy)];
     if (nd0.intra && !fast && medium) {
@@ -1172,12 +1413,12 @@ __device__ long long leaf_decide(Smem &S, const FrameParams &P, const Leaf &L,
         SYNC();
     }
     const long long best = S.best_cost;
-    PHASE(6);
+    PHASE_D(6, L.depth);
     // ---- replay of the winner ------------------------------------------
     // (luma from the scoring pass's cache where it holds the winner)
     const Node ndw = S.nodes[qt_index(L.depth, L.cx, L.cy)];
     leaf_code(S, P, L, ql, qc, false, nullptr, !fast && cu <= 16 && !ndw.skip && S.win_slot >= 0);
-    PHASE(7);
+    PHASE_D(7, L.depth);
     return best;
 }
 
@@ -1282,7 +1523,8 @@ __device__ void qt_write(Smem &S, const FrameParams &P, int ctu_x, int ctu_y, in
 // ====================================================================
 // In-loop filters on the CTU tile.
 // ====================================================================
-__device__ void deblock_tile(Smem &S, int qp) {
+__device__ __noinline__ void deblock_tile(Smem &, int qp) {
+    Smem &S = smem_state();
     const int tc = clampi(qp / 3, 1, 10);
     const int cqp = clampi(qp - 1, 0, 63), ctc = clampi(cqp / 4, 1, 6);
     // Luma vertical edges x = 4..60 and chroma (Cb) vertical edges x = 4..28.
@@ -1334,7 +1576,8 @@ __device__ void deblock_tile(Smem &S, int qp) {
 
 // Luma SAO band offset: choose (reference src/filter.c:269-319), rate gate
 // (src/encoder.c:1473-1493) and apply (src/filter.c:251-266).
-__device__ void sao_tile(Smem &S, int w, int h, int lambda_sao) {
+__device__ __noinline__ void sao_tile(Smem &, int w, int h, int lambda_sao) {
+    Smem &S = smem_state();
     if (threadIdx.x < 32) {
         S.band_sum[threadIdx.x] = 0; S.band_cnt[threadIdx.x] = 0;
         S.band_sq[threadIdx.x] = 0; S.band_new[threadIdx.x] = 0;
@@ -1497,7 +1740,7 @@ __global__ void __launch_bounds__(NT, CTAS_PER_SM)
 ctu_kernel(const FrameParams *__restrict__ params, const int *__restrict__ items) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     Smem &S = *reinterpret_cast<Smem *>(smem_raw);
-    __shared__ FrameParams P;
+    FrameParams &P = g_fp;
     const int item = items[blockIdx.x];
     if (threadIdx.x == 0) P = params[item >> 20];
     SYNC();
@@ -1530,7 +1773,7 @@ ctu_persistent_kernel(const FrameParams *__restrict__ params, const int *__restr
                       int *ctrl) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     Smem &S = *reinterpret_cast<Smem *>(smem_raw);
-    __shared__ FrameParams P;
+    FrameParams &P = g_fp;
     __shared__ int s_item;
 #ifdef TCB_PHASE_PROFILE
     const long long k0 = clock64();   // residency of the CTA (slot 14); neighbour waits in slot 13
@@ -1949,7 +2192,7 @@ __device__ void dec_leaf(Smem &S, const FrameParams &P, const Leaf &L, const int
         SYNC();
         if (r1 >= 0) {
             const int slots[1] = {0};
-            luma_mc_slots(S, P, L, 1, slots);
+            luma_mc_slots(S, P, L, 1, slots, false);
         } else {
             for (int i = threadIdx.x; i < cu * cu; i += NT) S.pred[0][i] = 128;
             SYNC();
@@ -2017,7 +2260,7 @@ __global__ void __launch_bounds__(NT, CTAS_PER_SM)
 decode_kernel(const FrameParams *__restrict__ params, const int *__restrict__ items) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     Smem &S = *reinterpret_cast<Smem *>(smem_raw);
-    __shared__ FrameParams P;
+    FrameParams &P = g_fp;   // the shared helpers (MC, chroma) read the frame from g_fp
     const int item = items[blockIdx.x];
     const int sid = item >> 20, row = (item >> 10) & 1023, col = item & 1023;
     if (threadIdx.x == 0) P = params[sid];
@@ -2101,10 +2344,11 @@ extern "C" __attribute__((visibility("default"))) int tcb_debug_op_counts(unsign
     unsigned long long z[4] = {0};
     return cudaMemcpyToSymbol(tcb::tcb_op_counts, z, sizeof(z)) == cudaSuccess ? 0 : -1;
 }
-extern "C" __attribute__((visibility("default"))) int tcb_debug_phase_cycles(unsigned long long *out16) {
+extern "C" __attribute__((visibility("default"))) int tcb_debug_phase_cycles(unsigned long long *out64) {
     cudaDeviceSynchronize();
-    if (cudaMemcpyFromSymbol(out16, tcb::tcb_phase_cycles, 16 * sizeof(unsigned long long)) != cudaSuccess) return -1;
-    unsigned long long z[16] = {0};
+    if (cudaMemcpyFromSymbol(out64, tcb::tcb_phase_cycles, tcb::PHASE_SLOTS * sizeof(unsigned long long)) != cudaSuccess)
+        return -1;
+    unsigned long long z[tcb::PHASE_SLOTS] = {0};
     return cudaMemcpyToSymbol(tcb::tcb_phase_cycles, z, sizeof(z)) == cudaSuccess ? 0 : -1;
 }
 #endif

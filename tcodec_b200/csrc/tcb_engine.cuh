@@ -6,14 +6,12 @@
 
 namespace tcb {
 
-#ifndef TCB_NT
-#define TCB_NT 512
-#endif
-constexpr int NT = TCB_NT;          // threads per CTA (one CTU)
-constexpr int CTAS_PER_SM = 512 / NT;   // CTUs resident per SM
+constexpr int NT = 512;             // threads per CTA (one CTU)
+constexpr int CTAS_PER_SM = 1;      // CTUs resident per SM
 constexpr int NW = NT / 32;         // warps per CTA
 constexpr int NGROUP = 4;           // motion-search warp groups
 constexpr int GT = NT / NGROUP;     // threads per motion-search group
+static_assert(GT == 128, "the motion-search work split assumes 4-warp groups");
 
 // Recon tile: luma rows -1..63 and columns -8..63 of the CTU, chroma rows
 // -1..31 and columns -4..31.  Column offsets keep the interior aligned.
@@ -39,8 +37,7 @@ constexpr int NPRED = 5;
 constexpr int IPRED_MAX = TCB_IPRED_MAX;   // largest leaf whose intra predictions are kept            // inter prediction buffers (slots 0..4)
 
 struct MeGroup {
-    int sad[8];
-    int part[GT / 32][8];
+    int part[2][32];    // per-warp partial sums, double-buffered (see group_int_sads)
     int mvx, mvy, best;
 };
 

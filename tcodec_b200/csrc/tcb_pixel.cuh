@@ -147,16 +147,14 @@ __device__ __forceinline__ int chroma_mc_at(const uint8_t *ref, int s, int W, in
 
 // ---------------------------------------------------------------- intra
 
-// Angular displacement tables in 1/32 sample per row/column
-// (reference src/predict.c:180-188 and 247-257).
-__device__ __forceinline__ int ang_disp_vert(int mode) {
-    const int t[7] = {32, 16, 6, 0, -6, -16, -32};
-    return t[mode - 2];
-}
-__device__ __forceinline__ int ang_disp_horiz(int mode) {
-    const int t[9] = {32, 16, 6, 0, -6, -16, -32, -48, 48};
-    return t[mode - 9];
-}
+// Angular displacement in 1/32 sample per row (modes 2..8) or column
+// (modes 9..17) (reference src/predict.c:180-188 and 247-257), indexed by
+// mode.  A file-scope constant table: a function-local array indexed at run
+// time would be rebuilt in local memory on every call.
+static __constant__ int8_t c_ang_disp[18] = {0, 0, 32, 16, 6, 0, -6, -16, -32,
+                                             32, 16, 6, 0, -6, -16, -32, -48, 48};
+__device__ __forceinline__ int ang_disp_vert(int mode) { return c_ang_disp[mode]; }
+__device__ __forceinline__ int ang_disp_horiz(int mode) { return c_ang_disp[mode]; }
 
 // Intra prediction sample (x, y) of an N x N block.  `ra` and `rl` point at
 // index 0 of the above / left reference runs built by the v2 reference
@@ -166,7 +164,8 @@ __device__ __forceinline__ int ang_disp_horiz(int mode) {
 __device__ __forceinline__ int intra_at(const uint8_t *ra, const uint8_t *rl, int N,
                                         int mode, int dc, int x, int y) {
     if (mode == 0) {
-        int v = (ra[x + 1] * (N - 1 - y) + rl[y + 1] * (N - 1 - x) + ra[0] * (x + y) + N) / (2 * N);
+        // every term is non-negative and 2N a power of two: the division is a shift
+        int v = (ra[x + 1] * (N - 1 - y) + rl[y + 1] * (N - 1 - x) + ra[0] * (x + y) + N) >> (__ffs(N));
         return clampi(v, 0, 255);
     }
     if (mode == 1 || mode < 0 || mode > 17) return dc;

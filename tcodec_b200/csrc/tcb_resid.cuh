@@ -111,10 +111,11 @@ __device__ __forceinline__ int quant_rdoq(int c, int band, const QuantParams &qp
     if (c > 0) q = udiv_rcp((uint32_t)(c + off), eff, rcp);
     else if (c < 0) q = -udiv_rcp((uint32_t)(-c + off), eff, rcp);
     if (q == 1 || q == -1) {
+        // zero wins when c^2 + lambda < (c - dq)^2 + 2 lambda, i.e. when
+        // dq * (2c - dq) < lambda; |c| <= 2^15 and |dq| <= 9194 keep the
+        // product below 2^30
         const int dq = q > 0 ? eff + qp.bias[band] : -eff - qp.bias[band];
-        const long long dz = (long long)c * c + qp.lambda;
-        const long long dk = (long long)(c - dq) * (c - dq) + 2 * qp.lambda;
-        if (dz < dk) q = 0;
+        if ((long long)(dq * (2 * c - dq)) < qp.lambda) q = 0;
     }
     return q;
 }
@@ -129,6 +130,53 @@ __device__ __forceinline__ int level_bits(int v) {
     return v == 0 ? 1 : 2 + 2 * bitlen((unsigned)absi(v));
 }
 
+// Exact 8- and 4-point DCT sums by partial butterflies.  The 14-bit
+// matrices keep the cosine symmetries exactly (lround is odd-symmetric):
+// c8[k][7-n] = (-1)^k c8[k][n], c8[2m][3-n] = (-1)^m c8[2m][n] for n < 4,
+// c4[k][3-n] = (-1)^k c4[k][n].  So every sum the reference forms,
+// out[k] = sum_n c[k][n] x[n] (forward) or out[n] = sum_k c[k][n] y[k]
+// (inverse), is the same integer from even / odd halves: 24 products per
+// 8-point transform instead of 64, 8 per 4-point instead of 16.
+__device__ __forceinline__ void fdct8_sums(const int x[8], int out[8]) {
+    int E[4], O[4];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) { E[n] = x[n] + x[7 - n]; O[n] = x[n] - x[7 - n]; }
+    const int EE0 = E[0] + E[3], EE1 = E[1] + E[2], EO0 = E[0] - E[3], EO1 = E[1] - E[2];
+    out[0] = c_dct8[0][0] * EE0 + c_dct8[0][1] * EE1;
+    out[4] = c_dct8[4][0] * EE0 + c_dct8[4][1] * EE1;
+    out[2] = c_dct8[2][0] * EO0 + c_dct8[2][1] * EO1;
+    out[6] = c_dct8[6][0] * EO0 + c_dct8[6][1] * EO1;
+#pragma unroll
+    for (int k = 1; k < 8; k += 2)
+        out[k] = c_dct8[k][0] * O[0] + c_dct8[k][1] * O[1] + c_dct8[k][2] * O[2] + c_dct8[k][3] * O[3];
+}
+__device__ __forceinline__ void idct8_sums(const int y[8], int out[8]) {
+    const int e0 = c_dct8[0][0] * y[0] + c_dct8[4][0] * y[4], e1 = c_dct8[0][1] * y[0] + c_dct8[4][1] * y[4];
+    const int o0 = c_dct8[2][0] * y[2] + c_dct8[6][0] * y[6], o1 = c_dct8[2][1] * y[2] + c_dct8[6][1] * y[6];
+    const int ev[4] = {e0 + o0, e1 + o1, e1 - o1, e0 - o0};
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+        const int od = c_dct8[1][n] * y[1] + c_dct8[3][n] * y[3] + c_dct8[5][n] * y[5] + c_dct8[7][n] * y[7];
+        out[n] = ev[n] + od;
+        out[7 - n] = ev[n] - od;
+    }
+}
+__device__ __forceinline__ void fdct4_sums(const int x[4], int out[4]) {
+    const int E0 = x[0] + x[3], E1 = x[1] + x[2], O0 = x[0] - x[3], O1 = x[1] - x[2];
+    out[0] = c_dct4[0][0] * E0 + c_dct4[0][1] * E1;
+    out[2] = c_dct4[2][0] * E0 + c_dct4[2][1] * E1;
+    out[1] = c_dct4[1][0] * O0 + c_dct4[1][1] * O1;
+    out[3] = c_dct4[3][0] * O0 + c_dct4[3][1] * O1;
+}
+__device__ __forceinline__ void idct4_sums(const int y[4], int out[4]) {
+#pragma unroll
+    for (int n = 0; n < 2; ++n) {
+        const int ev = c_dct4[0][n] * y[0] + c_dct4[2][n] * y[2], od = c_dct4[1][n] * y[1] + c_dct4[3][n] * y[3];
+        out[n] = ev + od;
+        out[3 - n] = ev - od;
+    }
+}
+
 // 8x8 TU on an octet.  In: res_row = clipped residual row `l8`.
 // Out: q_col[k] = quantised level at (k, l8); r_col[k] = reconstructed
 // residual at (k, l8) (int16-wrapped like tc_coeff_t); returns the bit
@@ -136,27 +184,20 @@ __device__ __forceinline__ int level_bits(int v) {
 __device__ __forceinline__ int tu8_code(int l8, const int res_row[8], int *scr,
                                         const QuantParams &qp, int q_col[8], int r_col[8]) {
     int t[8];
+    fdct8_sums(res_row, t);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        int acc = 0;
-#pragma unroll
-        for (int n = 0; n < 8; ++n) acc += c_dct8[k][n] * res_row[n];
-        t[k] = (acc + 8192) >> 14;
-    }
-#pragma unroll
-    for (int k = 0; k < 8; ++k) scr[l8 * 9 + k] = t[k];
+    for (int k = 0; k < 8; ++k) scr[l8 * 9 + k] = (t[k] + 8192) >> 14;
     __syncwarp();
     int col[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) col[i] = scr[i * 9 + l8];
     __syncwarp();
     int nz = 0, last = -1;
+    int cs8[8];
+    fdct8_sums(col, cs8);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-        int acc = 0;
-#pragma unroll
-        for (int n = 0; n < 8; ++n) acc += c_dct8[k][n] * col[n];
-        const int c = (int16_t)((acc + 8192) >> 14);
+        const int c = (int16_t)((cs8[k] + 8192) >> 14);
         const int pos = k * 8 + l8;
         const int q = (int16_t)quant_rdoq(c, band_rc<8>(k, l8), qp);
         q_col[k] = q;
@@ -180,24 +221,17 @@ __device__ __forceinline__ int tu8_code(int l8, const int res_row[8], int *scr,
 #pragma unroll
     for (int n = 0; n < 8; ++n) row[n] = scr[l8 * 9 + n];
     __syncwarp();
+    int is8[8];
+    idct8_sums(row, is8);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        int acc = 0;
-#pragma unroll
-        for (int n = 0; n < 8; ++n) acc += c_dct8[n][k] * row[n];
-        scr[l8 * 9 + k] = (acc + 8192) >> 14;
-    }
+    for (int k = 0; k < 8; ++k) scr[l8 * 9 + k] = (is8[k] + 8192) >> 14;
     __syncwarp();
 #pragma unroll
     for (int n = 0; n < 8; ++n) col[n] = scr[n * 9 + l8];
     __syncwarp();
+    idct8_sums(col, is8);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        int acc = 0;
-#pragma unroll
-        for (int n = 0; n < 8; ++n) acc += c_dct8[n][k] * col[n];
-        r_col[k] = (int16_t)((acc + 8192) >> 14);
-    }
+    for (int k = 0; k < 8; ++k) r_col[k] = (int16_t)((is8[k] + 8192) >> 14);
     return bits;
 }
 
@@ -206,27 +240,20 @@ __device__ __forceinline__ int tu8_code(int l8, const int res_row[8], int *scr,
 __device__ __forceinline__ int tu4_code(int l4, const int res_row[4], int *scr,
                                         const QuantParams &qp, int q_col[4], int r_col[4]) {
     int t[4];
+    fdct4_sums(res_row, t);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        int acc = 0;
-#pragma unroll
-        for (int n = 0; n < 4; ++n) acc += c_dct4[k][n] * res_row[n];
-        t[k] = (acc + 8192) >> 14;
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) scr[l4 * 5 + k] = t[k];
+    for (int k = 0; k < 4; ++k) scr[l4 * 5 + k] = (t[k] + 8192) >> 14;
     __syncwarp();
     int col[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) col[i] = scr[i * 5 + l4];
     __syncwarp();
     int nz = 0, last = -1;
+    int cs4[4];
+    fdct4_sums(col, cs4);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        int acc = 0;
-#pragma unroll
-        for (int n = 0; n < 4; ++n) acc += c_dct4[k][n] * col[n];
-        const int c = (int16_t)((acc + 8192) >> 14);
+        const int c = (int16_t)((cs4[k] + 8192) >> 14);
         const int pos = k * 4 + l4;
         const int q = (int16_t)quant_rdoq(c, band_rc<4>(k, l4), qp);
         q_col[k] = q;
@@ -249,24 +276,17 @@ __device__ __forceinline__ int tu4_code(int l4, const int res_row[4], int *scr,
 #pragma unroll
     for (int n = 0; n < 4; ++n) row[n] = scr[l4 * 5 + n];
     __syncwarp();
+    int is4[4];
+    idct4_sums(row, is4);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        int acc = 0;
-#pragma unroll
-        for (int n = 0; n < 4; ++n) acc += c_dct4[n][k] * row[n];
-        scr[l4 * 5 + k] = (acc + 8192) >> 14;
-    }
+    for (int k = 0; k < 4; ++k) scr[l4 * 5 + k] = (is4[k] + 8192) >> 14;
     __syncwarp();
 #pragma unroll
     for (int n = 0; n < 4; ++n) col[n] = scr[n * 5 + l4];
     __syncwarp();
+    idct4_sums(col, is4);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        int acc = 0;
-#pragma unroll
-        for (int n = 0; n < 4; ++n) acc += c_dct4[n][k] * col[n];
-        r_col[k] = (int16_t)((acc + 8192) >> 14);
-    }
+    for (int k = 0; k < 4; ++k) r_col[k] = (int16_t)((is4[k] + 8192) >> 14);
     return bits;
 }
 
