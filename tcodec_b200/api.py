@@ -146,6 +146,7 @@ class Encoder:
         if not self.h:
             raise RuntimeError("tc_encoder_create failed (no CUDA device or invalid config)")
         self.w, self.hgt = cfg.width, cfg.height
+        self.last_key_frame = None   # key_frame flag of the last packet encode() returned
 
     def close(self) -> None:
         if self.h:
@@ -173,6 +174,7 @@ class Encoder:
             return None
         if r != TC_OK:
             raise RuntimeError(f"tc_encoder_encode -> {r}")
+        self.last_key_frame = int(pkt.key_frame)
         return ctypes.string_at(pkt.data, pkt.size)
 
     def flush(self) -> List[bytes]:
@@ -535,6 +537,8 @@ def bind_server(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.tcb_server_step.restype = ctypes.c_int
     lib.tcb_server_stats.argtypes = [vp] + [vp] * 5
     lib.tcb_server_set_graphs.argtypes = [vp, ctypes.c_int]
+    lib.tcb_server_get_timing.argtypes = [vp, vp, vp, vp]
+    lib.tcb_server_get_timing.restype = None
     return lib
 
 
@@ -602,6 +606,13 @@ class Server:
             data = ctypes.string_at(e.packet.data, e.packet.size) if e.status == TC_OK else None
             res.append((e.session, e.status, data))
         return res
+
+    def timing(self):
+        """Host ms in admission and in whole steps since creation, sessions
+        admitted (tcb_server_get_timing)."""
+        a, st, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_longlong()
+        self.lib.tcb_server_get_timing(self.h, ctypes.byref(a), ctypes.byref(st), ctypes.byref(n))
+        return dict(admit_ms=a.value, step_ms=st.value, admitted=n.value)
 
     def stats(self):
         w, a, d = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

@@ -149,16 +149,39 @@ def test_preset_entropy_matrix_matches_reference(lib, ref_lib, size):
                     assert np.array_equal(pd, pb), (size, kw)
 
 
-@pytest.mark.parametrize("name", ["cfg0", "cfg1"])
+@pytest.mark.parametrize("name", ["cfg0", "cfg1", "cfg2"])
 def test_single_stream_configs_known_answers(lib, name):
-    """The two single-stream workloads at full length through tc_encoder_*:
-    320x240 x 30 frames (1 searched reference) and 1280x720 x 60 frames
-    (2 searched references, rectangles moving over global motion).  Every
-    packet and the final reconstruction equal the reference encoder's
-    (tests/golden/configs_v2.json, from tests/golden/make_config_golden.py)."""
+    """The single-stream workloads at full length through tc_encoder_*:
+    320x240 x 30 frames (1 searched reference), 1280x720 x 60 frames
+    (2 searched references, rectangles moving over global motion) and
+    1920x1080 x 120 frames of GOP4 hierarchical B frames (the headline
+    workload).  Every packet and the final reconstruction equal the
+    reference encoder's (tests/golden/configs_v2.json, from
+    tests/golden/make_config_golden.py)."""
     from tests.golden import make_config_golden as cg
     want = json.load(open(os.path.join(HERE, "golden", "configs_v2.json")))[name]
     got = cg.run(lib, name)
+    assert got["sizes"] == want["sizes"]
+    assert got["packets"] == want["packets"]
+    assert got["final_recon"] == want["final_recon"]
+
+
+SCASES = json.load(open(os.path.join(HERE, "golden", "scenecut_v2.json")))
+
+
+@pytest.mark.parametrize("name", sorted(SCASES))
+def test_scene_cut_keyframes(lib, name):
+    """P-only clips with hard cuts between two scenes whose luma histograms
+    barely overlap: the reference's chi-square scene-cut test
+    (src/encoder.c:2650-2679) turns the first frame of each new scene into a
+    key frame.  Key-frame flags, every packet and the final reconstruction
+    equal the reference encoder's (tests/golden/scenecut_v2.json, from
+    tests/golden/make_scenecut_golden.py)."""
+    from tests.golden import make_scenecut_golden as sg
+    want = SCASES[name]
+    assert sum(want["key_frames"][1:]) >= 1        # the cut fired in the reference
+    got = sg.run(lib, name)
+    assert got["key_frames"] == want["key_frames"]
     assert got["sizes"] == want["sizes"]
     assert got["packets"] == want["packets"]
     assert got["final_recon"] == want["final_recon"]
