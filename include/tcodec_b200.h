@@ -157,6 +157,12 @@ void tcb_server_stats(tcb_server_t *server, int *waiting, int *active, int *reti
                       size_t *bytes_in_use, size_t *bytes_budget);
 /* CUDA-graph replay of every step's device work (as tcb_batch_set_graphs). */
 void tcb_server_set_graphs(tcb_server_t *server, int enabled);
+/* Host milliseconds spent since creation admitting sessions (setting up
+ * their encoders in the budget's arena) and in whole tcb_server_step calls
+ * (admission, uploads, the device step and entropy coding), and the number
+ * of sessions admitted. */
+void tcb_server_get_timing(tcb_server_t *server, double *admit_ms, double *step_ms,
+                           long long *admitted);
 
 /* ---------------------------------------------------------------------
  * Part 2: standalone kernels.
@@ -213,7 +219,11 @@ tc_error_t tcb_ctu_encode_frame(const tcb_frame_desc_t *desc, void *scratch, siz
  *    TC_ERR_PARAM.
  *  - The first call on a device, made with that device current, looks up
  *    the array's device address and uploads the constant tables; make
- *    that first call before any stream capture.
+ *    that first call before any stream capture.  The first launch of the
+ *    CTU engine in a process (through this or any other entry point) can
+ *    also make the CUDA driver enlarge its local-memory reservation for
+ *    the engine's stack and register spills, which is device memory the
+ *    driver takes; later calls take none.
  *  - Every call on a device shares the one array, which keeps the last
  *    call's contents; each call resets what must start at zero on
  *    `stream` before its encode kernel runs.  Calls whose work overlaps

@@ -18,6 +18,7 @@
 //   output is bit-identical to encoding the session alone.
 #include <string.h>
 
+#include <chrono>
 #include <deque>
 #include <vector>
 
@@ -60,6 +61,10 @@ struct tcb_server {
     std::vector<tc_packet_t> pkts;
     std::vector<int> status;
     int device = 0;
+    // host time inside admission (encoder set-up on the arena) and inside
+    // whole steps, milliseconds since creation; sessions admitted
+    double admit_ms = 0.0, step_ms = 0.0;
+    long long admitted = 0;
 };
 
 namespace {
@@ -98,7 +103,12 @@ void admit(tcb_server *s) {
         ss.slot = slot;
         ss.state = ACTIVE;
         s->waiting.pop_front();
+        ++s->admitted;
     }
+}
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
 }  // namespace
@@ -183,10 +193,29 @@ int tcb_server_session_state(tcb_server_t *s, int id) {
     return s->sessions[id].state;
 }
 
+static int server_step(tcb_server_t *s, tcb_server_packet_t *out);
+
 int tcb_server_step(tcb_server_t *s, tcb_server_packet_t *out, int cap) {
     if (!s || !out || cap < s->max_active) return TC_ERR_PARAM;
     if (cudaSetDevice(s->device) != cudaSuccess) return TC_ERR_INTERNAL;
+    const auto t0 = std::chrono::steady_clock::now();
     admit(s);
+    s->admit_ms += ms_since(t0);
+    const int r = server_step(s, out);
+    s->step_ms += ms_since(t0);
+    return r;
+}
+
+void tcb_server_get_timing(tcb_server_t *s, double *admit_ms, double *step_ms, long long *admitted) {
+    if (!s) return;
+    if (admit_ms) *admit_ms = s->admit_ms;
+    if (step_ms) *step_ms = s->step_ms;
+    if (admitted) *admitted = s->admitted;
+}
+
+// The encoding part of a step: every admitted session with input (or a
+// B-frame tail) advances one frame.
+static int server_step(tcb_server_t *s, tcb_server_packet_t *out) {
     std::vector<int> part;
     for (int slot = 0; slot < s->max_active; ++slot) {
         const int id = s->slot_session[slot];

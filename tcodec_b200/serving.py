@@ -33,6 +33,8 @@ def serve(lib, sessions: List[dict], clips: List[list], hbm_budget_bytes: int, m
     packets: List[List[bytes]] = [[] for _ in range(n)]
     done = [False] * n
     lat: List[float] = []
+    first_pkt: List[float] = [0.0] * n      # arrival -> first packet of each session (s)
+    step_log: List[tuple] = []              # (end of step s, packets, active, waiting)
     steps = 0
     peak_active = 0
     peak_bytes = 0
@@ -62,8 +64,11 @@ def serve(lib, sessions: List[dict], clips: List[list], hbm_budget_bytes: int, m
                 if pkt is not None:
                     i = inv[s]
                     lat.append(t - push_t[i][len(packets[i])])
+                    if not packets[i]:
+                        first_pkt[i] = t - t0 - sessions[i]["arrival_s"]
                     packets[i].append(pkt)
             st = srv.stats()
+            step_log.append((t - t0, sum(1 for o in out if o[2] is not None), st["active"], st["waiting"]))
             peak_active = max(peak_active, st["active"])
             peak_bytes = max(peak_bytes, st["bytes_in_use"])
             for i, s in sid.items():
@@ -76,7 +81,9 @@ def serve(lib, sessions: List[dict], clips: List[list], hbm_budget_bytes: int, m
                 time.sleep(max(0.0, sessions[nxt]["arrival_s"] - (time.perf_counter() - t0)))
         makespan = time.perf_counter() - t0
         budget = srv.stats()["bytes_budget"]
+        timing = srv.timing()
     finally:
         srv.close()
     return dict(packets=packets, latencies=lat, makespan=makespan, steps=steps, peak_active=peak_active,
-                peak_bytes=peak_bytes, budget=budget, frames=sum(len(p) for p in packets))
+                peak_bytes=peak_bytes, budget=budget, frames=sum(len(p) for p in packets), timing=timing,
+                first_packet_s=first_pkt, step_log=step_log)

@@ -6,6 +6,11 @@ reference encoder's length-prefixed packets and the final reconstruction.
 bench.py and the GPU tests compare against these digests.  Run from the
 repository root (needs oracle/_ref; spawns one process per core):
     python tests/golden/make_mixed_golden.py [n_served]
+    python tests/golden/make_mixed_golden.py --served-sample STOP STEP
+The second form adds, to the existing file, the digests of a seeded sample
+of the served schedule (sessions 0, STEP, 2 STEP, ... below STOP; key
+"served_sample", by session index), which bench.py --served-sessions uses to
+check a long served run without a reference run of every session.
 """
 import hashlib
 import json
@@ -55,8 +60,27 @@ def _work(item):
     return kind, idx, dict(spec, digest=d, recon=r, bytes=n)
 
 
+def served_sample(stop, step):
+    from tcodec_b200 import synth
+    path = os.path.join(HERE, "mixed_streams.json")
+    out = json.load(open(path))
+    sessions = synth.served_sessions()
+    items = [("served_sample", j, sessions[j]) for j in range(0, stop, step)]
+    items.sort(key=lambda it: -it[2]["w"] * it[2]["h"] * it[2]["frames"])
+    sample = {}
+    with mp.get_context("spawn").Pool(os.cpu_count()) as pool:
+        for _, idx, rec in pool.imap_unordered(_work, items):
+            sample[str(idx)] = rec
+            print("served_sample", idx, rec["w"], rec["h"], rec["frames"], flush=True)
+    out["served_sample"] = {k: sample[k] for k in sorted(sample, key=int)}
+    json.dump(out, open(path, "w"), indent=0)
+
+
 def main():
     from tcodec_b200 import synth
+    if len(sys.argv) > 1 and sys.argv[1] == "--served-sample":
+        served_sample(int(sys.argv[2]), int(sys.argv[3]))
+        return
     n_served = int(sys.argv[1]) if len(sys.argv) > 1 else 64
     items = [("batch", i, s) for i, s in enumerate(synth.mixed_streams())]
     items += [("served", j, s) for j, s in enumerate(synth.served_sessions()[:n_served])]
