@@ -174,6 +174,9 @@ __device__ __forceinline__ int lg2i(int v) { return 31 - __clz(v); }
 //   blk == 16  64 words: warps 0-1 take candidates 0, 2, 4, 6 and warps 2-3
 //              candidates 1, 3, 5, one word of each per thread;
 //   blk == 8   16 words: each half warp takes one candidate (k = gt >> 4).
+// BIG: only blocks of 32x32 and up reach this copy (the small-block shapes
+// are left out of its code).
+template <bool BIG = false>
 __device__ __forceinline__ void group_int_sads(Smem &S, int g, int gt, int &par, const uint8_t *ref, int s, int W, int H,
                                const uint8_t *cur, int blk, int pat, int p0, int K, int bx, int by, int scale,
                                int sad[7]) {
@@ -181,7 +184,7 @@ __device__ __forceinline__ void group_int_sads(Smem &S, int g, int gt, int &par,
     const int wig = gt >> 5, lane = gt & 31;
     if (gt == 0) OPCOUNT(0, K * blk * blk);
     int *part = S.me[g].part[par];
-    if (blk >= 32) {
+    if (BIG || blk >= 32) {
         int cx[7], cy[7];
         bool in[7];
 #pragma unroll
@@ -246,7 +249,7 @@ __device__ __forceinline__ void group_int_sads(Smem &S, int g, int gt, int &par,
     for (int k = 0; k < 7; ++k) {
         if (k < K) {
             int sum;
-            if (blk >= 32) sum = part[k] + part[8 + k] + part[16 + k] + part[24 + k];
+            if (BIG || blk >= 32) sum = part[k] + part[8 + k] + part[16 + k] + part[24 + k];
             else if (blk == 16) sum = part[((k & 1) * 2) * 8 + (k >> 1)] + part[((k & 1) * 2 + 1) * 8 + (k >> 1)];
             else sum = part[k];
             int dx, dy;
@@ -261,6 +264,7 @@ __device__ __forceinline__ void group_int_sads(Smem &S, int g, int gt, int &par,
 // One integer stage: `iters` passes over pattern points 1..npts, each point
 // taken relative to the running best (sequential commit, first improvement
 // wins; reference src/motion.c:398-448).
+template <bool BIG = false>
 __device__ void int_stage(Smem &S, int g, int gt, int &par, const uint8_t *ref, int s, int W, int H,
                           const uint8_t *cur, int blk, int pat, int npts, int iters, int scale,
                           int &bx, int &by, int &bsad) {
@@ -270,7 +274,7 @@ __device__ void int_stage(Smem &S, int g, int gt, int &par, const uint8_t *ref, 
         while (p0 <= npts) {
             const int K = npts - p0 + 1;
             int sad[7];
-            group_int_sads(S, g, gt, par, ref, s, W, H, cur, blk, pat, p0, K, bx, by, scale, sad);
+            group_int_sads<BIG>(S, g, gt, par, ref, s, W, H, cur, blk, pat, p0, K, bx, by, scale, sad);
             int found = -1, fs = 0;
 #pragma unroll
             for (int k = 0; k < 7; ++k)
@@ -281,6 +285,78 @@ __device__ void int_stage(Smem &S, int g, int gt, int &par, const uint8_t *ref, 
             bx += dx * scale; by += dy * scale; bsad = fs;
             improved = true;
             p0 = p0 + found + 1;
+        }
+        if (!improved) break;
+    }
+}
+
+// ---- small hexagon and diamond of blocks up to 16x16 from a SAD table ----
+// Both stages move the running best by at most 2 samples per commit, so
+// their candidates are looked up in a table of the 9 x 9 integer positions
+// around a window centre: one position per thread, one barrier per table,
+// instead of one barrier round per batch of candidates.  The table is
+// refilled around the running best when a candidate falls outside it; the
+// walk (order of candidates, first-improvement commits) is that of
+// int_stage, on the same SAD values.  Two tables alternate in the search's
+// prediction slot (past the quarter-sample anchors), so refilling one never
+// races with a lagging thread still reading the other.
+constexpr int WIN_R = 4, WIN_N = 2 * WIN_R + 1, WIN_OFF = 2560;
+static_assert(WIN_OFF + 2 * WIN_N * WIN_N * 4 <= 64 * 64, "SAD tables overflow the 4 KB slot");
+
+template <int B>
+__device__ void fill_sad_window(Smem &S, int g, int gt, int buf, const uint8_t *ref, int s, int W, int H,
+                                const uint8_t *cur, int wx, int wy) {
+    int *tab = (int *)(S.pred[g] + WIN_OFF) + buf * WIN_N * WIN_N;
+    if (gt == 0) OPCOUNT(0, WIN_N * WIN_N * B * B);
+    if (gt < WIN_N * WIN_N) {
+        const int x = wx + gt % WIN_N - WIN_R, y = wy + gt / WIN_N - WIN_R;
+        int v = 0x7FFFFFFF;
+        if (x >= 0 && y >= 0 && x + B <= W && y + B <= H) {
+            int acc = 0;
+#pragma unroll 2
+            for (int r = 0; r < B; ++r)
+#pragma unroll
+                for (int c = 0; c < B / 4; ++c)
+                    acc += (int)__vsadu4(ld4u(ref + (size_t)(y + r) * s + x + 4 * c),
+                                         *(const uint32_t *)(cur + r * 64 + 4 * c));
+            v = acc;
+        }
+        tab[gt] = v;
+    }
+    group_bar(g);
+}
+
+struct SadWindow {
+    int wx = 0, wy = 0, buf = 0;
+    bool valid = false;
+};
+
+__device__ void int_stage_windowed(Smem &S, int g, int gt, const uint8_t *ref, int s, int W, int H,
+                                   const uint8_t *cur, int blk, int pat, int npts, int iters, SadWindow &win,
+                                   int &bx, int &by, int &bsad) {
+    for (int it = 0; it < iters; ++it) {
+        bool improved = false;
+        int p0 = 1;
+        while (p0 <= npts) {
+            int found = -1, fs = 0, fx = 0, fy = 0;
+            for (int p = p0; p <= npts; ++p) {
+                int dx, dy;
+                pat_point(pat, p, dx, dy);
+                const int x = bx + dx, y = by + dy;
+                if (!win.valid || x < win.wx - WIN_R || x > win.wx + WIN_R || y < win.wy - WIN_R ||
+                    y > win.wy + WIN_R) {
+                    win.buf ^= 1; win.wx = bx; win.wy = by; win.valid = true;
+                    if (blk == 16) fill_sad_window<16>(S, g, gt, win.buf, ref, s, W, H, cur, win.wx, win.wy);
+                    else fill_sad_window<8>(S, g, gt, win.buf, ref, s, W, H, cur, win.wx, win.wy);
+                }
+                const int *tab = (const int *)(S.pred[g] + WIN_OFF) + win.buf * WIN_N * WIN_N;
+                const int v = tab[(y - win.wy + WIN_R) * WIN_N + (x - win.wx + WIN_R)];
+                if (v < bsad) { found = p; fs = v; fx = dx; fy = dy; break; }
+            }
+            if (found < 0) break;
+            bx += fx; by += fy; bsad = fs;
+            improved = true;
+            p0 = found + 1;
         }
         if (!improved) break;
     }
@@ -403,6 +479,22 @@ struct QpelAnchors {
 // Quarter-pel refinement of a B x B block (B <= 16) from anchors: the eight
 // points of reference src/motion.c:450-481 with their first-improvement
 // commits, one group barrier per point.
+// Quarter-pel refinement straight from the reference frame, for searches
+// whose points may leave the six-tap margins or for blocks above 16x16
+// (out of line: most small-block searches never run it).
+__device__ __noinline__ void qpel_refine_direct(int g, int gt, int &par, const uint8_t *ref, int s, int W, int H,
+                                                const uint8_t *cur, int blk, int &mx, int &my, int &bsad) {
+    Smem &S = smem_state();
+    for (int p = 1; p < 9; ++p) {
+        const int qx = mx + c_qpel[p][0], qy = my + c_qpel[p][1];
+        const int fx = qx >> 2, fy = qy >> 2;
+        if (fx < 0 || fy < 0 || fx + blk + 1 > W || fy + blk + 1 > H) continue;
+        const bool six = fx >= 2 && fy >= 2 && fx + blk + 2 < W && fy + blk + 2 < H;
+        const int sum = group_subpel_sad(S, g, gt, par, ref, s, cur, blk, qx, qy, six);
+        if (sum < bsad) { bsad = sum; mx = qx; my = qy; }
+    }
+}
+
 template <int B>
 __device__ void qpel_refine_anchored(Smem &S, int g, int gt, int &par, const uint8_t *ref, int s,
                                      const uint8_t *cur, int bx, int by, int &mx, int &my, int &bsad) {
@@ -439,10 +531,17 @@ __device__ __noinline__ void me_run(Smem &, int g, int gt, const uint8_t *ref, i
     const int scale = maxi(1, sr / 4);
     // large hexagon (6 points, 2 passes, scaled), small hexagon (6, 3),
     // diamond (4, 4); a loop rather than three inlined copies of the stage
-#pragma unroll 1
-    for (int st = 0; st < 3; ++st)
-        int_stage(S, g, gt, par, ref, s, W, H, cur, blk, st, st == 2 ? 4 : 6, st + 2, st == 0 ? scale : 1, bx, by,
-                  bsad);
+    // large hexagon (6 points, 2 passes, scaled), then small hexagon (6, 3)
+    // and diamond (4, 4), the last two from SAD tables for blocks up to 16x16
+    int_stage(S, g, gt, par, ref, s, W, H, cur, blk, 0, 6, 2, scale, bx, by, bsad);
+    if (blk <= 16) {
+        SadWindow win;
+        int_stage_windowed(S, g, gt, ref, s, W, H, cur, blk, 1, 6, 3, win, bx, by, bsad);
+        int_stage_windowed(S, g, gt, ref, s, W, H, cur, blk, 2, 4, 4, win, bx, by, bsad);
+    } else {
+        int_stage<true>(S, g, gt, par, ref, s, W, H, cur, blk, 1, 6, 3, 1, bx, by, bsad);
+        int_stage<true>(S, g, gt, par, ref, s, W, H, cur, blk, 2, 4, 4, 1, bx, by, bsad);
+    }
     ME_MARK(11);
     // Quarter-pel refinement around the running best, first improvement
     // commits (reference src/motion.c:450-481).
@@ -453,14 +552,7 @@ __device__ __noinline__ void me_run(Smem &, int g, int gt, const uint8_t *ref, i
     } else if (inner && blk == 8) {
         qpel_refine_anchored<8>(S, g, gt, par, ref, s, cur, bx, by, mx, my, bsad);
     } else {
-        for (int p = 1; p < 9; ++p) {
-            const int qx = mx + c_qpel[p][0], qy = my + c_qpel[p][1];
-            const int fx = qx >> 2, fy = qy >> 2;
-            if (fx < 0 || fy < 0 || fx + blk + 1 > W || fy + blk + 1 > H) continue;
-            const bool six = fx >= 2 && fy >= 2 && fx + blk + 2 < W && fy + blk + 2 < H;
-            const int sum = group_subpel_sad(S, g, gt, par, ref, s, cur, blk, qx, qy, six);
-            if (sum < bsad) { bsad = sum; mx = qx; my = qy; }
-        }
+        qpel_refine_direct(g, gt, par, ref, s, W, H, cur, blk, mx, my, bsad);
     }
     ME_MARK(12);
     if (gt == 0) { S.me[g].mvx = mx; S.me[g].mvy = my; S.me[g].best = bsad; }
@@ -508,21 +600,23 @@ __device__ __noinline__ void build_refs(Smem &, const Leaf L, uint32_t mode_mask
         sum = __reduce_add_sync(0xffffffffu, sum);
         if (threadIdx.x == 0) { S.dc = (sum + N) / (2 * N); S.ipred_ok = fill; }
     } else if (fill) {
-        const int lg = __ffs(N) - 1, npx = N * N;
-        if ((fill & (fill - 1)) == 0) {
-            const int m = __ffs(fill) - 1;
-            for (int p = threadIdx.x - 32; p < npx; p += NT - 32)
-                S.ipred[m][p] = (uint8_t)intra_at(S.ra + 1, S.rl + 1, N, m, 0, p & (N - 1), p >> lg);
-        } else {
-            for (int i = threadIdx.x - 32; i < 18 * npx; i += NT - 32) {
-                const int m = i >> (2 * lg), p = i & (npx - 1);
-                if ((fill >> m) & 1)
-                    S.ipred[m][p] = (uint8_t)intra_at(S.ra + 1, S.rl + 1, N, m, 0, p & (N - 1), p >> lg);
-            }
+        // the nm modes of `fill`, N*N samples each: sample i belongs to the
+        // (i >> 2lg)-th set bit of fill
+        const int lg = __ffs(N) - 1, npx = N * N, nm = __popc(fill);
+        for (int i = threadIdx.x - 32; i < nm * npx; i += NT - 32) {
+            const int m = __fns(fill, 0, (i >> (2 * lg)) + 1), p = i & (npx - 1);
+            S.ipred[m][p] = (uint8_t)intra_at(S.ra + 1, S.rl + 1, N, m, 0, p & (N - 1), p >> lg);
         }
     }
     SYNC();
     PROBE(63);
+}
+
+// An intra sample the leaf's prediction cache does not hold (leaves above
+// IPRED_MAX): out of line, so the residual jobs' hot loops stay small.
+__device__ __noinline__ int intra_sample(int cu, int m, int dc, int x, int y) {
+    const Smem &S = smem_state();
+    return intra_at(S.ra + 1, S.rl + 1, cu, m, dc, x, y);
 }
 
 __device__ __forceinline__ int lpred(const Smem &S, int cu, int slot, int dc, int x, int y) {
@@ -530,7 +624,7 @@ __device__ __forceinline__ int lpred(const Smem &S, int cu, int slot, int dc, in
     const int m = slot - K_INTRA;
     if (m == 1) return dc;
     if (m < 18 && ((S.ipred_ok >> m) & 1u)) return S.ipred[m][y * cu + x];
-    return intra_at(S.ra + 1, S.rl + 1, cu, m, dc, x, y);
+    return intra_sample(cu, m, dc, x, y);
 }
 
 // Luma residual jobs, 8x8 TUs: one octet per (candidate, TU).

@@ -30,9 +30,11 @@ def serve(lib, sessions: List[dict], clips: List[list], hbm_budget_bytes: int, m
     inv: Dict[int, int] = {}
     fed = [0] * n
     push_t: List[List[float]] = [[] for _ in range(n)]
+    push_active: List[List[bool]] = [[] for _ in range(n)]   # session admitted when the frame was pushed
     packets: List[List[bytes]] = [[] for _ in range(n)]
     done = [False] * n
     lat: List[float] = []
+    lat_admitted: List[float] = []          # frames pushed after their session was admitted
     first_pkt: List[float] = [0.0] * n      # arrival -> first packet of each session (s)
     step_log: List[tuple] = []              # (end of step s, packets, active, waiting)
     steps = 0
@@ -50,8 +52,10 @@ def serve(lib, sessions: List[dict], clips: List[list], hbm_budget_bytes: int, m
             for i, s in sid.items():
                 if done[i]:
                     continue
+                active = srv.state(s) == api.SESSION_ACTIVE
                 while fed[i] < len(clips[i]) and srv.push(s, clips[i][fed[i]]):
                     push_t[i].append(time.perf_counter())
+                    push_active[i].append(active)
                     fed[i] += 1
                     if fed[i] == len(clips[i]):
                         srv.finish(s)
@@ -63,7 +67,10 @@ def serve(lib, sessions: List[dict], clips: List[list], hbm_budget_bytes: int, m
                     raise RuntimeError(f"session {inv[s]} failed: {status}")
                 if pkt is not None:
                     i = inv[s]
-                    lat.append(t - push_t[i][len(packets[i])])
+                    k = len(packets[i])
+                    lat.append(t - push_t[i][k])
+                    if push_active[i][k]:
+                        lat_admitted.append(t - push_t[i][k])
                     if not packets[i]:
                         first_pkt[i] = t - t0 - sessions[i]["arrival_s"]
                     packets[i].append(pkt)
@@ -86,4 +93,5 @@ def serve(lib, sessions: List[dict], clips: List[list], hbm_budget_bytes: int, m
         srv.close()
     return dict(packets=packets, latencies=lat, makespan=makespan, steps=steps, peak_active=peak_active,
                 peak_bytes=peak_bytes, budget=budget, frames=sum(len(p) for p in packets), timing=timing,
+                latencies_admitted=lat_admitted,
                 first_packet_s=first_pkt, step_log=step_log)
