@@ -264,21 +264,27 @@ __device__ __forceinline__ void group_int_sads(Smem &S, int g, int gt, int &par,
 // One integer stage: `iters` passes over pattern points 1..npts, each point
 // taken relative to the running best (sequential commit, first improvement
 // wins; reference src/motion.c:398-448).
+// with_center: the stage's first batch also takes pattern point 0 (the
+// centre itself, (0, 0) in every pattern), whose SAD becomes the starting
+// bsad, as the search's initial SAD at the centre would (one barrier round
+// fewer per search).
 template <bool BIG = false>
 __device__ void int_stage(Smem &S, int g, int gt, int &par, const uint8_t *ref, int s, int W, int H,
                           const uint8_t *cur, int blk, int pat, int npts, int iters, int scale,
-                          int &bx, int &by, int &bsad) {
+                          int &bx, int &by, int &bsad, bool with_center = false) {
     for (int it = 0; it < iters; ++it) {
         bool improved = false;
-        int p0 = 1;
+        int p0 = with_center ? 0 : 1;
         while (p0 <= npts) {
             const int K = npts - p0 + 1;
             int sad[7];
             group_int_sads<BIG>(S, g, gt, par, ref, s, W, H, cur, blk, pat, p0, K, bx, by, scale, sad);
             int found = -1, fs = 0;
+            const int k0 = p0 == 0 ? 1 : 0;
+            if (p0 == 0) { bsad = sad[0]; with_center = false; }
 #pragma unroll
             for (int k = 0; k < 7; ++k)
-                if (found < 0 && k < K && sad[k] < bsad) { found = k; fs = sad[k]; }
+                if (found < 0 && k >= k0 && k < K && sad[k] < bsad) { found = k; fs = sad[k]; }
             if (found < 0) break;
             int dx, dy;
             pat_point(pat, p0 + found, dx, dy);
@@ -525,15 +531,13 @@ __device__ __noinline__ void me_run(Smem &, int g, int gt, const uint8_t *ref, i
     const uint8_t *cur = S.cur_y + ly * 64 + lx;
     int par = 0;
     int bx = clampi(center_x, 0, W - blk), by = clampi(center_y, 0, H - blk);
-    int sad[7];
-    group_int_sads(S, g, gt, par, ref, s, W, H, cur, blk, 3, 0, 1, bx, by, 1, sad);
-    int bsad = sad[0];
+    int bsad = 0;                       // set from the centre by the first batch below
     const int scale = maxi(1, sr / 4);
     // large hexagon (6 points, 2 passes, scaled), small hexagon (6, 3),
     // diamond (4, 4); a loop rather than three inlined copies of the stage
     // large hexagon (6 points, 2 passes, scaled), then small hexagon (6, 3)
     // and diamond (4, 4), the last two from SAD tables for blocks up to 16x16
-    int_stage(S, g, gt, par, ref, s, W, H, cur, blk, 0, 6, 2, scale, bx, by, bsad);
+    int_stage(S, g, gt, par, ref, s, W, H, cur, blk, 0, 6, 2, scale, bx, by, bsad, true);
     if (blk <= 16) {
         SadWindow win;
         int_stage_windowed(S, g, gt, ref, s, W, H, cur, blk, 1, 6, 3, win, bx, by, bsad);
@@ -598,7 +602,7 @@ __device__ __noinline__ void build_refs(Smem &, const Leaf L, uint32_t mode_mask
         int sum = 0;
         for (int i = threadIdx.x; i < N; i += 32) sum += S.ra[i + 2] + S.rl[i + 2];
         sum = __reduce_add_sync(0xffffffffu, sum);
-        if (threadIdx.x == 0) { S.dc = (sum + N) / (2 * N); S.ipred_ok = fill; }
+        if (threadIdx.x == 0) { S.dc = (sum + N) / (2 * N); S.dc_u8 = (uint8_t)S.dc; S.ipred_ok = fill; }
     } else if (fill) {
         // the nm modes of `fill`, N*N samples each: sample i belongs to the
         // (i >> 2lg)-th set bit of fill
@@ -617,6 +621,23 @@ __device__ __noinline__ void build_refs(Smem &, const Leaf L, uint32_t mode_mask
 __device__ __noinline__ int intra_sample(int cu, int m, int dc, int x, int y) {
     const Smem &S = smem_state();
     return intra_at(S.ra + 1, S.rl + 1, cu, m, dc, x, y);
+}
+
+// Where a candidate's luma prediction comes from: sample (x, y) of a cu x cu
+// leaf is src[(y * cu + x) & mask] (an inter prediction slot or a cached
+// intra mode; the DC mode is a one-byte source under mask 0), or src is null
+// for an intra mode the leaf's cache does not hold (intra_sample).  Resolved
+// once per residual job, so the job's sample loops are plain loads.
+struct PredSrc {
+    const uint8_t *src;
+    int mask;
+};
+__device__ __forceinline__ PredSrc pred_src(const Smem &S, int slot) {
+    if (slot < NPRED) return {S.pred[slot], 0xFFFF};
+    const int m = slot - K_INTRA;
+    if (m == 1) return {&S.dc_u8, 0};
+    if (m < 18 && ((S.ipred_ok >> m) & 1u)) return {S.ipred[m], 0xFFFF};
+    return {nullptr, 0};
 }
 
 __device__ __forceinline__ int lpred(const Smem &S, int cu, int slot, int dc, int x, int y) {
@@ -645,23 +666,36 @@ __device__ __noinline__ void luma_jobs8(Smem &, const Leaf L, const int *cl, int
         const int jj = act ? j : 0;
         const int k = jj / ntu2, t = jj - k * ntu2, ty = t / ntu, tx = t - ty * ntu;
         const int slot = cl[k];
-        int res[8];
+        const PredSrc ps = pred_src(S, slot);
+        int res[8], pr[8];
         const int r = ty * 8 + l8;
+        if (ps.src) {
 #pragma unroll
-        for (int n = 0; n < 8; ++n) {
-            const int x = tx * 8 + n;
-            res[n] = clampi((int)S.cur_y[(L.ly + r) * 64 + L.lx + x] - lpred(S, cu, slot, dc, x, r), -512, 511);
+            for (int n = 0; n < 8; ++n) pr[n] = ps.src[(r * cu + tx * 8 + n) & ps.mask];
+        } else {
+#pragma unroll
+            for (int n = 0; n < 8; ++n) pr[n] = intra_sample(cu, slot - K_INTRA, dc, tx * 8 + n, r);
         }
+#pragma unroll
+        for (int n = 0; n < 8; ++n)
+            res[n] = clampi((int)S.cur_y[(L.ly + r) * 64 + L.lx + tx * 8 + n] - pr[n], -512, 511);
         int qc[8], rc[8];
         PROBE(60);
         const int bits = tu8_code(l8, res, scr, qp, qc, rc);
         PROBE(61);
         int sse = 0;
         const int x = tx * 8 + l8;
+        if (ps.src) {
+#pragma unroll
+            for (int kk = 0; kk < 8; ++kk) pr[kk] = ps.src[((ty * 8 + kk) * cu + x) & ps.mask];
+        } else {
+#pragma unroll
+            for (int kk = 0; kk < 8; ++kk) pr[kk] = intra_sample(cu, slot - K_INTRA, dc, x, ty * 8 + kk);
+        }
 #pragma unroll
         for (int kk = 0; kk < 8; ++kk) {
             const int y = ty * 8 + kk;
-            const int v = clampi(lpred(S, cu, slot, dc, x, y) + rc[kk], 0, 255);
+            const int v = clampi(pr[kk] + rc[kk], 0, 255);
             const int d = (int)S.cur_y[(L.ly + y) * 64 + L.lx + x] - v;
             sse += d * d;
             if (act && wrec) RY(S, L.lx + x, L.ly + y) = (uint8_t)v;
@@ -698,21 +732,34 @@ __device__ __noinline__ void luma_jobs4(Smem &, const Leaf L, const int *cl, int
         const int ty = t / ntu, tx = t - ty * ntu;
         const int sx = tx * 8 + (q & 1) * 4, sy = ty * 8 + (q & 2) * 2;
         const int slot = cl[k];
-        int res[4];
+        const PredSrc ps = pred_src(S, slot);
+        int res[4], pr[4];
+        if (ps.src) {
 #pragma unroll
-        for (int n = 0; n < 4; ++n) {
-            const int x = sx + n, y = sy + l4;
-            res[n] = clampi((int)S.cur_y[(L.ly + y) * 64 + L.lx + x] - lpred(S, cu, slot, dc, x, y), -512, 511);
+            for (int n = 0; n < 4; ++n) pr[n] = ps.src[((sy + l4) * cu + sx + n) & ps.mask];
+        } else {
+#pragma unroll
+            for (int n = 0; n < 4; ++n) pr[n] = intra_sample(cu, slot - K_INTRA, dc, sx + n, sy + l4);
         }
+#pragma unroll
+        for (int n = 0; n < 4; ++n)
+            res[n] = clampi((int)S.cur_y[(L.ly + sy + l4) * 64 + L.lx + sx + n] - pr[n], -512, 511);
         int qc[4], rc[4];
         int bits = tu4_code(l4, res, scr, qp, qc, rc);
         if (q == 0) bits += 1;
         int sse = 0;
         const int x = sx + l4;
+        if (ps.src) {
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) pr[kk] = ps.src[((sy + kk) * cu + x) & ps.mask];
+        } else {
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) pr[kk] = intra_sample(cu, slot - K_INTRA, dc, x, sy + kk);
+        }
 #pragma unroll
         for (int kk = 0; kk < 4; ++kk) {
             const int y = sy + kk;
-            const int v = clampi(lpred(S, cu, slot, dc, x, y) + rc[kk], 0, 255);
+            const int v = clampi(pr[kk] + rc[kk], 0, 255);
             const int d = (int)S.cur_y[(L.ly + y) * 64 + L.lx + x] - v;
             sse += d * d;
             if (act && wrec) RY(S, L.lx + x, L.ly + y) = (uint8_t)v;

@@ -74,6 +74,7 @@ struct Smem {
     int cl2[8];                // 8x8-only candidates (merges)
     int cand_mvx[NPRED], cand_mvy[NPRED], cand_ref[NPRED], cand_ref2[NPRED];
     int ncl, dc, flag;
+    uint8_t dc_u8;             // S.dc as a one-byte prediction source (PredSrc)
     long long best_cost;
     int sao[3];
     int band_sum[32], band_cnt[32], band_sq[32], band_new[32];
