@@ -544,6 +544,12 @@ def run_b200(args, rank, world):
     clip = make_clip(S + Wm + K)
     dplanes = [tuple(torch.from_numpy(np.ascontiguousarray(p)).to(dev) for p in f) for f in clip]
     torch.cuda.synchronize()
+    tuned = None
+    if not args.no_tune:
+        # the engine's knobs for this frame size, timed on this workload's own
+        # frames (one GOP per combination after the key frame and first GOP)
+        from tcodec_b200 import tuning
+        tuned = tuning.describe(tuning.tune_engine(lib, make_cfg(lib), clip, streams=S, steps=4, warmup=5))
 
     def timed(stream_ptr, fn_step, after_warmup=None, finish=None):
         # finish (pipelined batches): the packets still pending after the
@@ -655,7 +661,7 @@ def run_b200(args, rank, world):
         dev_run = batch_pass(True)
     e2e_run = batch_pass(False)
     plain = plain_pass() if not args.no_plain else None
-    return dev_run, e2e_run, plain, clocks.summary()
+    return dev_run, e2e_run, plain, clocks.summary(), tuned
 
 
 def check_bit_exact(dev_run, e2e_run, args):
@@ -729,6 +735,9 @@ def main():
                     help="only the served form over --served-sessions sessions of the Poisson schedule, with its "
                          "sampled bit-exact check (one JSON line)")
     ap.add_argument("--no-kernels", action="store_true", help="skip the standalone-kernel roofline section")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the engine's default knobs instead of timing every combination first "
+                         "(tcodec_b200.tuning)")
     ap.add_argument("--no-pipeline", action="store_true",
                     help="unpipelined batch steps (default: each call entropy-codes the previous call's frames "
                          "during its own device step)")
@@ -807,7 +816,7 @@ def main():
         torch.cuda.set_device(local)
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    dev_run, e2e_run, plain, clocks = run_b200(args, rank, world)
+    dev_run, e2e_run, plain, clocks, tuned = run_b200(args, rank, world)
     # Bit-exactness against the reference's committed answers for this
     # workload, on every rank (each rank encodes the same streams), both
     # runs (device-resident and host inputs).
@@ -902,6 +911,8 @@ def main():
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(import_rec),
                 "d2h_bytes_per_step": int(rec_bytes + e2e_run["bytes"] / max(1, args.steps))},
         "gpu_launches": int(dev_run["launches"]),
+        "engine_tuning": tuned if tuned else {"search_window": 4, "queue_order": "diagonal",
+                                              "what": "defaults (--no-tune)"},
         "clocks": clocks,
     }
     if forms:

@@ -334,6 +334,30 @@ int tcb_autotune_threads(int kernel, int width, int height);
 /* Record a choice directly (a table saved from an earlier tuning run):
  * threads must be a variant of the kernel, 0 removes the entry. */
 tc_error_t tcb_autotune_set_threads(int kernel, int width, int height, int threads);
+
+/* Engine knobs per frame size (no reference counterpart).  Neither changes
+ * any output; both change how long a step takes, which depends on the frame
+ * size and the content, so they are measured (tcodec_b200.tuning times every
+ * combination on the caller's frames) rather than fixed:
+ *   search_window  radius R (2..5) of the motion search's SAD tables: the
+ *                  small-hexagon and diamond stages of blocks up to 16x16
+ *                  read their candidates from (2R+1)^2 positions computed in
+ *                  one pass; larger R costs more per table and refills less;
+ *   queue_order    how a batch step merges its streams' CTU wavefronts:
+ *                  TCB_QUEUE_DIAGONAL takes every stream's anti-diagonal d
+ *                  before any stream's d+1; TCB_QUEUE_STAGGERED starts
+ *                  stream s s diagonals later, so the streams' short first
+ *                  and last diagonals do not all fall together.  A batch
+ *                  uses the order tuned for its largest frame size.
+ * Defaults (nothing set, or set back with 0, 0): R = 4, diagonal order.
+ * The setting applies to frames planned afterwards by any encoder, batch or
+ * server in the process, and to tcb_ctu_encode_frame(_static). */
+#define TCB_SEARCH_WINDOW_MIN 2
+#define TCB_SEARCH_WINDOW_MAX 5
+#define TCB_QUEUE_DIAGONAL 0
+#define TCB_QUEUE_STAGGERED 1
+tc_error_t tcb_engine_set_tuning(int width, int height, int search_window, int queue_order);
+tc_error_t tcb_engine_get_tuning(int width, int height, int *search_window, int *queue_order);
 /* Bounded waits of the frame kernels that gave up since the last call
  * (a staged tile that never arrived; the CTU is then left unfiltered).
  * 0 in a healthy run; reading resets.  Synchronises the device. */

@@ -21,6 +21,8 @@ TC_OK, TC_ERR_MEMORY, TC_ERR_PARAM, TC_ERR_BITSTREAM, TC_ERR_EOF, TC_ERR_INTERNA
     0, -1, -2, -3, -4, -5, -6)
 PRESET_ULTRAFAST, PRESET_FAST, PRESET_MEDIUM, PRESET_SLOW = 0, 1, 2, 3
 KERNEL_DEBLOCK, KERNEL_SAO, KERNEL_MC = 0, 1, 2   # tcb_autotune_* kernel ids
+QUEUE_DIAGONAL, QUEUE_STAGGERED = 0, 1            # tcb_engine_set_tuning queue orders
+SEARCH_WINDOW_MIN, SEARCH_WINDOW_MAX = 2, 5
 STAGING_TMA = 0x10000                             # TCB_STAGING_TMA: deblocking tiles staged by TMA
 
 
@@ -371,6 +373,10 @@ def bind_b200(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.tcb_autotune_threads.restype = ctypes.c_int
     lib.tcb_autotune_set_threads.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.tcb_autotune_set_threads.restype = ctypes.c_int
+    lib.tcb_engine_set_tuning.argtypes = [ctypes.c_int] * 4
+    lib.tcb_engine_set_tuning.restype = ctypes.c_int
+    lib.tcb_engine_get_tuning.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    lib.tcb_engine_get_tuning.restype = ctypes.c_int
     lib.tcb_frame_kernels_errors.argtypes = []
     lib.tcb_frame_kernels_errors.restype = ctypes.c_uint
     return lib
@@ -621,3 +627,19 @@ class Server:
                                   ctypes.byref(cap))
         return dict(waiting=w.value, active=a.value, retired=d.value, bytes_in_use=used.value,
                     bytes_budget=cap.value)
+
+
+def engine_tuning(lib: ctypes.CDLL, width: int, height: int) -> Tuple[int, int]:
+    """(search_window, queue_order) the engine uses for this frame size."""
+    w, q = ctypes.c_int(), ctypes.c_int()
+    r = lib.tcb_engine_get_tuning(width, height, ctypes.byref(w), ctypes.byref(q))
+    if r != TC_OK:
+        raise RuntimeError(f"tcb_engine_get_tuning -> {r}")
+    return w.value, q.value
+
+
+def set_engine_tuning(lib: ctypes.CDLL, width: int, height: int, search_window: int, queue_order: int) -> None:
+    """tcb_engine_set_tuning; (0, 0) restores the defaults."""
+    r = lib.tcb_engine_set_tuning(width, height, search_window, queue_order)
+    if r != TC_OK:
+        raise RuntimeError(f"tcb_engine_set_tuning({width}, {height}, {search_window}, {queue_order}) -> {r}")

@@ -96,6 +96,24 @@ void set_tuned_threads(int kernel, int width, int height, int threads) {
     else g_tuned.erase({kernel, width, height});
 }
 
+// Engine knobs per frame size (tcb_engine_set_tuning): neither changes any
+// output, only the time a step takes.
+namespace {
+std::map<std::pair<int, int>, EngineTuning> g_engine;
+}
+
+EngineTuning engine_tuning(int width, int height) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_engine.find({width, height});
+    return it == g_engine.end() ? EngineTuning{} : it->second;
+}
+
+void set_engine_tuning(int width, int height, const EngineTuning *t) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (t) g_engine[{width, height}] = *t;
+    else g_engine.erase({width, height});
+}
+
 }  // namespace tcb
 
 extern "C" {
@@ -179,6 +197,28 @@ tc_error_t tcb_autotune_set_threads(int kernel, int width, int height, int threa
     if (kernel < TCB_KERNEL_DEBLOCK || kernel > TCB_KERNEL_MC || width <= 0 || height <= 0 || !ok)
         return TC_ERR_PARAM;
     tcb::set_tuned_threads(kernel, width, height, threads);
+    return TC_OK;
+}
+
+tc_error_t tcb_engine_set_tuning(int width, int height, int search_window, int queue_order) {
+    if (width <= 0 || height <= 0) return TC_ERR_PARAM;
+    if (search_window == 0 && queue_order == 0) {        // back to the defaults
+        tcb::set_engine_tuning(width, height, nullptr);
+        return TC_OK;
+    }
+    if (search_window < TCB_SEARCH_WINDOW_MIN || search_window > TCB_SEARCH_WINDOW_MAX ||
+        (queue_order != TCB_QUEUE_DIAGONAL && queue_order != TCB_QUEUE_STAGGERED))
+        return TC_ERR_PARAM;
+    const tcb::EngineTuning t{search_window, queue_order};
+    tcb::set_engine_tuning(width, height, &t);
+    return TC_OK;
+}
+
+tc_error_t tcb_engine_get_tuning(int width, int height, int *search_window, int *queue_order) {
+    if (width <= 0 || height <= 0 || !search_window || !queue_order) return TC_ERR_PARAM;
+    const tcb::EngineTuning t = tcb::engine_tuning(width, height);
+    *search_window = t.search_window;
+    *queue_order = t.queue_order;
     return TC_OK;
 }
 

@@ -231,10 +231,10 @@ tc_error_t enqueue_step(tcb_batch *b, const std::vector<int> &part, const std::v
             return TC_ERR_INTERNAL;
         b->kernel_launches += 1;
     } else {
-        for (int d = 0; d < b->max_diag; ++d)
+        for (size_t d = 0; d < off.size(); ++d)
             if (cnt[d] && launch_ctu_items(b->d_params, b->d_items + off[d], cnt[d], b->st) != cudaSuccess)
                 return TC_ERR_INTERNAL;
-        for (int d = 0; d < b->max_diag; ++d) b->kernel_launches += cnt[d] ? 1 : 0;
+        for (size_t d = 0; d < off.size(); ++d) b->kernel_launches += cnt[d] ? 1 : 0;
     }
     if (b->timing && cudaEventRecordWithFlags(b->ev1, b->st, evf) != cudaSuccess) return TC_ERR_INTERNAL;
     for (int s : part) {
@@ -281,16 +281,33 @@ tc_error_t run_step(tcb_batch *b, const std::vector<int> &part, tc_packet_t *pkt
     for (int s : part) need_sync |= b->encs[s]->impl->pend.need_hist != 0;
     if (need_sync && cudaStreamSynchronize(b->st) != cudaSuccess) return TC_ERR_INTERNAL;
     // Merged anti-diagonal item lists of the participating streams (the
-    // queue order), staged in pinned memory.
-    std::vector<int> off(b->max_diag), cnt(b->max_diag);
+    // queue order), staged in pinned memory.  Merged slot m holds diagonal
+    // m - lag of every stream, where lag is 0 (TCB_QUEUE_DIAGONAL) or the
+    // stream's rank in the step (TCB_QUEUE_STAGGERED), as tuned for the
+    // step's largest frame size.  Either way each stream's diagonals stay in
+    // order and one slot never holds two CTUs of one stream, so every CTU's
+    // neighbours come earlier in the queue (the persistent wavefront's
+    // condition) and a slot's CTUs are independent.
+    int big = part[0];
+    for (int s : part) {
+        const EncImpl &e = *b->encs[s]->impl, &eb = *b->encs[big]->impl;
+        if ((long long)e.W * e.H > (long long)eb.W * eb.H) big = s;
+    }
+    const bool stagger =
+        engine_tuning(b->encs[big]->impl->W, b->encs[big]->impl->H).queue_order == TCB_QUEUE_STAGGERED;
+    int nslots = 0;
+    for (size_t r = 0; r < part.size(); ++r)
+        nslots = std::max(nslots, (stagger ? (int)r : 0) + (int)b->stream_diag[part[r]].size());
+    std::vector<int> off(nslots), cnt(nslots);
     b->h_items.clear();
-    for (int d = 0; d < b->max_diag; ++d) {
-        off[d] = (int)b->h_items.size();
-        for (int s : part) {
-            const auto &sd = b->stream_diag[s];
-            if (d < (int)sd.size()) b->h_items.insert(b->h_items.end(), sd[d].begin(), sd[d].end());
+    for (int m = 0; m < nslots; ++m) {
+        off[m] = (int)b->h_items.size();
+        for (size_t r = 0; r < part.size(); ++r) {
+            const auto &sd = b->stream_diag[part[r]];
+            const int d = m - (stagger ? (int)r : 0);
+            if (d >= 0 && d < (int)sd.size()) b->h_items.insert(b->h_items.end(), sd[d].begin(), sd[d].end());
         }
-        cnt[d] = (int)b->h_items.size() - off[d];
+        cnt[m] = (int)b->h_items.size() - off[m];
     }
     if (b->h_items.size() > b->items_cap) {
         cudaFree(b->d_items);

@@ -78,6 +78,7 @@ struct FrameParams {
     int32_t *err;                              // device error word
     int *done;                                 // per-CTU publish flags (persistent wavefront)
     int epoch;                                 // value this frame publishes in `done`
+    int search_window;                         // radius (2..5) of the search's SAD tables (engine tuning)
 };
 
 // ---------------------------------------------------------------------

@@ -375,6 +375,7 @@ tc_error_t EncImpl::stage_b() {
     P.err = d_err;
     P.done = d_done;
     P.epoch = ++epoch;
+    P.search_window = engine_tuning(W, H).search_window;
     *h_params_pin = P;   // the previous frame's upload has completed (every step ends synchronised)
     if (cudaMemcpyAsync(d_params, h_params_pin, sizeof(P), cudaMemcpyHostToDevice, st) != cudaSuccess)
         return TC_ERR_INTERNAL;
@@ -654,6 +655,7 @@ bool tcb::frame_params_from_desc(const tcb_frame_desc_t &d, FrameParams &P) {
         P.eff_l[b] = eff_scale(d.qp, b); P.rcp_l[b] = quant_rcp(P.eff_l[b]);
         P.eff_c[b] = eff_scale(P.qp_c, b); P.rcp_c[b] = quant_rcp(P.eff_c[b]);
     }
+    P.search_window = engine_tuning(d.width, d.height).search_window;
     return true;
 }
 

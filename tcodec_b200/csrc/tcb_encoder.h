@@ -25,6 +25,16 @@ struct DevFrame {
 long long tc_lambda_host(int qp);
 bool frame_params_from_desc(const tcb_frame_desc_t &d, FrameParams &P);
 
+// Engine knobs of one frame size (tcb_engine_set_tuning; defaults when
+// none were set): the search's SAD-table radius and the order in which a
+// batch step merges its streams' CTU wavefronts.
+struct EngineTuning {
+    int search_window = 4;
+    int queue_order = TCB_QUEUE_DIAGONAL;
+};
+EngineTuning engine_tuning(int width, int height);
+void set_engine_tuning(int width, int height, const EngineTuning *t);
+
 struct EncImpl {
     static constexpr int NPOOL = 6;   // 4 DPB slots + the frame being built + spare
     static constexpr size_t BF_MAX = 8;   // B-frame reorder buffers held at most

@@ -298,24 +298,31 @@ __device__ void int_stage(Smem &S, int g, int gt, int &par, const uint8_t *ref, 
 
 // ---- small hexagon and diamond of blocks up to 16x16 from a SAD table ----
 // Both stages move the running best by at most 2 samples per commit, so
-// their candidates are looked up in a table of the 9 x 9 integer positions
-// around a window centre: one position per thread, one barrier per table,
-// instead of one barrier round per batch of candidates.  The table is
-// refilled around the running best when a candidate falls outside it; the
-// walk (order of candidates, first-improvement commits) is that of
-// int_stage, on the same SAD values.  Two tables alternate in the search's
-// prediction slot (past the quarter-sample anchors), so refilling one never
-// races with a lagging thread still reading the other.
-constexpr int WIN_R = 4, WIN_N = 2 * WIN_R + 1, WIN_OFF = 2560;
-static_assert(WIN_OFF + 2 * WIN_N * WIN_N * 4 <= 64 * 64, "SAD tables overflow the 4 KB slot");
+// their candidates are looked up in a table of the (2R+1)^2 integer
+// positions around a window centre (R = FrameParams::search_window, 2..5,
+// chosen per frame size by the engine tuning; 4 by default): one position
+// per thread, one barrier per table, instead of one barrier round per batch
+// of candidates.  The table is refilled around the running best when a
+// candidate falls outside it (R >= 2 keeps every pattern point of the new
+// centre inside); the walk (order of candidates, first-improvement commits)
+// is that of int_stage, on the same SAD values, so R changes the speed and
+// never the result.  Two tables alternate in the search's prediction slot
+// (past the quarter-sample anchors), so refilling one never races with a
+// lagging thread still reading the other.
+constexpr int WIN_RMAX = 5, WIN_NMAX = 2 * WIN_RMAX + 1, WIN_OFF = 2560;
+static_assert(WIN_OFF + 2 * WIN_NMAX * WIN_NMAX * 4 <= 64 * 64, "SAD tables overflow the 4 KB slot");
+static_assert(WIN_NMAX * WIN_NMAX <= GT, "one table position per thread of the group");
+
+__device__ __forceinline__ int window_radius(int r) { return r >= 2 && r <= WIN_RMAX ? r : 4; }
 
 template <int B>
 __device__ void fill_sad_window(Smem &S, int g, int gt, int buf, const uint8_t *ref, int s, int W, int H,
-                                const uint8_t *cur, int wx, int wy) {
-    int *tab = (int *)(S.pred[g] + WIN_OFF) + buf * WIN_N * WIN_N;
-    if (gt == 0) OPCOUNT(0, WIN_N * WIN_N * B * B);
-    if (gt < WIN_N * WIN_N) {
-        const int x = wx + gt % WIN_N - WIN_R, y = wy + gt / WIN_N - WIN_R;
+                                const uint8_t *cur, int wx, int wy, int R) {
+    const int N = 2 * R + 1;
+    int *tab = (int *)(S.pred[g] + WIN_OFF) + buf * WIN_NMAX * WIN_NMAX;
+    if (gt == 0) OPCOUNT(0, N * N * B * B);
+    if (gt < N * N) {
+        const int x = wx + gt % N - R, y = wy + gt / N - R;
         int v = 0x7FFFFFFF;
         if (x >= 0 && y >= 0 && x + B <= W && y + B <= H) {
             int acc = 0;
@@ -333,7 +340,7 @@ __device__ void fill_sad_window(Smem &S, int g, int gt, int buf, const uint8_t *
 }
 
 struct SadWindow {
-    int wx = 0, wy = 0, buf = 0;
+    int wx = 0, wy = 0, buf = 0, R = 4;
     bool valid = false;
 };
 
@@ -349,14 +356,14 @@ __device__ void int_stage_windowed(Smem &S, int g, int gt, const uint8_t *ref, i
                 int dx, dy;
                 pat_point(pat, p, dx, dy);
                 const int x = bx + dx, y = by + dy;
-                if (!win.valid || x < win.wx - WIN_R || x > win.wx + WIN_R || y < win.wy - WIN_R ||
-                    y > win.wy + WIN_R) {
+                const int R = win.R;
+                if (!win.valid || x < win.wx - R || x > win.wx + R || y < win.wy - R || y > win.wy + R) {
                     win.buf ^= 1; win.wx = bx; win.wy = by; win.valid = true;
-                    if (blk == 16) fill_sad_window<16>(S, g, gt, win.buf, ref, s, W, H, cur, win.wx, win.wy);
-                    else fill_sad_window<8>(S, g, gt, win.buf, ref, s, W, H, cur, win.wx, win.wy);
+                    if (blk == 16) fill_sad_window<16>(S, g, gt, win.buf, ref, s, W, H, cur, win.wx, win.wy, R);
+                    else fill_sad_window<8>(S, g, gt, win.buf, ref, s, W, H, cur, win.wx, win.wy, R);
                 }
-                const int *tab = (const int *)(S.pred[g] + WIN_OFF) + win.buf * WIN_N * WIN_N;
-                const int v = tab[(y - win.wy + WIN_R) * WIN_N + (x - win.wx + WIN_R)];
+                const int *tab = (const int *)(S.pred[g] + WIN_OFF) + win.buf * WIN_NMAX * WIN_NMAX;
+                const int v = tab[(y - win.wy + R) * (2 * R + 1) + (x - win.wx + R)];
                 if (v < bsad) { found = p; fs = v; fx = dx; fy = dy; break; }
             }
             if (found < 0) break;
@@ -540,6 +547,7 @@ __device__ __noinline__ void me_run(Smem &, int g, int gt, const uint8_t *ref, i
     int_stage(S, g, gt, par, ref, s, W, H, cur, blk, 0, 6, 2, scale, bx, by, bsad, true);
     if (blk <= 16) {
         SadWindow win;
+        win.R = window_radius(g_fp.search_window);
         int_stage_windowed(S, g, gt, ref, s, W, H, cur, blk, 1, 6, 3, win, bx, by, bsad);
         int_stage_windowed(S, g, gt, ref, s, W, H, cur, blk, 2, 4, 4, win, bx, by, bsad);
     } else {

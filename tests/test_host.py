@@ -107,6 +107,28 @@ def test_autotune_choice_table():
     assert L.tcb_autotune_frame_kernels(w, h, 0) == api.TC_ERR_PARAM         # no frames
 
 
+def test_engine_tuning_choice_table():
+    """The engine autotuner's choice table (no GPU needed): defaults R = 4
+    and diagonal order, every radius 2..5 and both orders recorded per frame
+    size, other sizes untouched, invalid values refused, (0, 0) restores the
+    defaults."""
+    from tcodec_b200 import api
+    L = api.bind_b200(api.load_library())
+    w, h = 1922, 1084
+    assert api.engine_tuning(L, w, h) == (4, api.QUEUE_DIAGONAL)
+    for r in range(api.SEARCH_WINDOW_MIN, api.SEARCH_WINDOW_MAX + 1):
+        for o in (api.QUEUE_DIAGONAL, api.QUEUE_STAGGERED):
+            assert L.tcb_engine_set_tuning(w, h, r, o) == 0
+            assert api.engine_tuning(L, w, h) == (r, o)
+            assert api.engine_tuning(L, w + 2, h) == (4, api.QUEUE_DIAGONAL)
+    for r, o in ((1, 0), (6, 0), (4, 2), (4, -1), (0, 1)):
+        assert L.tcb_engine_set_tuning(w, h, r, o) == api.TC_ERR_PARAM, (r, o)
+    assert L.tcb_engine_set_tuning(0, h, 4, 0) == api.TC_ERR_PARAM
+    assert L.tcb_engine_get_tuning(w, h, None, None) == api.TC_ERR_PARAM
+    assert L.tcb_engine_set_tuning(w, h, 0, 0) == 0
+    assert api.engine_tuning(L, w, h) == (4, api.QUEUE_DIAGONAL)
+
+
 def test_transform_dc_paths(tmp_path):
     """The reference's transform checks (test/test_tcodec.c:3074-3149) on
     the library's residual transforms and the DC-only helpers of
