@@ -495,6 +495,59 @@ struct QpelAnchors {
 // Quarter-pel refinement straight from the reference frame, for searches
 // whose points may leave the six-tap margins or for blocks above 16x16
 // (out of line: most small-block searches never run it).
+// Six-tap sub-pel SAD of a 32x32 or 64x64 block on column segments: thread
+// gt takes column gt & (blk-1) and blk*blk/128 consecutive rows, walking
+// down them with six-row windows of the integer samples at x, x+1 and of
+// the horizontal half samples at x.  Each new row costs six byte loads and
+// one horizontal six-tap; the vertical (c, f) and centre (d) half samples
+// come from the windows, and the phase combination is luma_hv's (reference
+// src/motion.c:190-260).  luma_hv per sample re-derives up to eleven six-tap
+// filters; this is the same arithmetic on the same samples.
+__device__ int group_subpel_sad_cols(Smem &S, int g, int gt, int &par, const uint8_t *ref, int s,
+                                     const uint8_t *cur, int blk, int qx, int qy) {
+    const int fx = qx >> 2, fy = qy >> 2, dx = qx & 3, dy = qy & 3;
+    const int lgb = lg2i(blk), L = blk * blk / GT;      // rows per thread: 8 or 32
+    const int xx = gt & (blk - 1), y0 = (gt >> lgb) * L, X = fx + xx;
+    if (gt == 0) OPCOUNT(1, blk * blk);
+    int i0[6], i1[6], hw[6];   // rows Y-2 .. Y+3 of the current output row Y
+    const uint8_t *row = ref + (size_t)(fy + y0 - 2) * s + X;
+    auto load_row = [&](const uint8_t *r, int &a, int &b, int &h) {
+        const int m2 = r[-2], m1 = r[-1], c0 = r[0], c1 = r[1], p2 = r[2], p3 = r[3];
+        a = c0; b = c1;
+        h = (m2 - 5 * m1 + 20 * c0 + 20 * c1 - 5 * p2 + p3 + 16) >> 5;
+    };
+#pragma unroll
+    for (int k = 0; k < 5; ++k) load_row(row + (size_t)k * s, i0[k], i1[k], hw[k]);
+    int acc = 0;
+#pragma unroll 1
+    for (int j = 0; j < L; ++j) {
+        load_row(row + (size_t)(j + 5) * s, i0[5], i1[5], hw[5]);
+        const int a00 = i0[2], a10 = i1[2], a01 = i0[3], a11 = i1[3];
+        const int b = hw[2], e = hw[3];
+        const int c = (i0[0] - 5 * i0[1] + 20 * i0[2] + 20 * i0[3] - 5 * i0[4] + i0[5] + 16) >> 5;
+        const int f = (i1[0] - 5 * i1[1] + 20 * i1[2] + 20 * i1[3] - 5 * i1[4] + i1[5] + 16) >> 5;
+        const int d = (hw[0] - 5 * hw[1] + 20 * hw[2] + 20 * hw[3] - 5 * hw[4] + hw[5] + 16) >> 5;
+        int top, mid, bot;
+        switch (dx) {
+            case 0:  top = a00;               mid = c;               bot = a01; break;
+            case 1:  top = (a00 + b + 1) >> 1; mid = (c + d + 1) >> 1; bot = (a01 + e + 1) >> 1; break;
+            case 2:  top = b;                 mid = d;               bot = e; break;
+            default: top = (b + a10 + 1) >> 1; mid = (d + f + 1) >> 1; bot = (e + a11 + 1) >> 1; break;
+        }
+        int r;
+        switch (dy) {
+            case 0:  r = top; break;
+            case 1:  r = (top + mid + 1) >> 1; break;
+            case 2:  r = mid; break;
+            default: r = (mid + bot + 1) >> 1; break;
+        }
+        acc += absi((int)cur[(y0 + j) * 64 + xx] - clampi(r, 0, 255));
+#pragma unroll
+        for (int k = 0; k < 5; ++k) { i0[k] = i0[k + 1]; i1[k] = i1[k + 1]; hw[k] = hw[k + 1]; }
+    }
+    return group_sum(S, g, gt, par, acc);
+}
+
 __device__ __noinline__ void qpel_refine_direct(int g, int gt, int &par, const uint8_t *ref, int s, int W, int H,
                                                 const uint8_t *cur, int blk, int &mx, int &my, int &bsad) {
     Smem &S = smem_state();
@@ -503,7 +556,8 @@ __device__ __noinline__ void qpel_refine_direct(int g, int gt, int &par, const u
         const int fx = qx >> 2, fy = qy >> 2;
         if (fx < 0 || fy < 0 || fx + blk + 1 > W || fy + blk + 1 > H) continue;
         const bool six = fx >= 2 && fy >= 2 && fx + blk + 2 < W && fy + blk + 2 < H;
-        const int sum = group_subpel_sad(S, g, gt, par, ref, s, cur, blk, qx, qy, six);
+        const int sum = six && blk >= 32 ? group_subpel_sad_cols(S, g, gt, par, ref, s, cur, blk, qx, qy)
+                                         : group_subpel_sad(S, g, gt, par, ref, s, cur, blk, qx, qy, six);
         if (sum < bsad) { bsad = sum; mx = qx; my = qy; }
     }
 }
