@@ -919,65 +919,65 @@ __device__ __noinline__ void cfl_blend(Smem &, const Leaf L, int dst) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     __shared__ int s_sign[2], s_shift[2];
     if (warp < 2) {
+        // At most 64 neighbour pairs of 8-bit samples: every sum and product
+        // below stays under 2^29 (n * sum(la * cv) <= 64 * 64 * 255^2), so
+        // 32-bit integers give the reference's int64 values.
         const int c = warp;
-        long long sl = 0, sc = 0, slc = 0, sl2 = 0;
-        int n = 0;
+        int sl = 0, sc = 0, slc = 0, sl2 = 0;
         for (int i = lane; i < cs; i += 32) {
             if (up) {
                 const int la = (RY(S, L.lx + 2 * i, L.ly - 1) + RY(S, L.lx + 2 * i + 1, L.ly - 1) + 1) >> 1;
                 const int cv = RC(S, c, lxc + i, lyc - 1);
-                sl += la; sc += cv; slc += (long long)la * cv; sl2 += (long long)la * la;
+                sl += la; sc += cv; slc += la * cv; sl2 += la * la;
             }
             if (left) {
                 const int la = (RY(S, L.lx - 2, L.ly + 2 * i) + RY(S, L.lx - 1, L.ly + 2 * i) +
                                 RY(S, L.lx - 2, L.ly + 2 * i + 1) + RY(S, L.lx - 1, L.ly + 2 * i + 1) + 2) >> 2;
                 const int cv = RC(S, c, lxc - 1, lyc + i);
-                sl += la; sc += cv; slc += (long long)la * cv; sl2 += (long long)la * la;
+                sl += la; sc += cv; slc += la * cv; sl2 += la * la;
             }
         }
-        n = (up ? cs : 0) + (left ? cs : 0);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            sl += __shfl_xor_sync(0xffffffffu, sl, o);
-            sc += __shfl_xor_sync(0xffffffffu, sc, o);
-            slc += __shfl_xor_sync(0xffffffffu, slc, o);
-            sl2 += __shfl_xor_sync(0xffffffffu, sl2, o);
-        }
+        const int n = (up ? cs : 0) + (left ? cs : 0);
+        sl = (int)__reduce_add_sync(0xffffffffu, (unsigned)sl);
+        sc = (int)__reduce_add_sync(0xffffffffu, (unsigned)sc);
+        slc = (int)__reduce_add_sync(0xffffffffu, (unsigned)slc);
+        sl2 = (int)__reduce_add_sync(0xffffffffu, (unsigned)sl2);
         if (lane == 0) {
-            const long long nn = n;
-            const int sign = (nn == 0 || nn * slc >= sl * sc) ? 1 : -1;
+            const int sign = (n == 0 || n * slc >= sl * sc) ? 1 : -1;
             int ash = 3;
-            const long long cov = nn * slc - sl * sc, vl = nn * sl2 - sl * sl;
-            if (nn > 0 && vl > 0 && cov != 0) {
-                const unsigned long long acov = cov < 0 ? (unsigned long long)(-cov) : (unsigned long long)cov;
-                const unsigned long long q = (unsigned long long)vl / acov;
-                int s = (q < 1) ? 2 : (q > 0xFFFFFFFFull) ? 5 : 31 - __clz((int)(unsigned)q);
-                ash = s < 2 ? 2 : (s > 5 ? 5 : s);
+            const int cov = n * slc - sl * sc, vl = n * sl2 - sl * sl;
+            if (n > 0 && vl > 0 && cov != 0) {
+                const unsigned q = (unsigned)vl / (unsigned)(cov < 0 ? -cov : cov);
+                const int sh = q < 1 ? 2 : 31 - __clz((int)q);
+                ash = sh < 2 ? 2 : (sh > 5 ? 5 : sh);
             }
             s_sign[c] = sign;
             s_shift[c] = ash;
         }
     }
+    // The 2x2-averaged collocated luma of every chroma position, then its
+    // mean per 4x4 chroma tile, into the residual jobs' scratch (idle here).
+    const int nt = cs >> 2, lgs = lg2i(cs), lgt = lgs - 2;
+    int *la = &S.scratch[0][0];              // cs * cs entries
+    int *tile = la + 32 * 32;                // nt * nt entries
+    for (int i = threadIdx.x; i < cs * cs; i += NT) {
+        const int X = L.lx + 2 * (i & (cs - 1)), Y = L.ly + 2 * (i >> lgs);
+        la[i] = (RY(S, X, Y) + RY(S, X + 1, Y) + RY(S, X, Y + 1) + RY(S, X + 1, Y + 1) + 2) >> 2;
+    }
     SYNC();
-    // Per 4x4 chroma tile: mean of the 2x2-averaged collocated luma.
-    const int nt = cs >> 2, lgs = lg2i(cs);
-    for (int i = threadIdx.x; i < 2 * cs * cs; i += NT) {
-        const int c = i >> (2 * lgs), p = i & ((1 << (2 * lgs)) - 1), y = p >> lgs, x = p & (cs - 1);
-        const int ty = (y >> 2) << 2, tx = (x >> 2) << 2;
+    for (int t = threadIdx.x; t < nt * nt; t += NT) {
+        const int *q = la + ((t >> lgt) << 2) * cs + ((t & (nt - 1)) << 2);
         int sum = 0;
 #pragma unroll
-        for (int yy = 0; yy < 4; ++yy)
-#pragma unroll
-            for (int xx = 0; xx < 4; ++xx) {
-                const int X = L.lx + 2 * (tx + xx), Y = L.ly + 2 * (ty + yy);
-                sum += (RY(S, X, Y) + RY(S, X + 1, Y) + RY(S, X, Y + 1) + RY(S, X + 1, Y + 1) + 2) >> 2;
-            }
-        const int avg = (sum + 8) / 16;
-        const int X = L.lx + 2 * x, Y = L.ly + 2 * y;
-        const int la = (RY(S, X, Y) + RY(S, X + 1, Y) + RY(S, X, Y + 1) + RY(S, X + 1, Y + 1) + 2) >> 2;
+        for (int yy = 0; yy < 4; ++yy) sum += q[yy * cs] + q[yy * cs + 1] + q[yy * cs + 2] + q[yy * cs + 3];
+        tile[t] = (sum + 8) >> 4;            // sum >= 0
+    }
+    SYNC();
+    for (int i = threadIdx.x; i < 2 * cs * cs; i += NT) {
+        const int c = i >> (2 * lgs), p = i & ((1 << (2 * lgs)) - 1), y = p >> lgs, x = p & (cs - 1);
+        const int avg = tile[(y >> 2) * nt + (x >> 2)];
         uint8_t &d = S.cpred[dst + c][p];
-        d = (uint8_t)clampi((int)d + s_sign[c] * ((la - avg) >> s_shift[c]), 0, 255);
-        (void)nt;
+        d = (uint8_t)clampi((int)d + s_sign[c] * ((la[p] - avg) >> s_shift[c]), 0, 255);
     }
     SYNC();
 }
