@@ -47,6 +47,14 @@ void tcb_encoder_get_timing(tc_encoder_t *enc, double *ctu_ms, int64_t *ctu_laun
  * encoder->recon (default on, as the reference keeps it current). */
 void tcb_encoder_set_recon_readback(tc_encoder_t *enc, int enabled);
 
+/* Host threads that entropy-code a frame's entry-point rows (frames of
+ * more than one CTU row in entry-point mode code every row as its own
+ * range-coded substream).  Clamped to [1, 64]; the packets do not depend
+ * on it.  Default min(8, hardware threads) for tc_encoder_create, 1 for
+ * the encoders of a batch or server, which code their streams in
+ * parallel instead. */
+void tcb_encoder_set_entropy_threads(tc_encoder_t *enc, int threads);
+
 /* ---------------------------------------------------------------------
  * Batched form (no reference counterpart): N independent v2 streams that
  * advance one frame per call and share every CTU-engine launch.  Each

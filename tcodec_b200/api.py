@@ -320,6 +320,7 @@ def bind_b200(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.tcb_encoder_set_timing.argtypes = [vp, ctypes.c_int]
     lib.tcb_encoder_get_timing.argtypes = [vp] + [vp] * 5
     lib.tcb_encoder_set_recon_readback.argtypes = [vp, ctypes.c_int]
+    lib.tcb_encoder_set_entropy_threads.argtypes = [vp, ctypes.c_int]
     lib.tcb_batch_create.argtypes = [ctypes.POINTER(Config), ctypes.c_int]
     lib.tcb_batch_create.restype = vp
     lib.tcb_batch_destroy.argtypes = [vp]

@@ -416,6 +416,7 @@ int tcb::batch_attach(tcb_batch *b, tc_encoder_t *e) {
     EncImpl &im = *e->impl;
     im.st = b->st;                          // all device work on the batch stream
     im.defer_glob = true;
+    im.entropy_threads = 1;                 // the batch codes its streams in parallel
     std::vector<std::vector<int>> diags(im.diag_off.size());
     for (int d = 0; d < (int)im.diag_off.size(); ++d)
         for (int r = 0; r < im.ctu_rows; ++r) {

@@ -14,6 +14,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -519,27 +521,47 @@ tc_error_t EncImpl::stage_d(tc_packet_t *pkt) {
         const size_t ep_payload = bw.byte_pos;
         const size_t per_row = out_buf_size / (size_t)(nrows > 1 ? nrows : 1) + 1024;
         if (nrows > 64) return TC_ERR_MEMORY;
-        if (row_buf.size() < per_row) row_buf.resize(per_row);
+        // Every row is coded into its own slot of row_buf (rows spread over
+        // the encoder's entropy threads), then the rows are laid out in
+        // order: the same bytes as coding them one after another.
+        if (row_buf.size() < per_row * (size_t)nrows) row_buf.resize(per_row * (size_t)nrows);
+        size_t row_bytes[64];
+        bool row_bad[64];
+        auto code_rows = [&](int first, int step) {
+            for (int r = first; r < nrows; r += step) {
+                BitWriter rw;
+                rw.init(row_buf.data() + (size_t)r * per_row, per_row);
+                RangeEncoder rc;
+                uint8_t ctx[TC_NUM_CONTEXTS_RC];
+                memset(ctx, 0, sizeof(ctx));
+                rc.init(&rw);
+                SyntaxSink sink{&rw, entropy ? &rc : nullptr, ctx};
+                for (int c = 0; c < ctu_cols; ++c) {
+                    const CtuGeom g{c * 64, r * 64, W, H, frame_type, multiref};
+                    write_ctu_syntax(sink, rec_out[r * ctu_cols + c], g);
+                }
+                if (entropy) rc.flush();
+                rw.align();
+                row_bad[r] = rw.overflow;
+                row_bytes[r] = rw.bytes();
+            }
+        };
+        const int nth = std::max(1, std::min(entropy_threads, nrows));
+        if (nth > 1) {
+            std::vector<std::thread> th;
+            for (int t = 1; t < nth; ++t) th.emplace_back(code_rows, t, nth);
+            code_rows(0, nth);
+            for (auto &x : th) x.join();
+        } else {
+            code_rows(0, 1);
+        }
         uint32_t row_off[64];
         for (int r = 0; r < nrows; ++r) {
-            BitWriter rw;
-            rw.init(row_buf.data(), per_row);
-            RangeEncoder rc;
-            uint8_t ctx[TC_NUM_CONTEXTS_RC];
-            memset(ctx, 0, sizeof(ctx));
-            rc.init(&rw);
-            SyntaxSink sink{&rw, entropy ? &rc : nullptr, ctx};
-            for (int c = 0; c < ctu_cols; ++c) {
-                const CtuGeom g{c * 64, r * 64, W, H, frame_type, multiref};
-                write_ctu_syntax(sink, rec_out[r * ctu_cols + c], g);
-            }
-            if (entropy) rc.flush();
-            rw.align();
-            if (rw.overflow) return TC_ERR_MEMORY;
-            const size_t rb = rw.bytes();
+            if (row_bad[r]) return TC_ERR_MEMORY;
+            const size_t rb = row_bytes[r];
             if (rb > per_row || bw.byte_pos + rb > out_buf_size) return TC_ERR_MEMORY;
             row_off[r] = (uint32_t)(bw.byte_pos - ep_payload);
-            memcpy(buf + bw.byte_pos, row_buf.data(), rb);
+            memcpy(buf + bw.byte_pos, row_buf.data() + (size_t)r * per_row, rb);
             bw.byte_pos += rb;
         }
         for (int i = 0; i < nrows; ++i) {
@@ -787,6 +809,8 @@ tc_encoder_t *tcb::encoder_create(const tc_config_t *config, DeviceArena *arena)
     enc->recon = tcb_host_frame_alloc(config->width, config->height, 1);
     if (!enc->cur || !enc->recon) { tc_encoder_destroy(enc); return nullptr; }
     enc->impl->recon_host = enc->recon;
+    const unsigned hw = std::thread::hardware_concurrency();
+    enc->impl->entropy_threads = (int)std::min(8u, hw ? hw : 1u);
     return enc;
 }
 
@@ -846,6 +870,10 @@ void tcb_encoder_get_timing(tc_encoder_t *enc, double *ctu_ms, int64_t *ctu_laun
 
 void tcb_encoder_set_recon_readback(tc_encoder_t *enc, int enabled) {
     if (enc && enc->impl) enc->impl->recon_readback = enabled != 0;
+}
+
+void tcb_encoder_set_entropy_threads(tc_encoder_t *enc, int threads) {
+    if (enc && enc->impl) enc->impl->entropy_threads = std::max(1, std::min(64, threads));
 }
 
 tc_error_t tc_encoder_flush_tail(tc_encoder_t *enc, tc_packet_t *packet_out) {

@@ -141,6 +141,11 @@ struct EncImpl {
     bool defer_glob = false;
     BitWriter fbw;
     std::vector<uint8_t> row_buf;
+    // Host threads that entropy-code one frame's entry-point rows (each row
+    // is an independent range-coded substream). A lone encoder uses up to 8;
+    // a batch or server codes each of its streams on its own thread and sets
+    // its encoders to 1.
+    int entropy_threads = 1;
     tc_error_t plan_input();
     tc_error_t plan_flush();
     tc_error_t stage_a(int poc, int b_layer_qp_off);

@@ -28,13 +28,17 @@ CONFIGS = {   # name: (workload, width, height, frames, qp, profile, B frames)
 }
 
 
-def run(lib, name):
+def run(lib, name, entropy_threads=None):
+    """Encode configuration `name` with `lib`; `entropy_threads` (B200
+    library only) sets the encoder's host threads for entry-point rows."""
     from tcodec_b200 import api, synth
     from tests.golden.make_pframe_golden import digest_planes
     wl, w, h, n, qp, prof, bf = CONFIGS[name]
     cfg = api.make_config(lib, w, h, qp=qp, preset=api.PRESET_MEDIUM, profile=prof, keyframe_interval=1000,
                           b_frames=bf)
     enc = api.Encoder(lib, cfg)
+    if entropy_threads is not None:
+        lib.tcb_encoder_set_entropy_threads(enc.h, entropy_threads)
     pk = []
     try:
         for f in synth.workload(wl, frames=n):

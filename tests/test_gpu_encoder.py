@@ -166,6 +166,21 @@ def test_single_stream_configs_known_answers(lib, name):
     assert got["final_recon"] == want["final_recon"]
 
 
+@pytest.mark.parametrize("threads", [1, 5])
+def test_entry_point_rows_any_thread_count(lib, threads):
+    """Entry-point frames code every CTU row as its own range-coded
+    substream, on up to tcb_encoder_set_entropy_threads host threads (12
+    rows of 1280x720 spread unevenly over 5, or all on one): the packets
+    and reconstruction equal the reference encoder's whatever the count."""
+    from tcodec_b200 import api
+    from tests.golden import make_config_golden as cg
+    api.bind_b200(lib)
+    want = json.load(open(os.path.join(HERE, "golden", "configs_v2.json")))["cfg1"]
+    got = cg.run(lib, "cfg1", entropy_threads=threads)
+    assert got["packets"] == want["packets"]
+    assert got["final_recon"] == want["final_recon"]
+
+
 SCASES = json.load(open(os.path.join(HERE, "golden", "scenecut_v2.json")))
 
 
