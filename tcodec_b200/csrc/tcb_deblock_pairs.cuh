@@ -34,7 +34,13 @@ namespace tcb {
 // (reference src/filter.c:23-38: strength > 0 iff the difference is below
 // the third threshold).  Lanes 0..255, t in 8..48.
 __host__ __device__ __forceinline__ uint32_t deblock_keep(uint32_t p0, uint32_t q0, uint32_t t) {
+    // |p0 - q0| per lane: the lanes' high bytes are 0 in both, so the
+    // byte-wise absolute difference is the lane-wise one
+#ifdef __CUDA_ARCH__
+    const uint32_t diff = __vabsdiffu4(p0, q0);
+#else
     const uint32_t diff = pair_max(p0, q0) - pair_min(p0, q0);
+#endif
     const uint32_t ge = diff + (0x8000u - t) * 0x00010001u;   // bit 15 of a lane set iff diff >= t
     return pair_prmt(ge, 0, 0xBB99);                           // sign of each lane's high byte, replicated
 }

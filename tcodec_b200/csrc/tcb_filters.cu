@@ -19,8 +19,11 @@
 // segments (kept in registers for the whole CTU) and a private column of a
 // [row][thread] table in shared memory, so its read-modify-writes never
 // conflict.  A table word packs count and difference sum as
-// count * 65536 + sum (|sum| <= 32 * 255), which one integer add per pixel
-// maintains exactly.  Rows are the 30 inner bands plus the 16 single
+// count * 65536 + sum of (256 + o - r), which one integer add per pixel
+// maintains exactly (tcb_sao_decide.cuh: SAO_BIAS, sao_unpack); the rows and increments of a
+// word's four pixels come from a few word operations (sao_rows4,
+// sao_incr4), leaving a lane extract, an address and the read-modify-write
+// per pixel.  Rows are the 30 inner bands plus the 16 single
 // sample values of bands 0 and 31, where an offset can clip; the SSE of
 // every band after its offset then follows in closed form, clipping
 // included (tcb_sao_decide.cuh), with no second pass over the pixels.
@@ -246,12 +249,10 @@ __device__ __forceinline__ int byte_i(const uint4 &v, int i) {
 
 // One sample pair into the thread's statistics column: the word of the
 // sample's row (sao_row_of, computed: a lookup table would add a shared
-// load with bank conflicts to every pixel) gains count 1 and o - r.
+// load with bank conflicts to every pixel) gains 65536 + SAO_BIAS + o - r.
 template <int SFT>
 __device__ __forceinline__ void sao_count(int *col, int r, int o) {
-    int row = r >> 3;
-    if ((unsigned)(r - 8) >= 240u) row = 32 + (r & 7) + ((r >> 4) & 8);   // values 0..7 -> 32.., 248..255 -> 40..
-    col[row * SFT] += 65536 + o - r;
+    col[sao_row_of(r) * SFT] += 65536 + (int)SAO_BIAS + o - r;
 }
 
 template <int SFT>
@@ -259,13 +260,13 @@ __global__ void __launch_bounds__(SFT) sao_frames_kernel(SaoJobs J) {
     constexpr int NSEG = 256 / SFT;           // 16-pixel segments per thread
     static_assert(SFT == 64 || SFT == 128, "SAO CTA: 256 16-pixel segments per CTU, table within 48 KB");
     // G columns of the table are summed before unpacking: a column holds
-    // at most 16 * NSEG pixels, so G columns keep |sum| <= G * 16 * NSEG *
-    // 255 = 32640, inside the 16-bit field.
+    // at most 16 * NSEG samples, and a sum of words splits exactly up to
+    // 128 (sao_unpack).
     constexpr int G = NSEG <= 2 ? 4 : 2;
     constexpr int TPR = SFT >= 2 * SAO_ROWS ? 2 : 1;   // threads summing one row
-    __shared__ __align__(16) int hist[SAO_ROWS][SFT];   // count * 65536 + sum of (org - rec), per thread
+    __shared__ __align__(16) int hist[SAO_ROWS][SFT];   // count * 65536 + sum of (256 + org - rec), per thread
     __shared__ int row_cnt[SAO_ROWS], row_sum[SAO_ROWS];
-    __shared__ long long red[SFT / 32];
+    __shared__ int red[SFT / 32];
     __shared__ int dec[3];
     const int k = find_frame(J.ctu_off, J.n, blockIdx.x);
     const SaoFrame &F = J.f[k];
@@ -277,9 +278,18 @@ __global__ void __launch_bounds__(SFT) sao_frames_kernel(SaoJobs J) {
     uint4 rv[NSEG], ov[NSEG];
     int nvalid[NSEG];
     bool vec[NSEG];
+    const uint8_t *const rec0 = F.rec + (size_t)y0 * F.sr + x0, *const org0 = F.org + (size_t)y0 * F.so + x0;
+    const bool full = w == 64 && h == 64 && aligned16(rec0, F.sr) && aligned16(org0, F.so);
 #pragma unroll
     for (int j = 0; j < NSEG; ++j) {
         const int sg = t + j * SFT, row = sg >> 2, c0 = (sg & 3) * 16;
+        if (full) {   // every segment whole and 16-byte aligned
+            nvalid[j] = 16;
+            vec[j] = true;
+            rv[j] = __ldcs((const uint4 *)(rec0 + (size_t)row * F.sr + c0));
+            ov[j] = __ldcs((const uint4 *)(org0 + (size_t)row * F.so + c0));
+            continue;
+        }
         nvalid[j] = row < h ? max(0, min(16, w - c0)) : 0;
         const uint8_t *gr = F.rec + (size_t)(y0 + row) * F.sr + x0 + c0;
         const uint8_t *go = F.org + (size_t)(y0 + row) * F.so + x0 + c0;
@@ -313,16 +323,25 @@ __global__ void __launch_bounds__(SFT) sao_frames_kernel(SaoJobs J) {
             base = (int)__dp4a(ad, ad, (unsigned)base);
         }
         if (nvalid[j] == 16) {
+            // rows and increments of four samples per word operation
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-#pragma unroll
-                for (int b = 0; b < 4; ++b) sao_count<SFT>(col, byte_k(rw[q], b), byte_k(ow[q], b));
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t rows = sao_rows4(rw[q]);
+                uint32_t even, odd;
+                sao_incr4(rw[q], ow[q], even, odd);
+                // shared-memory atomic adds with no result: one instruction
+                // per sample instead of a load / add / store chain (the
+                // column is private, so they never contend)
+                atomicAdd(&col[(rows & 0xFF) * SFT], (int)sao_lane_lo(even));
+                atomicAdd(&col[((rows >> 8) & 0xFF) * SFT], (int)sao_lane_lo(odd));
+                atomicAdd(&col[((rows >> 16) & 0xFF) * SFT], (int)sao_lane_hi(even));
+                atomicAdd(&col[(rows >> 24) * SFT], (int)sao_lane_hi(odd));
+            }
         } else {
             for (int i = 0; i < nvalid[j]; ++i) sao_count<SFT>(col, byte_i(rv[j], i), byte_i(ov[j], i));
         }
     }
-    long long bsum = base;
-    for (int o = 16; o > 0; o >>= 1) bsum += __shfl_xor_sync(0xffffffffu, bsum, o);
+    const int bsum = __reduce_add_sync(0xffffffffu, (unsigned)base);
     if ((t & 31) == 0) red[t >> 5] = bsum;
     __syncthreads();
     // ---- row totals: TPR threads per row, summing G columns at a time
@@ -331,11 +350,7 @@ __global__ void __launch_bounds__(SFT) sao_frames_kernel(SaoJobs J) {
         const int row = t / TPR, part = t % TPR;
         const int4 *p = (const int4 *)&hist[row][part * (SFT / TPR)];
         int cnt = 0, sum = 0;
-        auto unpack = [&](int x) {
-            const int sv = (int)(int16_t)(x & 0xffff);
-            sum += sv;
-            cnt += (x - sv) >> 16;
-        };
+        auto unpack = [&](int x) { sao_unpack((uint32_t)x, cnt, sum); };
         // start each thread at its own 16-byte column group: the rows are
         // 128 words apart, so unrotated every lane would read the same banks
         constexpr int NV = SFT / TPR / 4;
@@ -350,6 +365,7 @@ __global__ void __launch_bounds__(SFT) sao_frames_kernel(SaoJobs J) {
                 unpack(v.z + v.w);
             }
         }
+        sum -= (int)SAO_BIAS * cnt;
         if (TPR == 2) {
             cnt += __shfl_xor_sync(0xffffffffu, cnt, 1);
             sum += __shfl_xor_sync(0xffffffffu, sum, 1);
@@ -360,14 +376,14 @@ __global__ void __launch_bounds__(SFT) sao_frames_kernel(SaoJobs J) {
     // ---- decision (warp 0): lane b scores band b; first band with the
     // smallest SSE; rate gate of 6 lambda
     if (t < 32) {
-        long long b0 = 0;
+        int b0 = 0;
         for (int i = 0; i < SFT / 32; ++i) b0 += red[i];
         int cand;
-        const long long sse = sao_band_sse(t, b0, row_cnt, row_sum, &cand);
-        long long best = cand ? sse : b0;
+        const int sse = sao_band_sse(t, b0, row_cnt, row_sum, &cand);
+        int best = cand ? sse : b0;
         int bb = cand ? t : 32;
         for (int o = 16; o > 0; o >>= 1) {
-            const long long ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int ob = __shfl_xor_sync(0xffffffffu, best, o);
             const int obb = __shfl_xor_sync(0xffffffffu, bb, o);
             const int oc = __shfl_xor_sync(0xffffffffu, cand, o);
             if (ob < best || (ob == best && obb < bb)) { best = ob; bb = obb; cand = oc; }

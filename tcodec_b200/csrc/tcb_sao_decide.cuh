@@ -19,6 +19,8 @@
 #pragma once
 #include <cstdint>
 
+#include "tcb_pair16.cuh"
+
 namespace tcb {
 
 constexpr int SAO_ROWS = 48;
@@ -28,12 +30,48 @@ __host__ __device__ __forceinline__ int sao_row_of(int v) {
     return v < 8 ? 32 + v : (v >= 248 ? v - 208 : v >> 3);
 }
 
+// sao_row_of of the four samples of a word at once (byte i of the result
+// for byte i of r).  Bands 1..30 keep their band; bands 0 and 31 (band + 1
+// is 1 or 32, with no bit of 0x1E set) take 32 + (v & 15), which is
+// 32..39 for 0..7 and 40..47 for 248..255.
+__host__ __device__ __forceinline__ uint32_t sao_rows4(uint32_t r) {
+    const uint32_t band = (r >> 3) & 0x1F1F1F1Fu;
+    const uint32_t value_row = (r & 0x0F0F0F0Fu) | 0x20202020u;
+    const uint32_t inner = pair_prmt(((band + 0x01010101u) & 0x1E1E1E1Eu) + 0x7F7F7F7Fu, 0, 0xBA98);
+    return (band & inner) | (value_row & ~inner);
+}
+
+// A statistics word gains 65536 + 256 + o - r per sample: the count in
+// its high half and the biased difference 256 + o - r (1..511) in its low
+// half.  Up to 128 samples keep the low half below 65536, so words of up
+// to 128 samples in total can be added before they are split
+// (sao_unpack); the sum is the low halves less 256 per sample.
+constexpr uint32_t SAO_BIAS = 256;
+
+// The biased differences 256 + o - r of the four samples of (r, o): bytes
+// 0 and 2 in the low and high lanes of `even`, bytes 1 and 3 in those of
+// `odd`.
+__host__ __device__ __forceinline__ void sao_incr4(uint32_t r, uint32_t o, uint32_t &even, uint32_t &odd) {
+    even = (o & 0x00FF00FFu) + SAO_BIAS * 0x00010001u - (r & 0x00FF00FFu);
+    odd = pair_prmt(o, 0, 0x4341) + SAO_BIAS * 0x00010001u - pair_prmt(r, 0, 0x4341);
+}
+// The statistics increment of a lane: the lane with 1 in the count half.
+__host__ __device__ __forceinline__ uint32_t sao_lane_lo(uint32_t x) { return pair_prmt(x, 1, 0x5410); }
+__host__ __device__ __forceinline__ uint32_t sao_lane_hi(uint32_t x) { return pair_prmt(x, 1, 0x5432); }
+
+// Count and biased sum of a word (or sum of words) of at most 128 samples;
+// the row's sum of o - r is then bsum - SAO_BIAS * cnt.
+__host__ __device__ __forceinline__ void sao_unpack(uint32_t w, int &cnt, int &bsum) {
+    cnt += (int)(w >> 16);
+    bsum += (int)(w & 0xFFFF);
+}
+
 // SSE of the CTU after offsetting band b by its candidate (written to
 // *cand; 0 when the band is empty or its offset rounds to 0, and then the
-// SSE returned is base).
-__host__ __device__ inline long long sao_band_sse(int b, long long base, const int *row_cnt, const int *row_sum,
-                                                  int *cand) {
-    long long n = 0, s = 0;
+// SSE returned is base).  Every term fits in 32 bits for a 64x64 CTU:
+// base <= 4096 * 255^2 < 2^28, |S| <= 4096 * 255, |c| <= 7.
+__host__ __device__ inline int sao_band_sse(int b, int base, const int *row_cnt, const int *row_sum, int *cand) {
+    int n = 0, s = 0;
     if (b == 0 || b == 31) {
         const int r0 = b ? 40 : 32;
         for (int k = 0; k < 8; ++k) { n += row_cnt[r0 + k]; s += row_sum[r0 + k]; }
@@ -43,19 +81,18 @@ __host__ __device__ inline long long sao_band_sse(int b, long long base, const i
     }
     *cand = 0;
     if (n == 0) return base;
-    long long c = (s + (s >= 0 ? n / 2 : -(n / 2))) / n;
+    int c = (s + (s >= 0 ? n / 2 : -(n / 2))) / n;
     c = c < -7 ? -7 : (c > 7 ? 7 : c);
-    *cand = (int)c;
+    *cand = c;
     if (c == 0) return base;
-    long long sse = base - 2 * c * s + n * c * c;
+    int sse = base - 2 * c * s + n * c * c;
     if (b == 0 && c < 0) {
         for (int v = 0; v < 8; ++v)
-            if (v + c < 0) sse += 2 * (v + c) * row_sum[32 + v] + (long long)row_cnt[32 + v] * (v + c) * (v - c);
+            if (v + c < 0) sse += 2 * (v + c) * row_sum[32 + v] + row_cnt[32 + v] * (v + c) * (v - c);
     } else if (b == 31 && c > 0) {
         for (int v = 248; v < 256; ++v)
             if (v + c > 255)
-                sse += 2 * (v - 255 + c) * row_sum[v - 208] +
-                       (long long)row_cnt[v - 208] * (v - 255 + c) * (v - 255 - c);
+                sse += 2 * (v - 255 + c) * row_sum[v - 208] + row_cnt[v - 208] * (v - 255 + c) * (v - 255 - c);
     }
     return sse;
 }

@@ -7,7 +7,8 @@
 //   * deblocking: every vertical and horizontal work item of a CTU, run in a
 //     random order, against or_deblock_ctu;
 //   * SAO: the closed-form band SSE (sao_band_sse) against a brute-force
-//     SSE of the offset, clipped CTU.
+//     SSE of the offset, clipped CTU, and the word-level statistics
+//     helpers (sao_rows4, sao_incr4, sao_unpack) exhaustively.
 // Built for the host only by tests/test_packed_lanes.py; exit status 0 when
 // every case matches.
 #include <algorithm>
@@ -139,12 +140,12 @@ long check_sao(std::mt19937 &rng, long &bands) {
             org[i] = std::min(255, std::max(0, rec[i] + (int)(rng() % 31) - 15));
         }
         int cnt[SAO_ROWS] = {}, sum[SAO_ROWS] = {};
-        long long base = 0;
+        int base = 0;
         for (int i = 0; i < 64 * 64; ++i) {
             const int r = sao_row_of(rec[i]);
             ++cnt[r];
             sum[r] += org[i] - rec[i];
-            base += (long long)(org[i] - rec[i]) * (org[i] - rec[i]);
+            base += (org[i] - rec[i]) * (org[i] - rec[i]);
         }
         for (int b = 0; b < 32; ++b) {
             int c = 0;
@@ -161,6 +162,38 @@ long check_sao(std::mt19937 &rng, long &bands) {
     return bad;
 }
 
+// The word-level statistics helpers of the SAO kernel: sao_rows4 against
+// sao_row_of for every sample value in every byte, sao_incr4 for every
+// (reconstruction, source) pair, and sao_unpack at the largest counts a
+// word can hold with the most negative and positive sums.
+long check_sao_words() {
+    long bad = 0;
+    for (uint32_t v = 0; v < 256; ++v)
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t w = (0x5A3C81F0u & ~(0xFFu << (8 * k))) | v << (8 * k);
+            const uint32_t rows = sao_rows4(w);
+            for (int i = 0; i < 4; ++i) bad += (int)((rows >> (8 * i)) & 0xFF) != sao_row_of((w >> (8 * i)) & 0xFF);
+        }
+    for (uint32_t r = 0; r < 256; ++r)
+        for (uint32_t o = 0; o < 256; ++o) {
+            const uint32_t rw = r | (255 - r) << 8 | ((r * 7) & 255) << 16 | ((r + 128) & 255) << 24;
+            const uint32_t ow = o | ((o * 3) & 255) << 8 | (255 - o) << 16 | ((o + 77) & 255) << 24;
+            uint32_t even, odd;
+            sao_incr4(rw, ow, even, odd);
+            const uint32_t inc[4] = {sao_lane_lo(even), sao_lane_lo(odd), sao_lane_hi(even), sao_lane_hi(odd)};
+            for (int i = 0; i < 4; ++i)
+                bad += (int)inc[i] != 65536 + (int)SAO_BIAS + (int)((ow >> (8 * i)) & 0xFF) -
+                                          (int)((rw >> (8 * i)) & 0xFF);
+        }
+    for (int n = 0; n <= 128; ++n)
+        for (int d : {-255, -1, 0, 1, 255}) {
+            int cnt = 0, bsum = 0;
+            sao_unpack((uint32_t)n * (65536u + SAO_BIAS + d), cnt, bsum);
+            bad += cnt != n || bsum - (int)SAO_BIAS * cnt != n * d;
+        }
+    return bad;
+}
+
 }  // namespace
 
 int main() {
@@ -169,6 +202,8 @@ int main() {
     const long mc = check_mc(rng, blocks), db = check_deblock(rng, ctus), sao = check_sao(rng, bands);
     printf("mc blocks %ld mismatching samples %ld\n", blocks, mc);
     printf("deblock ctus %ld mismatching %ld\n", ctus, db);
+    const long saow = check_sao_words();
     printf("sao bands %ld mismatching %ld\n", bands, sao);
-    return (mc || db || sao) ? 1 : 0;
+    printf("sao word helpers mismatching %ld\n", saow);
+    return (mc || db || sao || saow) ? 1 : 0;
 }
