@@ -6,16 +6,20 @@
 // 32.  Filtering an edge changes only p0 and q0, and the edges of one
 // direction are 4 samples apart while a filter reads p1..q1, so all edges of
 // one direction are independent; the kernel runs them as work items in any
-// order, vertical before horizontal, luma and chroma side by side.  An item
-// filters two edge positions at once, one per lane:
+// order, vertical before horizontal, luma and chroma side by side.  Every
+// filter call handles two edge positions at once, one per lane:
 //
-//   luma / Cb vertical  (row, edges 2j+1 and 2j+2 of the row): the four
-//                       bytes around each edge come from the words at
-//                       columns 8j, 8j+4, 8j+8; the item rewrites word 8j+4
-//                       whole and the two bytes it owns in the other two
-//                       (their other bytes belong to neighbouring items)
-//   luma horizontal     (edge, four columns): one word from each of the
-//                       rows y-2 .. y+1, two items per word pair of lanes
+//   luma / Cb vertical  (edges 2j+1 and 2j+2 of a row): the four bytes
+//                       around each edge come from the words at columns 8j,
+//                       8j+4, 8j+8; the pair rewrites word 8j+4 whole and
+//                       one byte of each of the other two.  The kernels take
+//                       a whole row per item (deblock_vert_row: 16-byte
+//                       loads and stores, the bytes merged in registers);
+//                       deblock_vert keeps the single-pair items, which the
+//                       CPU check runs against the rows
+//   luma horizontal     (edge, 4 WPI columns): WPI words from each of the
+//                       rows y-2 .. y+1, two pairs per word; the kernels
+//                       use WPI = 4 (16-byte rows)
 //   chroma horizontal   (edge, four columns): rows 4e and 4e+1 of Cr decide
 //                       and filter Cr and Cb (the reference filters across
 //                       the row pair 4e / 4e+1 for both planes)
@@ -120,15 +124,87 @@ __host__ __device__ __forceinline__ void deblock_vert_item(uint8_t *row, int row
     }
 }
 
-// Horizontal luma edge e (y = 4e), columns 4c..4c+3; rows 64 bytes apart.
-__host__ __device__ __forceinline__ void deblock_luma_horiz_item(uint8_t *tile, int e, int c, DeblockQp q) {
-    uint32_t *w = (uint32_t *)(tile + (4 * e - 2) * 64 + 4 * c);
-    const uint32_t r0 = w[0], r1 = w[16], r2 = w[32], r3 = w[48];
-    uint32_t p0a = pair_lo(r1), q0a = pair_lo(r2), p0b = pair_hi(r1), q0b = pair_hi(r2);
-    deblock_luma_pair(pair_lo(r0), p0a, q0a, pair_lo(r3), q.t3, q.tc);
-    deblock_luma_pair(pair_hi(r0), p0b, q0b, pair_hi(r3), q.t3, q.tc);
-    w[16] = pair_pack(p0a, p0b);
-    w[32] = pair_pack(q0a, q0b);
+// Every vertical edge of one row of NW words (16: luma, 8: Cb), in
+// registers: the row is read and written with 16-byte accesses, and the
+// filtered bytes are merged into the words by byte permutes.  The inputs
+// of every edge are taken from the unfiltered words (no edge reads a byte
+// another edge writes), so this equals the items of the row in any order.
+template <int NW>
+__host__ __device__ __forceinline__ void deblock_vert_row(uint8_t *row, bool luma, DeblockQp q) {
+    uint32_t w[NW], o[NW];
+#pragma unroll
+    for (int i = 0; i < NW / 4; ++i) {
+        const uint4 v = ((const uint4 *)row)[i];
+        w[4 * i] = v.x; w[4 * i + 1] = v.y; w[4 * i + 2] = v.z; w[4 * i + 3] = v.w;
+    }
+#pragma unroll
+    for (int i = 0; i < NW; ++i) o[i] = w[i];
+#pragma unroll
+    for (int j = 0; j < NW / 2; ++j) {
+        const bool two = 2 * j + 2 < NW;
+        const uint32_t wa = w[2 * j], wb = w[2 * j + 1], wc = two ? w[2 * j + 2] : wb;
+        const uint32_t lp = pair_prmt(wa, wb, 0x7632), lq = pair_prmt(wb, wc, 0x5410);
+        uint32_t p1 = lp & 0x00FF00FFu, p0 = (lp >> 8) & 0x00FF00FFu;
+        uint32_t q0 = lq & 0x00FF00FFu, q1 = (lq >> 8) & 0x00FF00FFu;
+        if (luma) deblock_luma_pair(p1, p0, q0, q1, q.t3, q.tc);
+        else deblock_chroma_pair(p0, q0, deblock_keep(p0, q0, q.ct3), q.ctc);
+        o[2 * j] = pair_prmt(o[2 * j], p0, 0x4210);                       // byte 3 <- p0 of edge 2j+1
+        if (two) {
+            o[2 * j + 1] = pair_prmt(wb, pair_prmt(q0, p0, 0x6000), 0x7214);
+            o[2 * j + 2] = pair_prmt(o[2 * j + 2], q0, 0x3216);           // byte 0 <- q0 of edge 2j+2
+        } else {
+            o[2 * j + 1] = pair_prmt(wb, q0, 0x3214);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NW / 4; ++i) ((uint4 *)row)[i] = make_uint4(o[4 * i], o[4 * i + 1], o[4 * i + 2], o[4 * i + 3]);
+}
+
+// Rows of the vertical phase: 64 luma rows, then 32 Cb rows.
+constexpr int DEBLOCK_VERT_ROWS = 64 + 32;
+__host__ __device__ __forceinline__ void deblock_vert_rows(uint8_t *ty, uint8_t *tcb, int i, DeblockQp q) {
+    if (i < 64) deblock_vert_row<16>(ty + i * 64, true, q);
+    else deblock_vert_row<8>(tcb + (i - 64) * 32, false, q);
+}
+
+// Horizontal luma edge e, columns 4 WPI c .. 4 WPI c + 4 WPI - 1: the
+// four rows around the edge read and the two filtered rows written as
+// WPI-word vectors.
+template <int WPI>
+__host__ __device__ __forceinline__ void deblock_luma_horiz_wide(uint8_t *tile, int e, int c, DeblockQp q) {
+    uint32_t r[4][WPI];
+    uint8_t *base = tile + (4 * e - 2) * 64 + 4 * WPI * c;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if constexpr (WPI == 4) {
+            const uint4 v = *(const uint4 *)(base + k * 64);
+            r[k][0] = v.x; r[k][1] = v.y; r[k][2] = v.z; r[k][3] = v.w;
+        } else if constexpr (WPI == 2) {
+            const uint2 v = *(const uint2 *)(base + k * 64);
+            r[k][0] = v.x; r[k][1] = v.y;
+        } else {
+            r[k][0] = *(const uint32_t *)(base + k * 64);
+        }
+    }
+    uint32_t np[WPI], nq[WPI];
+#pragma unroll
+    for (int i = 0; i < WPI; ++i) {
+        uint32_t p0a = pair_lo(r[1][i]), q0a = pair_lo(r[2][i]), p0b = pair_hi(r[1][i]), q0b = pair_hi(r[2][i]);
+        deblock_luma_pair(pair_lo(r[0][i]), p0a, q0a, pair_lo(r[3][i]), q.t3, q.tc);
+        deblock_luma_pair(pair_hi(r[0][i]), p0b, q0b, pair_hi(r[3][i]), q.t3, q.tc);
+        np[i] = pair_pack(p0a, p0b);
+        nq[i] = pair_pack(q0a, q0b);
+    }
+    if constexpr (WPI == 4) {
+        *(uint4 *)(base + 64) = make_uint4(np[0], np[1], np[2], np[3]);
+        *(uint4 *)(base + 128) = make_uint4(nq[0], nq[1], nq[2], nq[3]);
+    } else if constexpr (WPI == 2) {
+        *(uint2 *)(base + 64) = make_uint2(np[0], np[1]);
+        *(uint2 *)(base + 128) = make_uint2(nq[0], nq[1]);
+    } else {
+        *(uint32_t *)(base + 64) = np[0];
+        *(uint32_t *)(base + 128) = nq[0];
+    }
 }
 
 // Horizontal chroma edge e (rows 4e and 4e + 1), columns 4c..4c+3 of both
@@ -150,10 +226,8 @@ __host__ __device__ __forceinline__ void deblock_chroma_horiz_item(uint8_t *cb, 
     wb[8] = pair_pack(qa, qb);
 }
 
-// Item counts of the two phases: vertical = 64 luma rows x 8 + 32 Cb rows
-// x 4; horizontal = 15 luma edges x 16 + 7 chroma edges x 8.
+// Items of the vertical phase: 64 luma rows x 8 + 32 Cb rows x 4.
 constexpr int DEBLOCK_VERT_ITEMS = 64 * 8 + 32 * 4;
-constexpr int DEBLOCK_HORIZ_ITEMS = 15 * 16 + 7 * 8;
 
 __host__ __device__ __forceinline__ void deblock_vert(uint8_t *ty, uint8_t *tcb, int i, DeblockQp q) {
     if (i < 64 * 8) deblock_vert_item(ty + (i >> 3) * 64, 64, i & 7, true, q);
@@ -162,11 +236,17 @@ __host__ __device__ __forceinline__ void deblock_vert(uint8_t *ty, uint8_t *tcb,
         deblock_vert_item(tcb + (i >> 2) * 32, 32, i & 3, false, q);
     }
 }
-__host__ __device__ __forceinline__ void deblock_horiz(uint8_t *ty, uint8_t *tcb, uint8_t *tcr, int i,
-                                                     DeblockQp q) {
-    if (i < 15 * 16) deblock_luma_horiz_item(ty, (i >> 4) + 1, i & 15, q);
+// The horizontal phase with luma items WPI words wide: 15 luma edges x
+// 16 / WPI items, then the 7 x 8 chroma items.
+template <int WPI>
+constexpr int deblock_horiz_wide_items() { return 15 * (16 / WPI) + 7 * 8; }
+template <int WPI>
+__host__ __device__ __forceinline__ void deblock_horiz_wide(uint8_t *ty, uint8_t *tcb, uint8_t *tcr, int i,
+                                                          DeblockQp q) {
+    constexpr int PER = 16 / WPI;
+    if (i < 15 * PER) deblock_luma_horiz_wide<WPI>(ty, i / PER + 1, i % PER, q);
     else {
-        i -= 15 * 16;
+        i -= 15 * PER;
         deblock_chroma_horiz_item(tcb, tcr, (i >> 3) + 1, i & 7, q);
     }
 }

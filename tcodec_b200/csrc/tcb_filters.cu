@@ -116,14 +116,14 @@ __global__ void __launch_bounds__(DFT) deblock_frames_kernel(DeblockJobs J) {
         }
     }
     __syncthreads();
-    // ---- vertical edges, then horizontal edges, as independent two-lane
-    // items (tcb_deblock_pairs.cuh): 640 vertical items (5 per thread at
-    // 128 threads), 296 horizontal
+    // ---- vertical edges, then horizontal edges, as independent items
+    // (tcb_deblock_pairs.cuh): 96 vertical rows (64 luma, 32 Cb), then 60
+    // luma items of 16 columns and 56 chroma items of 4
     DeblockQp q;
     q.init(F.qp);
-    for (int i = t; i < DEBLOCK_VERT_ITEMS; i += DFT) deblock_vert(ty, tc[0], i, q);
+    for (int i = t; i < DEBLOCK_VERT_ROWS; i += DFT) deblock_vert_rows(ty, tc[0], i, q);
     __syncthreads();
-    for (int i = t; i < DEBLOCK_HORIZ_ITEMS; i += DFT) deblock_horiz(ty, tc[0], tc[1], i, q);
+    for (int i = t; i < deblock_horiz_wide_items<4>(); i += DFT) deblock_horiz_wide<4>(ty, tc[0], tc[1], i, q);
     __syncthreads();
     // ---- store
     if (vec) {
@@ -220,9 +220,9 @@ __global__ void __launch_bounds__(DFT) deblock_tma_kernel(const __grid_constant_
     }
     DeblockQp q;
     q.init(J.qp[k]);
-    for (int i = t; i < DEBLOCK_VERT_ITEMS; i += DFT) deblock_vert(ty, tc[0], i, q);
+    for (int i = t; i < DEBLOCK_VERT_ROWS; i += DFT) deblock_vert_rows(ty, tc[0], i, q);
     __syncthreads();
-    for (int i = t; i < DEBLOCK_HORIZ_ITEMS; i += DFT) deblock_horiz(ty, tc[0], tc[1], i, q);
+    for (int i = t; i < deblock_horiz_wide_items<4>(); i += DFT) deblock_horiz_wide<4>(ty, tc[0], tc[1], i, q);
     // the filters' shared-memory writes become visible to the bulk-copy
     // (async) proxy before the stores read the tile
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

@@ -4,8 +4,9 @@
 //     of the 15 compile-time phases, mc_chroma_bilinear, on row strides that
 //     are multiples of 4 (the kernels' condition for the packed path),
 //     against or_pred_luma / or_pred_chroma;
-//   * deblocking: every vertical and horizontal work item of a CTU, run in a
-//     random order, against or_deblock_ctu;
+//   * deblocking: every vertical and horizontal work item of a CTU (the
+//     vertical ones also as whole rows), run in a random order, against
+//     or_deblock_ctu;
 //   * SAO: the closed-form band SSE (sao_band_sse) against a brute-force
 //     SSE of the offset, clipped CTU, and the word-level statistics
 //     helpers (sao_rows4, sao_incr4, sao_unpack) exhaustively.
@@ -115,14 +116,28 @@ long check_deblock(std::mt19937 &rng, long &ctus) {
         or_deblock_ctu(wy, 64, wb, 32, wr, 32, 0, 0, qp);
         DeblockQp q;
         q.init(qp);
-        std::vector<int> ord(DEBLOCK_VERT_ITEMS);
-        for (int i = 0; i < DEBLOCK_VERT_ITEMS; ++i) ord[i] = i;
+        // vertical phase as single items (even iterations) or as whole
+        // rows (odd), both in a random order
+        const int nv = (it & 1) ? DEBLOCK_VERT_ROWS : DEBLOCK_VERT_ITEMS;
+        std::vector<int> ord(nv);
+        for (int i = 0; i < nv; ++i) ord[i] = i;
         std::shuffle(ord.begin(), ord.end(), rng);
-        for (int i : ord) deblock_vert(ty, tb, i, q);
-        ord.resize(DEBLOCK_HORIZ_ITEMS);
-        for (int i = 0; i < DEBLOCK_HORIZ_ITEMS; ++i) ord[i] = i;
+        for (int i : ord) {
+            if (it & 1) deblock_vert_rows(ty, tb, i, q);
+            else deblock_vert(ty, tb, i, q);
+        }
+        // horizontal phase with luma items 1, 2 or 4 words wide
+        const int wpi = 1 << (it % 3);
+        const int nh = wpi == 1 ? deblock_horiz_wide_items<1>() : wpi == 2 ? deblock_horiz_wide_items<2>()
+                                                                         : deblock_horiz_wide_items<4>();
+        ord.resize(nh);
+        for (int i = 0; i < nh; ++i) ord[i] = i;
         std::shuffle(ord.begin(), ord.end(), rng);
-        for (int i : ord) deblock_horiz(ty, tb, tr, i, q);
+        for (int i : ord) {
+            if (wpi == 1) deblock_horiz_wide<1>(ty, tb, tr, i, q);
+            else if (wpi == 2) deblock_horiz_wide<2>(ty, tb, tr, i, q);
+            else deblock_horiz_wide<4>(ty, tb, tr, i, q);
+        }
         bad += memcmp(ty, wy, sizeof wy) != 0 || memcmp(tb, wb, sizeof wb) != 0 || memcmp(tr, wr, sizeof wr) != 0;
         ++ctus;
     }
