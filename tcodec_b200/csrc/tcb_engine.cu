@@ -1053,6 +1053,14 @@ __device__ void sad_jobs(Smem &S, const Leaf &L, const int *cl, int ncl) {
     }
 }
 
+// Thirteen nibbles a0..a12 packed low to high (kind k at bits 4k..4k+3).
+__host__ __device__ constexpr uint64_t nib13(int a0, int a1, int a2, int a3, int a4, int a5, int a6, int a7,
+                                             int a8, int a9, int a10, int a11, int a12) {
+    return (uint64_t)a0 | (uint64_t)a1 << 4 | (uint64_t)a2 << 8 | (uint64_t)a3 << 12 | (uint64_t)a4 << 16 |
+           (uint64_t)a5 << 20 | (uint64_t)a6 << 24 | (uint64_t)a7 << 28 | (uint64_t)a8 << 32 | (uint64_t)a9 << 36 |
+           (uint64_t)a10 << 40 | (uint64_t)a11 << 44 | (uint64_t)a12 << 48;
+}
+
 __device__ __forceinline__ long long best_of(const Smem &S, int slot, bool use4, long long lambda,
                                              int &lb, int &dct) {
     const long long d8 = S.acc_sse[slot][0];
@@ -1474,57 +1482,65 @@ __device__ __noinline__ long long leaf_decide(Smem &, const FrameParams &, const
     if (tid < 32) {
         enum { C_NONE, C_P_ME0, C_P_ME1, C_P_GLB, C_P_TMP, C_P_MRG, C_P_SKIP,
                C_B_DIR0, C_B_DIR1, C_B_M2, C_B_M3, C_B_M4, C_INTRA };
+        // Scan parameters of each kind, one nibble per kind (kind k in bits
+        // 4k..4k+3), so that every lane runs the same code whatever its kind:
+        //   SL1   slot + 1 of the candidate's sums (0: none; intra: its slot)
+        //   EXT   extra bits; MRX: added with multiref; PLB: level bits of
+        //         the SAD proxy
+        //   FA    1 MV bits, 2 SAD proxy on fast presets, 4 merge (8x8-only
+        //         sums), 8 second reference
+        //   FB    1 bi-predicted, 2 skip, 4 intra, 8 merge MV (the MVP)
+        //        NONE ME0 ME1 GLB TMP MRG SKIP DIR0 DIR1 M2  M3  M4  INTRA
+        constexpr uint64_t SL1 = nib13(0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0);
+        constexpr uint64_t EXT = nib13(0, 6, 8, 6, 6, 6, 2, 6, 6, 6, 6, 6, 8);
+        constexpr uint64_t MRX = nib13(0, 2, 0, 1, 2, 0, 0, 0, 0, 0, 0, 0, 0);
+        constexpr uint64_t PLB = nib13(0, 3, 0, 0, 0, 0, 0, 3, 3, 0, 0, 0, 8);
+        constexpr uint64_t FA = nib13(0, 3, 9, 1, 1, 4, 0, 3, 11, 4, 4, 12, 2);
+        constexpr uint64_t FB = nib13(0, 0, 0, 0, 0, 8, 2, 0, 0, 1, 0, 0, 4);
+        static_assert(K_ME0 == 0 && K_ME1 == 1 && K_GLB == 2 && K_TMP == 3 && K_MRG == 4 && K_B0 == 0,
+                      "SL1 holds the candidate slots + 1");
         const int lane = tid;
         const long long lam = P.lambda;
         const int base_x = mvpx + L.px * 4, base_y = mvpy + L.py * 4;
-        int kinds[6], nk = 0;
+        uint32_t klist = 0;   // the inter kinds of the scan order, a nibble each
+        int nk = 0;
+        auto push = [&](int k) { klist |= (uint32_t)k << (4 * nk); ++nk; };
         if (is_b) {
-            if (rf >= 0) kinds[nk++] = C_B_DIR0;
-            if (rb >= 0) kinds[nk++] = C_B_DIR1;
+            if (rf >= 0) push(C_B_DIR0);
+            if (rb >= 0) push(C_B_DIR1);
             if (medium && !fast) {
-                if (rf >= 0 && rb >= 0) kinds[nk++] = C_B_M2;
-                if (rf >= 0) kinds[nk++] = C_B_M3;
-                if (rb >= 0) kinds[nk++] = C_B_M4;
+                if (rf >= 0 && rb >= 0) push(C_B_M2);
+                if (rf >= 0) push(C_B_M3);
+                if (rb >= 0) push(C_B_M4);
             }
         } else if (is_p) {
-            kinds[nk++] = C_P_ME0;
-            if (has_me1) kinds[nk++] = C_P_ME1;
-            if (has_glb) kinds[nk++] = C_P_GLB;
-            if (has_tmp) kinds[nk++] = C_P_TMP;
+            push(C_P_ME0);
+            if (has_me1) push(C_P_ME1);
+            if (has_glb) push(C_P_GLB);
+            if (has_tmp) push(C_P_TMP);
             if (medium) {
-                kinds[nk++] = C_P_MRG;
-                if (P.ref_valid[0] && S.acc64[0] == 0 && S.acc64[1] == 0) kinds[nk++] = C_P_SKIP;
+                push(C_P_MRG);
+                if (P.ref_valid[0] && S.acc64[0] == 0 && S.acc64[1] == 0) push(C_P_SKIP);
             }
         }
         const int n = nk + (try_intra ? ncl - ninter : 0);
         int kind = C_NONE, slot = 0;
-        if (lane < nk) kind = kinds[lane];
+        if (lane < nk) kind = (klist >> (4 * lane)) & 15;
         else if (lane < n) { kind = C_INTRA; slot = S.cl[ninter + lane - nk]; }
-        // Each kind only sets its parameters (a short divergent switch); the
-        // cost then comes from one common path for all lanes:
-        //   cost = distortion + lambda * (extra + MV bits + level bits)
-        // with distortion / level bits from best_of (explicit inter and
-        // intra), the 8x8-only sums (merges), the SAD proxy (fast presets)
-        // or nothing (skip).
-        int sl = -1, extra = 0, plb = 0, mvsl = -1;
-        bool mvbits = false, merge8 = false, proxy = false;
-        int f_intra = 0, f_skip = 0, f_merge = 0, f_bi = 0, f_dct = 1, f_ref = 0, f_mx = 0, f_my = 0, f_mode = 1;
-        switch (kind) {
-            case C_P_ME0: sl = K_ME0; extra = 6 + (P.multiref ? 2 : 0); mvbits = true; proxy = fast; plb = 3; break;
-            case C_P_ME1: sl = K_ME1; extra = 8; mvbits = true; f_ref = 1; break;
-            case C_P_GLB: sl = K_GLB; extra = 6 + (P.multiref ? 1 : 0); mvbits = true; break;
-            case C_P_TMP: sl = K_TMP; extra = 6 + (P.multiref ? 2 : 0); mvbits = true; break;
-            case C_P_MRG: sl = K_MRG; extra = 6; merge8 = true; f_merge = 1; mvsl = K_ME0; break;
-            case C_P_SKIP: extra = 2; f_skip = 1; break;
-            case C_B_DIR0: sl = K_B0; extra = 6; mvbits = true; proxy = fast; plb = 3; break;
-            case C_B_DIR1: sl = K_B0 + 1; extra = 6; mvbits = true; proxy = fast; plb = 3; f_ref = 1; break;
-            case C_B_M2: sl = K_B0 + 2; extra = 6; merge8 = true; f_merge = 1; f_bi = 1; break;
-            case C_B_M3: sl = K_B0 + 3; extra = 6; merge8 = true; f_merge = 1; break;
-            case C_B_M4: sl = K_B0 + 4; extra = 6; merge8 = true; f_merge = 1; f_ref = 1; break;
-            case C_INTRA: sl = slot; extra = 8; proxy = fast; plb = 8; f_intra = 1; f_mode = slot - K_INTRA; break;
-            default: break;
-        }
-        if (mvbits) mvsl = sl;
+        const int sh = 4 * kind;
+        const int fa = (int)(FA >> sh) & 15, fb = (int)(FB >> sh) & 15;
+        const int sl = kind == C_INTRA ? slot : (int)((SL1 >> sh) & 15) - 1;
+        const bool mvbits = fa & 1, proxy = fast && (fa & 2), merge8 = fa & 4;
+        const int extra = (int)((EXT >> sh) & 15) + (P.multiref ? (int)((MRX >> sh) & 15) : 0);
+        const int plb = (int)((PLB >> sh) & 15);
+        const int mvsl = mvbits ? sl : ((fb & 8) ? K_ME0 : -1);
+        const int f_intra = (fb >> 2) & 1, f_skip = (fb >> 1) & 1, f_merge = merge8, f_bi = fb & 1;
+        const int f_ref = fa >> 3, f_mode = f_intra ? slot - K_INTRA : 1;
+        int f_dct = 1, f_mx = 0, f_my = 0;
+        // cost = distortion + lambda * (extra + MV bits + level bits), with
+        // distortion / level bits from best_of (explicit inter and intra),
+        // the 8x8-only sums (merges), the SAD proxy (fast presets) or
+        // nothing (skip)
         long long cost = (long long)1 << 60;   // no candidate: defaults, as the sequential scan
         if (kind != C_NONE) {
             long long dl = 0;
@@ -1557,21 +1573,7 @@ __device__ __noinline__ long long leaf_decide(Smem &, const FrameParams &, const
             if (oc < bc || (oc == bc && ol < bl)) { bc = oc; bl = ol; }
         }
         if (lane == bl) {
-            int ws = -1;
-            switch (kind) {
-                case C_P_ME0: ws = K_ME0; break;
-                case C_P_ME1: ws = K_ME1; break;
-                case C_P_GLB: ws = K_GLB; break;
-                case C_P_TMP: ws = K_TMP; break;
-                case C_P_MRG: ws = K_MRG; break;
-                case C_B_DIR0: ws = K_B0; break;
-                case C_B_DIR1: ws = K_B0 + 1; break;
-                case C_B_M2: ws = K_B0 + 2; break;
-                case C_B_M3: ws = K_B0 + 3; break;
-                case C_B_M4: ws = K_B0 + 4; break;
-                case C_INTRA: ws = slot; break;
-                default: ws = -1; break;
-            }
+            const int ws = sl;   // every kind's winner slot is its sums' slot (-1: skip, none)
             S.win_slot = ws;
             Node &nd = S.nodes[qt_index(L.depth, L.cx, L.cy)];
             nd.intra = (uint8_t)f_intra; nd.skip = (uint8_t)f_skip; nd.merge = (uint8_t)f_merge;
