@@ -89,6 +89,7 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.tc_decoder_create.argtypes = [ctypes.c_int32, ctypes.c_int32]
     lib.tc_decoder_create.restype = ctypes.c_void_p
     lib.tc_decoder_destroy.argtypes = [ctypes.c_void_p]
+    lib.tc_decoder_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.tc_decoder_destroy.restype = None
     lib.tc_decoder_decode.argtypes = [ctypes.c_void_p, u8p, ctypes.c_size_t, pp, ip, pp, ip, pp, ip]
     lib.tc_decoder_decode.restype = ctypes.c_int
@@ -215,11 +216,13 @@ class Encoder:
 class Decoder:
     """One decode session through the C ABI (tc_decoder_*)."""
 
-    def __init__(self, lib: ctypes.CDLL, width: int = 0, height: int = 0):
+    def __init__(self, lib: ctypes.CDLL, width: int = 0, height: int = 0, threads: Optional[int] = None):
         self.lib = lib
         self.h = lib.tc_decoder_create(width, height)
         if not self.h:
             raise RuntimeError("tc_decoder_create failed")
+        if threads is not None:
+            lib.tc_decoder_set_threads(self.h, threads)
 
     def close(self) -> None:
         if self.h:
@@ -482,9 +485,10 @@ class BatchEncoder:
                     out[i].append(ctypes.string_at(pk[i].data, pk[i].size))
 
 
-def decode_sequence(lib: ctypes.CDLL, packets, width: int = 0, height: int = 0):
-    """Decode packets (coding order) into display-order frames."""
-    dec = Decoder(lib, width, height)
+def decode_sequence(lib: ctypes.CDLL, packets, width: int = 0, height: int = 0, threads: Optional[int] = None):
+    """Decode packets (coding order) into display-order frames
+    (`threads`: tc_decoder_set_threads, when given)."""
+    dec = Decoder(lib, width, height, threads)
     out = []
     try:
         for p in packets:

@@ -11,7 +11,9 @@
 #include <string.h>
 #include <time.h>
 
+#include <algorithm>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -562,14 +564,35 @@ tc_error_t DecImpl::decode(const uint8_t *data, size_t size, const tc_pixel_t **
             const size_t start = payload + off[r];
             const size_t end = r + 1 < rows ? payload + off[r + 1] : data_end;
             if (end < start || end > size) return TC_ERR_BITSTREAM;
-            Reader rr;
-            rr.init(data + start, end - start);
-            RDec rc;
-            uint8_t ctx[TC_NUM_CONTEXTS_RC];
-            memset(ctx, 0, sizeof(ctx));
-            if (entropy) rc.init(&rr);
-            if (!parse_rows(rr, entropy ? &rc : nullptr, ctx, r, r + 1)) return TC_ERR_BITSTREAM;
         }
+        // Every row is its own substream with fresh contexts and writes
+        // only its own CTU records, so the rows parse on up to `threads`
+        // host threads (tc_decoder_set_threads); any bad row fails the frame.
+        bool row_bad[64];
+        auto parse_part = [&](int first, int step) {
+            for (int r = first; r < rows; r += step) {
+                const size_t start = payload + off[r];
+                const size_t end = r + 1 < rows ? payload + off[r + 1] : data_end;
+                Reader rr;
+                rr.init(data + start, end - start);
+                RDec rc;
+                uint8_t ctx[TC_NUM_CONTEXTS_RC];
+                memset(ctx, 0, sizeof(ctx));
+                if (entropy) rc.init(&rr);
+                row_bad[r] = !parse_rows(rr, entropy ? &rc : nullptr, ctx, r, r + 1);
+            }
+        };
+        const int nth = std::max(1, std::min(threads, rows));
+        if (nth > 1) {
+            std::vector<std::thread> th;
+            for (int t = 1; t < nth; ++t) th.emplace_back(parse_part, t, nth);
+            parse_part(0, nth);
+            for (auto &x : th) x.join();
+        } else {
+            parse_part(0, 1);
+        }
+        for (int r = 0; r < rows; ++r)
+            if (row_bad[r]) return TC_ERR_BITSTREAM;
     } else {
         RDec rc;
         uint8_t ctx[TC_NUM_CONTEXTS_RC];

@@ -52,6 +52,23 @@ def test_decoder_matches_encoder_recon_and_reference_decoder(lib, ref_lib, ci):
                 assert np.array_equal(pa, pb)
 
 
+@pytest.mark.parametrize("threads", [1, 3, 16])
+def test_decoder_entry_point_rows_any_thread_count(lib, ref_lib, threads):
+    """A 1280x720 GOP4-B stream (12 CTU rows, each an entry-point
+    substream) decodes to the reference decoder's pictures whatever the
+    number of host threads parsing the rows (tc_decoder_set_threads)."""
+    from tcodec_b200 import api, synth
+    frames = synth.workload("rects", frames=6, width=1280, height=720)
+    cfg = api.make_config(lib, 1280, 720, qp=27, preset=2, profile=1, keyframe_interval=1000, b_frames=True)
+    pk = api.encode_sequence(lib, cfg, frames)
+    mine = api.decode_sequence(lib, pk, threads=threads)
+    ref = api.decode_sequence(ref_lib, pk)
+    assert len(mine) == len(ref) == len(frames)
+    for a, b in zip(mine, ref):
+        for pa, pb in zip(a, b):
+            assert np.array_equal(pa, pb)
+
+
 def test_decoder_on_reference_streams(lib, ref_lib):
     from tcodec_b200 import api, synth
     frames = synth.moving_rects_clip(160, 96, 5, seed_rects=5)
