@@ -562,26 +562,55 @@ __device__ __noinline__ void qpel_refine_direct(int g, int gt, int &par, const u
     }
 }
 
+// An 8x8 block's 64 samples leave half the group idle, so the idle half
+// scores the next point around the same best: a pair of points per group
+// barrier, the first improvement committed (the second point is scored
+// again around the new best when the first one wins).  16x16 blocks take
+// one point per barrier.  Either way the commits are the sequential walk's.
 template <int B>
 __device__ void qpel_refine_anchored(Smem &S, int g, int gt, int &par, const uint8_t *ref, int s,
                                      const uint8_t *cur, int bx, int by, int &mx, int &my, int &bsad) {
     const QpelAnchors<B> A(S.pred[g]);
     A.build(S, g, gt, ref, s, bx, by);
-    for (int p = 1; p < 9; ++p) {
-        const int qx = mx + c_qpel[p][0], qy = my + c_qpel[p][1];
-        const int X0 = (qx >> 2) - (bx - 1), Y0 = (qy >> 2) - (by - 1), dx = qx & 3, dy = qy & 3;
-        if (gt == 0) OPCOUNT(1, B * B);
+    constexpr int NS = B * B;                     // samples of a point: 64 or 256
+    constexpr int PPP = NS < GT ? GT / NS : 1;    // points per barrier: 2 (8x8) or 1 (16x16)
+    constexpr int SPT = NS > GT ? NS / GT : 1;    // samples per thread and point: 1 or 2
+    static_assert(PPP * NS == GT * SPT && PPP <= 2, "one pass covers the group");
+    const int wig = gt >> 5, lane = gt & 31;
+    const int kk = PPP == 2 ? gt / NS : 0;        // this thread's point of the pair
+    const int i0 = gt & (NS - 1);
+    int p = 1;
+    while (p < 9) {
+        const int K = mini(9 - p, PPP);
+        if (gt == 0) OPCOUNT(1, K * NS);
+        int *part = S.me[g].part[par];
         int acc = 0;
+        if (kk < K) {
+            const int qx = mx + c_qpel[p + kk][0], qy = my + c_qpel[p + kk][1];
+            const int X0 = (qx >> 2) - (bx - 1), Y0 = (qy >> 2) - (by - 1), dx = qx & 3, dy = qy & 3;
 #pragma unroll
-        for (int j = 0; j < (B * B + GT - 1) / GT; ++j) {
-            const int i = gt + j * GT;
-            if (i < B * B) {
-                const int x = i % B, y = i / B;
+            for (int j = 0; j < SPT; ++j) {
+                const int i = i0 + j * GT, x = i % B, y = i / B;
                 acc += absi((int)cur[y * 64 + x] - A.sample(X0 + x, Y0 + y, dx, dy));
             }
         }
-        const int sum = group_sum(S, g, gt, par, acc);
-        if (sum < bsad) { bsad = sum; mx = qx; my = qy; }
+        acc = (int)__reduce_add_sync(0xffffffffu, (unsigned)acc);   // kk is warp-uniform
+        if (lane == 0) part[wig * 8] = acc;
+        group_bar(g);
+        const int s0 = PPP == 2 ? part[0] + part[8] : part[0] + part[8] + part[16] + part[24];
+        const int s1 = part[16] + part[24];           // the pair's second point (8x8)
+        par ^= 1;
+        int found = -1, fs = 0;
+        if (s0 < bsad) { found = 0; fs = s0; }
+        else if (K > 1 && s1 < bsad) { found = 1; fs = s1; }
+        if (found < 0) {
+            p += K;
+            continue;
+        }
+        mx += c_qpel[p + found][0];
+        my += c_qpel[p + found][1];
+        bsad = fs;
+        p += found + 1;
     }
 }
 
