@@ -344,32 +344,47 @@ struct SadWindow {
     bool valid = false;
 };
 
+// The walk looks up a pass's remaining points all at once, lane p of every
+// warp taking point p, and a ballot finds the first one (in point order)
+// that improves on the running best or leaves the table: the sequential
+// walk's next event.  An improvement is committed and the points after it
+// are looked up around the new best; a point off the table refills the
+// table around the running best (as the sequential walk does on reaching
+// it) and the lookups start again from that point.  Every warp of the group
+// runs the same walk, so the refills stay group-uniform.
 __device__ void int_stage_windowed(Smem &S, int g, int gt, const uint8_t *ref, int s, int W, int H,
                                    const uint8_t *cur, int blk, int pat, int npts, int iters, SadWindow &win,
                                    int &bx, int &by, int &bsad) {
+    const int lane = gt & 31;
+    int ldx = 0, ldy = 0;   // this lane's pattern point (lanes 1..npts)
+    if (lane >= 1 && lane <= npts) pat_point(pat, lane, ldx, ldy);
     for (int it = 0; it < iters; ++it) {
         bool improved = false;
         int p0 = 1;
         while (p0 <= npts) {
-            int found = -1, fs = 0, fx = 0, fy = 0;
-            for (int p = p0; p <= npts; ++p) {
-                int dx, dy;
-                pat_point(pat, p, dx, dy);
-                const int x = bx + dx, y = by + dy;
-                const int R = win.R;
-                if (!win.valid || x < win.wx - R || x > win.wx + R || y < win.wy - R || y > win.wy + R) {
-                    win.buf ^= 1; win.wx = bx; win.wy = by; win.valid = true;
-                    if (blk == 16) fill_sad_window<16>(S, g, gt, win.buf, ref, s, W, H, cur, win.wx, win.wy, R);
-                    else fill_sad_window<8>(S, g, gt, win.buf, ref, s, W, H, cur, win.wx, win.wy, R);
-                }
+            const bool act = lane >= p0 && lane <= npts;
+            const int x = bx + ldx, y = by + ldy, R = win.R;
+            const bool off = !win.valid || x < win.wx - R || x > win.wx + R || y < win.wy - R || y > win.wy + R;
+            int v = 0x7FFFFFFF;
+            if (act && !off) {
                 const int *tab = (const int *)(S.pred[g] + WIN_OFF) + win.buf * WIN_NMAX * WIN_NMAX;
-                const int v = tab[(y - win.wy + R) * (2 * R + 1) + (x - win.wx + R)];
-                if (v < bsad) { found = p; fs = v; fx = dx; fy = dy; break; }
+                v = tab[(y - win.wy + R) * (2 * R + 1) + (x - win.wx + R)];
             }
-            if (found < 0) break;
-            bx += fx; by += fy; bsad = fs;
+            const unsigned ev = __ballot_sync(0xffffffffu, act && (off || v < bsad));
+            if (!ev) break;                       // no point of this pass improves
+            const int f = __ffs(ev) - 1;
+            if (__shfl_sync(0xffffffffu, (int)off, f)) {
+                win.buf ^= 1; win.wx = bx; win.wy = by; win.valid = true;
+                if (blk == 16) fill_sad_window<16>(S, g, gt, win.buf, ref, s, W, H, cur, win.wx, win.wy, R);
+                else fill_sad_window<8>(S, g, gt, win.buf, ref, s, W, H, cur, win.wx, win.wy, R);
+                p0 = f;                           // look point f up in the new table
+                continue;
+            }
+            bsad = __shfl_sync(0xffffffffu, v, f);
+            bx += __shfl_sync(0xffffffffu, ldx, f);
+            by += __shfl_sync(0xffffffffu, ldy, f);
             improved = true;
-            p0 = found + 1;
+            p0 = f + 1;
         }
         if (!improved) break;
     }
