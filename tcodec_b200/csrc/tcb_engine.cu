@@ -713,8 +713,12 @@ __device__ __noinline__ void build_refs(Smem &, const Leaf L, uint32_t mode_mask
         // the nm modes of `fill`, N*N samples each: sample i belongs to the
         // (i >> 2lg)-th set bit of fill
         const int lg = __ffs(N) - 1, npx = N * N, nm = __popc(fill);
+        // every mode but DC (the medium and slow presets' set): the k-th
+        // mode is k, or k + 1 past DC, with no bit search
+        const bool all = fill == ((1u << 18) - 1) - 2u;
         for (int i = threadIdx.x - 32; i < nm * npx; i += NT - 32) {
-            const int m = __fns(fill, 0, (i >> (2 * lg)) + 1), p = i & (npx - 1);
+            const int k = i >> (2 * lg);
+            const int m = all ? k + (k != 0) : __fns(fill, 0, k + 1), p = i & (npx - 1);
             S.ipred[m][p] = (uint8_t)intra_at(S.ra + 1, S.rl + 1, N, m, 0, p & (N - 1), p >> lg);
         }
     }
