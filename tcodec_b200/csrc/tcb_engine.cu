@@ -764,6 +764,7 @@ __device__ __noinline__ void luma_jobs8(Smem &, const Leaf L, const int *cl, int
     Smem &S = smem_state();
     const QuantParams &qp = S.qparam[0];
     const int cu = L.cu, ntu = cu >> 3, ntu2 = ntu * ntu, J = ncl * ntu2;
+    const int lt = lg2i(ntu);   // TU counts are powers of two: shifts, not divisions
     if (threadIdx.x == 0) OPCOUNT(2, J);
     const int hw = threadIdx.x >> 5, lane = threadIdx.x & 31, oct = lane >> 3, l8 = lane & 7;
     const int warp = (hw + NW - woff % NW) % NW;   // job rank of this warp
@@ -774,7 +775,7 @@ __device__ __noinline__ void luma_jobs8(Smem &, const Leaf L, const int *cl, int
         const int j = base + warp * 4 + oct;
         const bool act = j < J;
         const int jj = act ? j : 0;
-        const int k = jj / ntu2, t = jj - k * ntu2, ty = t / ntu, tx = t - ty * ntu;
+        const int k = jj >> (2 * lt), t = jj & (ntu2 - 1), ty = t >> lt, tx = t & (ntu - 1);
         const int slot = cl[k];
         const PredSrc ps = pred_src(S, slot);
         int res[8], pr[8];
@@ -829,6 +830,7 @@ __device__ __noinline__ void luma_jobs4(Smem &, const Leaf L, const int *cl, int
     Smem &S = smem_state();
     const QuantParams &qp = S.qparam[0];
     const int cu = L.cu, ntu = cu >> 3, ntu2 = ntu * ntu, per = ntu2 * 4, J = ncl * per;
+    const int lt = lg2i(ntu);   // TU counts are powers of two: shifts, not divisions
     if (threadIdx.x == 0) OPCOUNT(3, J);
     const int hw = threadIdx.x >> 5, lane = threadIdx.x & 31, qd = lane >> 2, l4 = lane & 3;
     const int warp = (hw + NW - woff % NW) % NW;   // job rank of this warp
@@ -838,8 +840,8 @@ __device__ __noinline__ void luma_jobs4(Smem &, const Leaf L, const int *cl, int
         const int j = base + warp * 8 + qd;
         const bool act = j < J;
         const int jj = act ? j : 0;
-        const int k = jj / per, rem = jj - k * per, t = rem >> 2, q = rem & 3;
-        const int ty = t / ntu, tx = t - ty * ntu;
+        const int k = jj >> (2 * lt + 2), rem = jj & (per - 1), t = rem >> 2, q = rem & 3;
+        const int ty = t >> lt, tx = t & (ntu - 1);
         const int sx = tx * 8 + (q & 1) * 4, sy = ty * 8 + (q & 2) * 2;
         const int slot = cl[k];
         const PredSrc ps = pred_src(S, slot);
@@ -892,6 +894,7 @@ __device__ __noinline__ void chroma_jobs(Smem &, const Leaf L, int nopt, int cba
     Smem &S = smem_state();
     const QuantParams &qp = S.qparam[1];
     const int cs = L.cu >> 1, nt = cs >> 2, nt2 = nt * nt, per = 2 * nt2, J = nopt * per;
+    const int ln = lg2i(nt);    // TU counts are powers of two: shifts, not divisions
     if (threadIdx.x == 0) OPCOUNT(3, J);
     const int lxc = L.lx >> 1, lyc = L.ly >> 1;
     const int hw = threadIdx.x >> 5, lane = threadIdx.x & 31, qd = lane >> 2, l4 = lane & 3;
@@ -901,8 +904,8 @@ __device__ __noinline__ void chroma_jobs(Smem &, const Leaf L, int nopt, int cba
         const int j = base + warp * 8 + qd;
         const bool act = j < J;
         const int jj = act ? j : 0;
-        const int o = jj / per, rem = jj - o * per, c = rem / nt2, t = rem - c * nt2;
-        const int ty = t / nt, tx = t - ty * nt;
+        const int o = jj >> (2 * ln + 1), rem = jj & (per - 1), c = rem >> (2 * ln), t = rem & (nt2 - 1);
+        const int ty = t >> ln, tx = t & (nt - 1);
         const uint8_t *pr = S.cpred[cbase + 2 * o + c];
         const uint8_t *org = S.cur_c[c];
         int res[4];
