@@ -160,6 +160,9 @@ __device__ __forceinline__ void pat_point(int pat, int p, int &dx, int &dy) {
 }
 
 __device__ __forceinline__ int lg2i(int v) { return 31 - __clz(v); }
+// i / d for d > 0, by a shift when d is a power of two (full CTU rows and
+// tiles: 64, 32), else by division (partial CTUs at the frame edge).
+__device__ __forceinline__ int div_p2(int i, int d) { return (d & (d - 1)) == 0 ? i >> lg2i(d) : i / d; }
 
 // SADs of the K <= 7 integer candidates base + pat[p0 + k] * scale, k < K,
 // on the 128 threads of group g; every thread ends with all K values in
@@ -950,7 +953,7 @@ __device__ __noinline__ void chroma_dc_pred(Smem &, const Leaf L, int dst) {
         }
         sum = __reduce_add_sync(0xffffffffu, sum);
         const int n = (ha ? cs : 0) + (hl ? cs : 0);
-        if (lane == 0) S.sao[c] = n ? (sum + n / 2) / n : 128;
+        if (lane == 0) S.sao[c] = n ? (sum + n / 2) >> lg2i(n) : 128;   // n: cs or 2 cs
     }
     SYNC();
     const int lg2 = 2 * lg2i(cs);
@@ -1840,19 +1843,23 @@ __device__ __noinline__ void sao_tile(Smem &, int w, int h, int lambda_sao) {
     }
     SYNC();
     for (int i = threadIdx.x; i < w * h; i += NT) {
-        const int y = i / w, x = i - y * w;
+        const int y = div_p2(i, w), x = i - y * w;
         const int o = S.cur_y[y * 64 + x], r = RY(S, x, y), d = o - r, b = r >> 3;
         atomicAdd(&S.band_sum[b], d);
         atomicAdd(&S.band_cnt[b], 1);
         atomicAdd(&S.band_sq[b], d * d);
     }
     SYNC();
+    // each band's candidate offset once (rounded mean of o - r, within +-7)
+    if (threadIdx.x < 32) {
+        const int cnt = S.band_cnt[threadIdx.x], sum = S.band_sum[threadIdx.x];
+        S.band_cand[threadIdx.x] = cnt ? clampi((sum + (sum >= 0 ? cnt / 2 : -(cnt / 2))) / cnt, -7, 7) : 0;
+    }
+    SYNC();
     for (int i = threadIdx.x; i < w * h; i += NT) {
-        const int y = i / w, x = i - y * w;
+        const int y = div_p2(i, w), x = i - y * w;
         const int o = S.cur_y[y * 64 + x], r = RY(S, x, y), b = r >> 3;
-        const int cnt = S.band_cnt[b], sum = S.band_sum[b];
-        int cand = (sum + (sum >= 0 ? cnt / 2 : -(cnt / 2))) / cnt;
-        cand = clampi(cand, -7, 7);
+        const int cand = S.band_cand[b];
         if (cand) {
             const int d = o - clampi(r + cand, 0, 255);
             atomicAdd(&S.band_new[b], d * d);
@@ -1865,10 +1872,7 @@ __device__ __noinline__ void sao_tile(Smem &, int w, int h, int lambda_sao) {
         long long best = base;
         int bb = 0, bo = 0;
         for (int b = 0; b < 32; ++b) {
-            const int cnt = S.band_cnt[b];
-            if (!cnt) continue;
-            const int sum = S.band_sum[b];
-            int cand = clampi((sum + (sum >= 0 ? cnt / 2 : -(cnt / 2))) / cnt, -7, 7);
+            const int cand = S.band_cand[b];   // 0 for an empty band
             if (!cand) continue;
             const long long sse = base - S.band_sq[b] + S.band_new[b];
             if (sse < best) { best = sse; bb = b; bo = cand; }
@@ -1881,7 +1885,7 @@ __device__ __noinline__ void sao_tile(Smem &, int w, int h, int lambda_sao) {
     if (S.sao[0]) {
         const int band = S.sao[1], off = S.sao[2];
         for (int i = threadIdx.x; i < w * h; i += NT) {
-            const int y = i / w, x = i - y * w;
+            const int y = div_p2(i, w), x = i - y * w;
             uint8_t &p = RY(S, x, y);
             if ((p >> 3) == band) p = (uint8_t)clampi(p + off, 0, 255);
         }
@@ -1968,11 +1972,11 @@ __device__ void encode_ctu(Smem &S, const FrameParams &P, int row, int col) {
     PHASE(10);
     // ---- exports --------------------------------------------------------
     for (int i = threadIdx.x; i < w * h; i += NT) {
-        const int y = i / w, x = i - y * w;
+        const int y = div_p2(i, w), x = i - y * w;
         P.rec_y[(size_t)(ctu_y + y) * P.stride_y + ctu_x + x] = RY(S, x, y);
     }
     for (int i = threadIdx.x; i < 2 * wc * hc; i += NT) {
-        const int c = i / (wc * hc), p = i - c * wc * hc, y = p / wc, x = p - y * wc;
+        const int c = div_p2(i, wc * hc), p = i - c * wc * hc, y = div_p2(p, wc), x = p - y * wc;
         uint8_t *dst = c ? P.rec_cr : P.rec_cb;
         dst[(size_t)((ctu_y >> 1) + y) * P.stride_c + (ctu_x >> 1) + x] = RC(S, c, x, y);
     }
@@ -2561,18 +2565,18 @@ decode_kernel(const FrameParams *__restrict__ params, const int *__restrict__ it
     if (rec->sao_has) {
         const int band = clampi(rec->sao_band, 0, 31), off = clampi(rec->sao_offset, -7, 7);
         for (int i = threadIdx.x; i < w * h; i += NT) {
-            const int y = i / w, x = i - y * w;
+            const int y = div_p2(i, w), x = i - y * w;
             uint8_t &p = RY(S, x, y);
             if ((p >> 3) == band) p = (uint8_t)clampi(p + off, 0, 255);
         }
         SYNC();
     }
     for (int i = threadIdx.x; i < w * h; i += NT) {
-        const int y = i / w, x = i - y * w;
+        const int y = div_p2(i, w), x = i - y * w;
         P.rec_y[(size_t)(ctu_y + y) * P.stride_y + ctu_x + x] = RY(S, x, y);
     }
     for (int i = threadIdx.x; i < 2 * wc * hc; i += NT) {
-        const int c = i / (wc * hc), p = i - c * wc * hc, y = p / wc, x = p - y * wc;
+        const int c = div_p2(i, wc * hc), p = i - c * wc * hc, y = div_p2(p, wc), x = p - y * wc;
         uint8_t *dst = c ? P.rec_cr : P.rec_cb;
         dst[(size_t)((ctu_y >> 1) + y) * P.stride_c + (ctu_x >> 1) + x] = RC(S, c, x, y);
     }

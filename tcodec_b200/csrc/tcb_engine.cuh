@@ -77,7 +77,7 @@ struct Smem {
     uint8_t dc_u8;             // S.dc as a one-byte prediction source (PredSrc)
     long long best_cost;
     int sao[3];
-    int band_sum[32], band_cnt[32], band_sq[32], band_new[32];
+    int band_sum[32], band_cnt[32], band_sq[32], band_new[32], band_cand[32];
     int ncoef;
     unsigned long long tu8mask;
 };
