@@ -192,7 +192,7 @@ __device__ __forceinline__ int tu8_code(int l8, const int res_row[8], int *scr,
 #pragma unroll
     for (int i = 0; i < 8; ++i) col[i] = scr[i * 9 + l8];
     __syncwarp();
-    int nz = 0, last = -1;
+    int nz = 0, last = -1, lball = 0;
     int cs8[8];
     fdct8_sums(col, cs8);
 #pragma unroll
@@ -202,14 +202,16 @@ __device__ __forceinline__ int tu8_code(int l8, const int res_row[8], int *scr,
         const int q = (int16_t)quant_rdoq(c, band_rc<8>(k, l8), qp);
         q_col[k] = q;
         if (q) { ++nz; last = pos; }
+        lball += level_bits(q);
     }
-    nz = oct_sum(nz);
+    // The level bits of positions up to `last` are those of all 64 less one
+    // per zero past it (level_bits(0) == 1), so they need not wait for
+    // `last`: one packed sum (level bits << 8 | nonzero count, at most 2048
+    // and 64) and one max, side by side.
+    const int packed = oct_sum((lball << 8) | nz);
     last = oct_max(last);
-    int lb = 0;
-#pragma unroll
-    for (int k = 0; k < 8; ++k)
-        if (k * 8 + l8 <= last) lb += level_bits(q_col[k]);
-    lb = oct_sum(lb);
+    nz = packed & 0xFF;
+    const int lb = (packed >> 8) - (63 - last);
     const int bits = 1 + 2 * nz + lb + lastpos_cost(last);
     // Dequantise and hand columns back as rows for the inverse row pass.
 #pragma unroll
@@ -248,7 +250,7 @@ __device__ __forceinline__ int tu4_code(int l4, const int res_row[4], int *scr,
 #pragma unroll
     for (int i = 0; i < 4; ++i) col[i] = scr[i * 5 + l4];
     __syncwarp();
-    int nz = 0, last = -1;
+    int nz = 0, last = -1, lball = 0;
     int cs4[4];
     fdct4_sums(col, cs4);
 #pragma unroll
@@ -258,14 +260,13 @@ __device__ __forceinline__ int tu4_code(int l4, const int res_row[4], int *scr,
         const int q = (int16_t)quant_rdoq(c, band_rc<4>(k, l4), qp);
         q_col[k] = q;
         if (q) { ++nz; last = pos; }
+        lball += level_bits(q);
     }
-    nz = quad_sum(nz);
+    // as in tu8_code: all 16 level bits less one per zero past `last`
+    const int packed = quad_sum((lball << 8) | nz);
     last = quad_max(last);
-    int lb = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-        if (k * 4 + l4 <= last) lb += level_bits(q_col[k]);
-    lb = quad_sum(lb);
+    nz = packed & 0xFF;
+    const int lb = (packed >> 8) - (15 - last);
     const int bits = 1 + 2 * nz + lb + lastpos_cost(last);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
