@@ -123,16 +123,23 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
 
 def make_config(lib: ctypes.CDLL, width: int, height: int, qp: int = 32, preset: int = PRESET_MEDIUM,
                 profile: int = 0, keyframe_interval: int = 30, entropy: bool = True,
-                b_frames: bool = False, crc: bool = False) -> Config:
-    """tc_config_defaults + the fields `tcenc --v2` sets (reference
-    tools/tcenc.c:127-185)."""
+                b_frames: bool = False, crc: bool = False, version: int = 2, threads: int = 0) -> Config:
+    """tc_config_defaults + the fields `tcenc` sets (reference
+    tools/tcenc.c:127-185): `version` 2 is `--v2` (quadtree syntax), 0 and 1
+    are `--bs-version 0/1` (legacy 8x8 block syntax); `threads` 0 is the
+    default worker count, which lays legacy rows out as separate runs."""
     cfg = Config()
     lib.tc_config_defaults(ctypes.byref(cfg), width, height)
     cfg.preset = preset
     cfg.qp = qp
     cfg.keyframe_interval = keyframe_interval
     cfg.profile = profile
-    cfg.use_v2 = 1
+    cfg.threads = threads
+    if version == 2:
+        cfg.use_v2 = 1
+    else:
+        cfg.use_v2 = 0
+        cfg.bitstream_version = version
     cfg.enable_entropy_coded = 1 if entropy else 0
     cfg.enable_b_frames = 1 if b_frames else 0
     cfg.enable_crc = 1 if crc else 0

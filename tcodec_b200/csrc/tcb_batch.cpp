@@ -465,6 +465,8 @@ tcb_batch_t *tcb_batch_create(const tc_config_t *configs, int n) {
     if (!configs || n <= 0 || n > MAX_STREAMS) return nullptr;
     tcb_batch *b = batch_new(n);
     if (!b) return nullptr;
+    for (int s = 0; s < n; ++s)
+        if (!configs[s].use_v2) { release(b); return nullptr; }   // batches run the v2 CTU engine
     for (int s = 0; s < n; ++s) {
         tc_encoder_t *e = tc_encoder_create(&configs[s]);
         if (!e || batch_attach(b, e) != s) {

@@ -319,6 +319,90 @@ struct Parser {
     }
 };
 
+// Legacy (v0 / v1) block syntax of one CTU (reference src/decoder.c:260-440
+// and 486-552, the parse side of decode_block): fills the records the
+// reconstruction kernel reads, motion vectors made absolute with the
+// median of the left, above and above-right blocks inside the CTU.  Blocks
+// outside the frame are not coded and count as inter blocks with a zero
+// vector (the reference's zeroed block info).
+void parse_legacy_ctu(Parser &p, legacy::LBlock *blk, int ox, int oy, int W, int H, int ft) {
+    uint8_t inter[legacy::BLOCKS];
+    int mvx[legacy::BLOCKS], mvy[legacy::BLOCKS];
+    for (int i = 0; i < legacy::BLOCKS; ++i) { inter[i] = 1; mvx[i] = 0; mvy[i] = 0; }
+    auto med = [](int a, int b, int c) {
+        if (a > b) std::swap(a, b);
+        if (b > c) std::swap(b, c);
+        if (a > b) std::swap(a, b);
+        return b;
+    };
+    for (int b = 0; b < legacy::BLOCKS; ++b) {
+        legacy::LBlock &k = blk[b];
+        k.coded = 0;
+        const int bx = b & 7, by = b >> 3, fx = ox + bx * 8, fy = oy + by * 8;
+        if (fx + 8 > W || fy + 8 > H) continue;
+        k.coded = 1;
+        const int mode = ft != 0 ? (int)p.bits(CTX_BLOCK_MODE, 2) : 2;
+        const bool intra = mode == 2, merge = mode == 3;
+        int bmx = 0, bmy = 0, ref = 0;
+        k.intra_mode = 1;
+        if (intra) {
+            uint32_t im = p.bits(CTX_INTRA_MODE, 5);
+            if (im >= 18) im = 1;
+            k.intra_mode = (uint8_t)im;
+        } else {
+            int ref_sel = 0;
+            if (ft == 2) {
+                ref_sel = (int)p.bits(CTX_REF_SEL, 2);
+                if (ref_sel > 2) ref_sel = 1;
+            }
+            int px = fx * 4, py = fy * 4;
+            int ax = 0, ay = 0, bvx = 0, bvy = 0, cvx = 0, cvy = 0;
+            bool ha = false, hb = false, hc = false;
+            if (bx > 0 && inter[b - 1]) { ax = mvx[b - 1]; ay = mvy[b - 1]; ha = true; }
+            if (by > 0 && inter[b - 8]) { bvx = mvx[b - 8]; bvy = mvy[b - 8]; hb = true; }
+            if (by > 0 && bx < 7 && inter[b - 7]) { cvx = mvx[b - 7]; cvy = mvy[b - 7]; hc = true; }
+            if (ha || hb || hc) {
+                if (!ha) { ax = hb ? bvx : cvx; ay = hb ? bvy : cvy; }
+                if (!hb) { bvx = ha ? ax : cvx; bvy = ha ? ay : cvy; }
+                if (!hc) { cvx = ha ? ax : bvx; cvy = ha ? ay : bvy; }
+                px = med(ax, bvx, cvx);
+                py = med(ay, bvy, cvy);
+            }
+            if (merge) {
+                bmx = px; bmy = py;
+                ref = ft == 2 ? ref_sel : 0;
+            } else {
+                int ri = 0;
+                if (ft == 1) {
+                    ri = (int)p.bits(CTX_REF_IDX, 2);
+                    if (ri >= TC_REF_FRAMES) ri = 0;
+                } else if (ft == 2) {
+                    ri = ref_sel;
+                }
+                const int dx = p.se(CTX_MVD_X), dy = p.se(CTX_MVD_Y);
+                bmx = dx + px; bmy = dy + py;
+                ref = ri;
+            }
+        }
+        k.mode = (uint8_t)mode;
+        k.ref = (uint8_t)ref;
+        k.mvd_x = bmx;
+        k.mvd_y = bmy;
+        k.tid = 0;
+        if (mode == 1 || mode == 2) {
+            k.tid = (uint8_t)p.bits(CTX_DCT_SIZE, 2);
+            if (k.tid & 2) p.coeffs(k.luma, 64, false, false);
+            else for (int q = 0; q < 4; ++q) p.coeffs(k.luma + 16 * q, 16, true, false);
+        }
+        p.coeffs(k.chroma, 16, true, false);
+        p.coeffs(k.chroma + 16, 16, true, false);
+        inter[b] = intra ? 0 : 1;
+        mvx[b] = intra ? 0 : bmx;
+        mvy[b] = intra ? 0 : bmy;
+        if (p.bs->error) return;
+    }
+}
+
 struct Header {
     int version = 0, W = 0, H = 0, flags = 0, qp = 0, frame_num = 0, tools = 0;
     int profile = 0, level = 0, has_crc = 0, has_ext = 0, frame_type = 0;
@@ -377,6 +461,11 @@ struct DecImpl {
     int dpb_poc[TC_REF_FRAMES] = {-1, -1, -1, -1};
     std::vector<DevFrame> spare;      // free device frames
     CtuOut *d_rec = nullptr, *h_rec = nullptr;
+    // Legacy (v0 / v1) streams: block records and the wavefront of
+    // diagonals c + 2r (see tcb_legacy.cu).
+    legacy::LBlock *d_lblk = nullptr, *h_lblk = nullptr;
+    int *d_litems = nullptr;
+    std::vector<int> ldiag_off, ldiag_cnt;
     FrameParams *d_params = nullptr;
     int *d_items = nullptr;
     std::vector<int> diag_off, diag_cnt;
@@ -409,6 +498,8 @@ struct DecImpl {
         for (int i = 0; i < TC_REF_FRAMES; ++i) { dpb_ok[i] = 0; dpb_poc[i] = -1; }
         cudaFree(d_rec); cudaFreeHost(h_rec); cudaFree(d_items);
         d_rec = nullptr; h_rec = nullptr; d_items = nullptr;
+        cudaFree(d_lblk); cudaFreeHost(h_lblk); cudaFree(d_litems);
+        d_lblk = nullptr; h_lblk = nullptr; d_litems = nullptr;
         tcb_host_frame_free(out);
         out = nullptr;
     }
@@ -443,6 +534,21 @@ struct DecImpl {
         }
         if (dev_alloc(&d_items, sizeof(int) * items.size()) != cudaSuccess) return false;
         cudaMemcpy(d_items, items.data(), sizeof(int) * items.size(), cudaMemcpyHostToDevice);
+        std::vector<int> litems;
+        ldiag_off.clear(); ldiag_cnt.clear();
+        for (int d = 0; d < cols + 2 * (rows - 1); ++d) {
+            ldiag_off.push_back((int)litems.size());
+            for (int r = 0; r < rows; ++r) {
+                const int c = d - 2 * r;
+                if (c >= 0 && c < cols) litems.push_back((r << 10) | c);
+            }
+            ldiag_cnt.push_back((int)litems.size() - ldiag_off.back());
+        }
+        if (dev_alloc(&d_litems, sizeof(int) * litems.size()) != cudaSuccess) return false;
+        cudaMemcpy(d_litems, litems.data(), sizeof(int) * litems.size(), cudaMemcpyHostToDevice);
+        const size_t nblk = (size_t)cols * rows * legacy::BLOCKS;
+        if (dev_alloc(&d_lblk, sizeof(legacy::LBlock) * nblk) != cudaSuccess) return false;
+        if (pinned_alloc(&h_lblk, sizeof(legacy::LBlock) * nblk) != cudaSuccess) return false;
         out = tcb_host_frame_alloc(w, h, 1);
         return out != nullptr;
     }
@@ -460,6 +566,7 @@ struct DecImpl {
     }
     tc_error_t decode(const uint8_t *data, size_t size, const tc_pixel_t **y, int *ys, const tc_pixel_t **cb,
                       int *cbs, const tc_pixel_t **cr, int *crs);
+    tc_error_t legacy_body(const uint8_t *data, size_t size, Reader &bs, const Header &hdr);
     tc_error_t emit(tc_frame_buf_t *f, const tc_pixel_t **y, int *ys, const tc_pixel_t **cb, int *cbs,
                     const tc_pixel_t **cr, int *crs) {
         if (y) *y = f->y;
@@ -502,9 +609,9 @@ tc_error_t DecImpl::decode(const uint8_t *data, size_t size, const tc_pixel_t **
     Header hdr;
     tc_error_t err = read_header(bs, hdr);
     if (err != TC_OK) return err;
-    // This library decodes the v2 quadtree bitstream only.
-    if (hdr.version != TC_VERSION_V2) return TC_ERR_BITSTREAM;
+    const bool legacy_stream = hdr.version != TC_VERSION_V2;
     if ((hdr.W & 1) || (hdr.H & 1)) return TC_ERR_BITSTREAM;
+    if (legacy_stream && (hdr.tools & TC_TOOL_ENTRY_POINTS)) return TC_ERR_BITSTREAM;
     if (W == 0 || H == 0) { W = hdr.W; H = hdr.H; }
     if (!cur.y || fw != hdr.W || fh != hdr.H)
         if (!setup(hdr.W, hdr.H)) return TC_ERR_MEMORY;
@@ -517,14 +624,20 @@ tc_error_t DecImpl::decode(const uint8_t *data, size_t size, const tc_pixel_t **
             crc_valid = 0;
         }
     }
-    if (hdr.flags & TC_FLAG_WPP) return TC_ERR_BITSTREAM;
-    entropy = (hdr.tools & TC_TOOL_ENTROPY_CODED) ? 1 : 0;
+    if (!legacy_stream && (hdr.flags & TC_FLAG_WPP)) return TC_ERR_BITSTREAM;
+    entropy = (hdr.version != TC_VERSION_V0 && (hdr.tools & TC_TOOL_ENTROPY_CODED)) ? 1 : 0;
     bs.align();
     if (hdr.frame_type == 0 && hdr.frame_num > 0)
         for (int i = 0; i < TC_REF_FRAMES; ++i) {
             if (dpb_ok[i]) spare.push_back(dpb[i]);
             dpb_ok[i] = 0; dpb_poc[i] = -1; dpb[i] = DevFrame();
         }
+    uint64_t t_parse1 = 0;
+    if (legacy_stream) {
+        const tc_error_t le = legacy_body(data, size, bs, hdr);
+        if (le != TC_OK) return le;
+        t_parse1 = now_ns();
+    } else {
     // ---- parse every CTU into its record ------------------------------
     const int multiref_tool = (hdr.tools & TC_TOOL_MULTI_REF) != 0;
     const int sao_tool = (hdr.tools & TC_TOOL_SAO) != 0;
@@ -600,7 +713,7 @@ tc_error_t DecImpl::decode(const uint8_t *data, size_t size, const tc_pixel_t **
         if (entropy) rc.init(&bs);
         if (!parse_rows(bs, entropy ? &rc : nullptr, ctx, 0, rows)) return TC_ERR_BITSTREAM;
     }
-    const uint64_t t_parse1 = now_ns();
+    t_parse1 = now_ns();
     // ---- device reconstruction ------------------------------------------
     FrameParams P;
     memset(&P, 0, sizeof(P));
@@ -632,6 +745,7 @@ tc_error_t DecImpl::decode(const uint8_t *data, size_t size, const tc_pixel_t **
     for (size_t d = 0; d < diag_off.size(); ++d)
         if (launch_decode_items(d_params, d_items + diag_off[d], diag_cnt[d], st) != cudaSuccess)
             return TC_ERR_INTERNAL;
+    }   // v2 stream
     // DPB: slot 3 falls out and its buffer takes a copy of the
     // reconstruction into slot 0 (another buffer when slot 3 is empty, taken
     // before anything moves, so a failed allocation leaves the DPB as it
@@ -675,6 +789,72 @@ tc_error_t DecImpl::decode(const uint8_t *data, size_t size, const tc_pixel_t **
         return pop_display(y, ys, cb, cbs, cr, crs);
     }
     return emit(out, y, ys, cb, cbs, cr, crs);
+}
+
+// Legacy stream body: rows as per-row runs behind a 16-bit entry table
+// (TC_FLAG_WPP) or one run, raw or range coded; parse on the host, then
+// the legacy CTU wavefront reconstructs into `cur`, whose previous contents
+// (the last decoded frame) stand in for samples not yet decoded, as in the
+// reference decoder (src/decoder.c:2620-2770, 652-683).
+tc_error_t DecImpl::legacy_body(const uint8_t *data, size_t size, Reader &bs, const Header &hdr) {
+    if (upload_legacy_tables() != cudaSuccess) return TC_ERR_INTERNAL;
+    const int ft = hdr.frame_type;
+    const size_t nblk = (size_t)cols * rows * legacy::BLOCKS;
+    uint8_t ctx[TC_NUM_CONTEXTS_RC];
+    memset(ctx, 0, sizeof(ctx));
+    bool bad = false;
+    if (hdr.flags & TC_FLAG_WPP) {
+        const uint32_t noff = bs.bits(16);
+        if (bs.error || noff > 63 || (int)noff != rows - 1) return TC_ERR_BITSTREAM;
+        size_t off[64];
+        off[0] = 0;
+        for (uint32_t i = 0; i < noff; ++i) off[i + 1] = bs.bits(16);
+        if (bs.error) return TC_ERR_BITSTREAM;
+        bs.align();
+        const size_t start = bs.pos;
+        for (int r = 0; r < rows; ++r)
+            if (start + off[r] > size || (r > 0 && off[r] < off[r - 1])) return TC_ERR_BITSTREAM;
+        for (int r = 0; r < rows && !bad; ++r) {
+            const size_t b0 = start + off[r], b1 = r + 1 < rows ? start + off[r + 1] : size;
+            Reader rr;
+            rr.init(data + b0, b1 - b0);
+            Parser p{&rr, nullptr, ctx, fw, fh, ft, 0, 0, dpb_ok, nullptr, 0, 0, 0};
+            for (int c = 0; c < cols && !bad; ++c) {
+                parse_legacy_ctu(p, h_lblk + (size_t)(r * cols + c) * legacy::BLOCKS, c * 64, r * 64, fw, fh, ft);
+                bad = rr.error != 0;
+            }
+        }
+    } else {
+        RDec rc;
+        if (entropy) rc.init(&bs);
+        Parser p{&bs, entropy ? &rc : nullptr, ctx, fw, fh, ft, 0, 0, dpb_ok, nullptr, 0, 0, 0};
+        for (int r = 0; r < rows && !bad; ++r)
+            for (int c = 0; c < cols && !bad; ++c) {
+                parse_legacy_ctu(p, h_lblk + (size_t)(r * cols + c) * legacy::BLOCKS, c * 64, r * 64, fw, fh, ft);
+                bad = bs.error != 0;
+            }
+    }
+    if (bad) return TC_ERR_BITSTREAM;
+    legacy::LFrame F;
+    memset(&F, 0, sizeof(F));
+    F.W = fw; F.H = fh; F.sy = sy; F.sc = sc; F.ctu_cols = cols; F.ctu_rows = rows;
+    F.rec_y = cur.y; F.rec_cb = cur.cb; F.rec_cr = cur.cr;
+    int fp = -1, bp = 0x7FFFFFFF;
+    for (int i = 0; i < TC_REF_FRAMES; ++i) {
+        F.dpb_y[i] = dpb_ok[i] ? dpb[i].y : nullptr;
+        if (!dpb_ok[i] || dpb_poc[i] < 0) continue;
+        if (dpb_poc[i] < hdr.frame_num && dpb_poc[i] > fp) { fp = dpb_poc[i]; F.fwd_y = dpb[i].y; }
+        if (dpb_poc[i] > hdr.frame_num && dpb_poc[i] < bp) { bp = dpb_poc[i]; F.bwd_y = dpb[i].y; }
+    }
+    F.frame_type = ft;
+    F.qp = hdr.qp;
+    F.blocks = d_lblk;
+    if (cudaMemcpyAsync(d_lblk, h_lblk, sizeof(legacy::LBlock) * nblk, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return TC_ERR_INTERNAL;
+    for (size_t d = 0; d < ldiag_off.size(); ++d)
+        if (launch_legacy_ctus(F, d_litems + ldiag_off[d], ldiag_cnt[d], false, st) != cudaSuccess)
+            return TC_ERR_INTERNAL;
+    return TC_OK;
 }
 
 }  // namespace tcb

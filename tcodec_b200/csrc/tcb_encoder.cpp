@@ -180,6 +180,29 @@ bool EncImpl::init(const tc_config_t &c) {
     CK(dmalloc(&d_items, sizeof(int) * items.size()));
     CK(cudaMemcpy(d_items, items.data(), sizeof(int) * items.size(), cudaMemcpyHostToDevice));
     for (int i = 0; i < TC_REF_FRAMES; ++i) { dpb_slot[i] = -1; dpb_poc[i] = -1; }
+    if (!c.use_v2) {
+        // Legacy 8x8 block path: records, wavefront of diagonals c + 2r,
+        // and the row layout (reference src/encoder.c:2495-2506: rows as
+        // separate runs when there are several rows and threads and no
+        // range coder).
+        legacy = true;
+        const int threads = c.threads > 0 ? c.threads : 4;
+        legacy_wpp = ctu_rows > 1 && threads > 1 && !c.enable_entropy_coded;
+        CK(upload_legacy_tables());
+        CK(dmalloc(&d_lblk, sizeof(legacy::LBlock) * (size_t)nctu * legacy::BLOCKS));
+        CK(pinned_alloc(&h_lblk, sizeof(legacy::LBlock) * (size_t)nctu * legacy::BLOCKS));
+        std::vector<int> litems;
+        for (int d = 0; d < ctu_cols + 2 * (ctu_rows - 1); ++d) {
+            ldiag_off.push_back((int)litems.size());
+            for (int r = 0; r < ctu_rows; ++r) {
+                const int col = d - 2 * r;
+                if (col >= 0 && col < ctu_cols) litems.push_back((r << 10) | col);
+            }
+            ldiag_cnt.push_back((int)litems.size() - ldiag_off.back());
+        }
+        CK(dmalloc(&d_litems, sizeof(int) * litems.size()));
+        CK(cudaMemcpy(d_litems, litems.data(), sizeof(int) * litems.size(), cudaMemcpyHostToDevice));
+    }
     out_buf_size = (size_t)W * H * 3;
     out_buf = (uint8_t *)calloc(out_buf_size, 1);
     if (!out_buf) return false;
@@ -220,6 +243,7 @@ void EncImpl::release() {
     free(out_buf);
     free(out_buf_alt);
     cudaFreeHost(h_out_alt);
+    dfree(d_lblk); cudaFreeHost(h_lblk); cudaFreeHost(h_lblk_alt); dfree(d_litems);
 }
 
 int EncImpl::free_pool_slot() const {
@@ -339,6 +363,7 @@ tc_error_t EncImpl::stage_b() {
     // ---- device frame parameters ------------------------------------------
     const int rs = free_pool_slot();
     if (rs < 0) return TC_ERR_INTERNAL;
+    if (legacy) return stage_b_legacy(is_key, frame_type, qp, rs);
     const DevFrame rec = pool[rs];
     FrameParams &P = h_params;
     memset(&P, 0, sizeof(P));
@@ -395,7 +420,69 @@ tc_error_t EncImpl::stage_b() {
     return TC_OK;
 }
 
+// Legacy frame parameters (reference src/encoder.c:1648-1677 candidate
+// references, 1646-1648 search range, 1846 lambda).
+tc_error_t EncImpl::stage_b_legacy(int is_key, int frame_type, int qp, int rs) {
+    const DevFrame rec = pool[rs];
+    legacy::LFrame &F = lframe;
+    memset(&F, 0, sizeof(F));
+    F.W = W; F.H = H; F.sy = sy; F.sc = sc; F.ctu_cols = ctu_cols; F.ctu_rows = ctu_rows;
+    F.cur_y = cur.y; F.cur_cb = cur.cb; F.cur_cr = cur.cr;
+    F.rec_y = rec.y; F.rec_cb = rec.cb; F.rec_cr = rec.cr;
+    for (int i = 0; i < TC_REF_FRAMES; ++i) F.dpb_y[i] = dpb_slot[i] >= 0 ? pool[dpb_slot[i]].y : nullptr;
+    if (frame_type == 2) {
+        // Forward: the largest POC below this frame's; backward: the
+        // smallest above (reference src/encoder.c:204-228).
+        int fp = -1, bp = 0x7FFFFFFF;
+        for (int i = 0; i < TC_REF_FRAMES; ++i) {
+            const int sl = dpb_slot[i], p = dpb_poc[i];
+            if (sl < 0 || p < 0) continue;
+            if (p < pend.poc && p > fp) { fp = p; F.fwd_y = pool[sl].y; }
+            if (p > pend.poc && p < bp) { bp = p; F.bwd_y = pool[sl].y; }
+        }
+        if (F.fwd_y) { F.cand_y[F.n_cand] = F.fwd_y; F.cand_sel[F.n_cand] = 0; F.n_cand++; }
+        if (F.bwd_y) { F.cand_y[F.n_cand] = F.bwd_y; F.cand_sel[F.n_cand] = 1; F.n_cand++; }
+    } else if (frame_type == 1) {
+        const int max_refs = (cfg.preset == TC_PRESET_SLOW && cfg.profile >= TC_PROFILE_STREAMING_MAIN) ? TC_REF_FRAMES : 1;
+        for (int ri = 0; ri < max_refs && F.n_cand < 2; ++ri)
+            if (dpb_slot[ri] >= 0) { F.cand_y[F.n_cand] = pool[dpb_slot[ri]].y; F.cand_sel[F.n_cand] = ri; F.n_cand++; }
+    }
+    F.frame_type = frame_type;
+    F.qp = qp;
+    F.search_range = cfg.preset == TC_PRESET_ULTRAFAST ? 16 : (cfg.preset == TC_PRESET_SLOW ? 64 : 32);
+    F.lambda = tc_lambda_host(qp);
+    F.blocks = d_lblk;
+    pend.glob = 0;
+    pend.is_key = is_key;
+    pend.frame_type = frame_type;
+    pend.qp = qp;
+    pend.rs = rs;
+    pend.multiref = 0;
+    return TC_OK;
+}
+
+// The new reconstruction starts as a copy of the previous one, then the
+// legacy CTU wavefront runs one diagonal per launch.
+tc_error_t EncImpl::launch_legacy() {
+    const DevFrame rec = pool[pend.rs];
+    if (timing) cudaEventRecord(ev0, st);
+    if (prev_rs >= 0 && prev_rs != pend.rs) {
+        const DevFrame &pv = pool[prev_rs];
+        if (cudaMemcpyAsync(rec.y, pv.y, (size_t)sy * H, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+            cudaMemcpyAsync(rec.cb, pv.cb, (size_t)sc * (H / 2), cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+            cudaMemcpyAsync(rec.cr, pv.cr, (size_t)sc * (H / 2), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            return TC_ERR_INTERNAL;
+    }
+    for (size_t d = 0; d < ldiag_off.size(); ++d)
+        if (launch_legacy_ctus(lframe, d_litems + ldiag_off[d], ldiag_cnt[d], true, st) != cudaSuccess)
+            return TC_ERR_INTERNAL;
+    kernel_launches += (long long)ldiag_off.size();
+    if (timing) cudaEventRecord(ev1, st);
+    return TC_OK;
+}
+
 tc_error_t EncImpl::launch_own() {
+    if (legacy) return launch_legacy();
     if (timing) cudaEventRecord(ev0, st);
     if (persistent) {
         if (cudaMemsetAsync(d_ctrl, 0, 2 * sizeof(int), st) != cudaSuccess ||
@@ -415,8 +502,13 @@ tc_error_t EncImpl::launch_own() {
 tc_error_t EncImpl::stage_c(bool with_recon) {
     const int nctu = ctu_cols * ctu_rows;
     const DevFrame rec = pool[pend.rs];
-    if (cudaMemcpyAsync(h_out, d_out, sizeof(CtuOut) * nctu, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    if (legacy) {
+        if (cudaMemcpyAsync(h_lblk, d_lblk, sizeof(legacy::LBlock) * (size_t)nctu * legacy::BLOCKS,
+                            cudaMemcpyDeviceToHost, st) != cudaSuccess)
+            return TC_ERR_INTERNAL;
+    } else if (cudaMemcpyAsync(h_out, d_out, sizeof(CtuOut) * nctu, cudaMemcpyDeviceToHost, st) != cudaSuccess) {
         return TC_ERR_INTERNAL;
+    }
     if (launch_frame_sse(cur.y, rec.y, W, H, sy, d_sse, st) != cudaSuccess) return TC_ERR_INTERNAL;
     ++kernel_launches;
     if (cudaMemcpyAsync(h_sse, d_sse, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
@@ -460,10 +552,12 @@ bool EncImpl::set_pipelined(bool on) {
 // pipelined encoder switches to its second record and packet buffers here,
 // so the next device step can land while this frame is entropy coded.
 tc_error_t EncImpl::commit_frame() {
-    if (persistent && h_ctrl[1]) return TC_ERR_INTERNAL;   // a bounded wait expired on the device
+    if (!legacy && persistent && h_ctrl[1]) return TC_ERR_INTERNAL;   // a bounded wait expired on the device
     ent.p = pend;
     ent.sse = *h_sse;
     ent.rec = h_out;
+    ent.lrec = h_lblk;
+    prev_rs = pend.rs;
     ent.buf = out_buf;
     ent_ready = true;
     // DPB shift: slot 3 falls out, the new reconstruction enters slot 0
@@ -492,6 +586,7 @@ tc_error_t EncImpl::commit_frame() {
 tc_error_t EncImpl::stage_d(tc_packet_t *pkt) {
     if (!ent_ready) return TC_ERR_INTERNAL;
     ent_ready = false;
+    if (legacy) return stage_d_legacy(pkt);
     const Pending &pd = ent.p;
     const int poc = pd.poc, is_key = pd.is_key, frame_type = pd.frame_type, qp = pd.qp, multiref = pd.multiref;
     const CtuOut *rec_out = ent.rec;
@@ -610,6 +705,30 @@ tc_error_t EncImpl::stage_d(tc_packet_t *pkt) {
     return TC_OK;
 }
 
+// Legacy packet (reference src/encoder.c:2713-3121 for use_v2 == 0).
+tc_error_t EncImpl::stage_d_legacy(tc_packet_t *pkt) {
+    const Pending &pd = ent.p;
+    const LegacyFrameSyntax h = legacy_frame_syntax(cfg, pd.is_key, pd.frame_type, pd.qp, pd.poc, bf_b_mode != 0,
+                                                    legacy_wpp);
+    const size_t frame_bytes = write_legacy_frame(ent.buf, out_buf_size, h, ent.lrec, ctu_cols, ctu_rows, row_buf);
+    if (!frame_bytes) return TC_ERR_MEMORY;
+    rc_frame_end((long long)frame_bytes * 8);
+    const unsigned long long sse = ent.sse;
+    double psnr = 100.0;
+    if (sse) {
+        const double mse = (double)sse / ((double)W * (double)H);
+        psnr = 10.0 * log10(255.0 * 255.0 / mse);
+    }
+    sum_psnr += psnr;
+    pkt->data = ent.buf;
+    pkt->size = frame_bytes;
+    pkt->pts = pd.poc;
+    pkt->key_frame = pd.is_key;
+    total_bytes += (long long)frame_bytes;
+    total_frames++;
+    return TC_OK;
+}
+
 tc_error_t EncImpl::encode_planned(tc_packet_t *pkt) {
     tc_error_t r = stage_a(pend.poc, pend.qp_off);
     if (r != TC_OK) return r;
@@ -622,7 +741,7 @@ tc_error_t EncImpl::encode_planned(tc_packet_t *pkt) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ev0, ev1);
         ctu_ms += ms;
-        ctu_launches += (long long)diag_off.size();
+        ctu_launches += (long long)(legacy ? ldiag_off.size() : diag_off.size());
         ctu_count += (long long)ctu_cols * ctu_rows;
         frames_timed++;
     }
@@ -792,7 +911,6 @@ tc_error_t EncImpl::encode_input(tc_packet_t *out) {
 // ---------------------------------------------------------------------------
 tc_encoder_t *tcb::encoder_create(const tc_config_t *config, DeviceArena *arena) {
     if (!config) return nullptr;
-    if (!config->use_v2) return nullptr;   // this library implements the v2 bitstream
     if (config->width <= 0 || config->height <= 0 || (config->width & 1) || (config->height & 1) ||
         config->width > TC_MAX_WIDTH || config->height > TC_MAX_HEIGHT)
         return nullptr;

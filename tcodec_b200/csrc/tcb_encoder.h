@@ -13,6 +13,7 @@
 #include "tcb_arena.h"
 #include "tcb_common.cuh"
 #include "tcb_entropy.h"
+#include "tcb_legacy_types.h"
 
 struct tc_encoder;
 
@@ -126,6 +127,7 @@ struct EncImpl {
         Pending p;
         unsigned long long sse = 0;
         const CtuOut *rec = nullptr;   // its decision records (host copy)
+        const legacy::LBlock *lrec = nullptr;   // legacy path: its block records
         uint8_t *buf = nullptr;        // its packet buffer
     } ent;
     bool ent_ready = false;
@@ -141,6 +143,18 @@ struct EncImpl {
     bool defer_glob = false;
     BitWriter fbw;
     std::vector<uint8_t> row_buf;
+    // Legacy (v0 / v1) 8x8 block path (use_v2 == 0): block records on the
+    // device and their host copies, the wavefront of diagonals c + 2r, the
+    // pool slot of the previous reconstruction (the frame being coded
+    // starts as its copy: the reference codes in place and reads samples of
+    // not yet coded blocks from it) and whether rows are coded as separate
+    // byte-aligned runs (the reference's WPP layout).
+    bool legacy = false, legacy_wpp = false;
+    legacy::LBlock *d_lblk = nullptr, *h_lblk = nullptr, *h_lblk_alt = nullptr;
+    legacy::LFrame lframe{};
+    int *d_litems = nullptr;
+    std::vector<int> ldiag_off, ldiag_cnt;
+    int prev_rs = -1;
     // Host threads that entropy-code one frame's entry-point rows (each row
     // is an independent range-coded substream). A lone encoder uses up to 8;
     // a batch or server codes each of its streams on its own thread and sets
@@ -151,6 +165,9 @@ struct EncImpl {
     tc_error_t stage_a(int poc, int b_layer_qp_off);
     tc_error_t stage_b();
     tc_error_t launch_own();
+    tc_error_t stage_b_legacy(int is_key, int frame_type, int qp, int rs);
+    tc_error_t launch_legacy();
+    tc_error_t stage_d_legacy(tc_packet_t *pkt);
     tc_error_t stage_c(bool with_recon = true);   // copy-back; the host recon copy unless with_recon is false
     tc_error_t readback_recon();
     tc_error_t commit_frame();

@@ -1,4 +1,6 @@
 // tcb_entropy.cpp — host v2 syntax emission (see tcb_entropy.h).
+#include <string.h>
+
 #include "tcb_entropy.h"
 
 namespace tcb {
@@ -273,6 +275,136 @@ void write_ctu_syntax(SyntaxSink &s, const CtuOut &o, const CtuGeom &g) {
 }
 
 // CRC-16/CCITT, init 0xFFFF, poly 0x1021 (reference src/bitstream.c:21-36).
+void write_legacy_ctu(SyntaxSink &s, const legacy::LBlock *blocks, int frame_type) {
+    for (int i = 0; i < legacy::BLOCKS; ++i) {
+        const legacy::LBlock &b = blocks[i];
+        if (!b.coded) continue;
+        const bool intra = b.mode == 2, merge = b.mode == 3, skip = b.mode == 0;
+        if (frame_type != 0) s.bits(CTX_BLOCK_MODE, b.mode, 2);
+        if (frame_type == 2 && !intra) s.bits(CTX_REF_SEL, (uint32_t)(b.ref & 3), 2);
+        if (intra) s.bits(CTX_INTRA_MODE, b.intra_mode, 5);
+        if (!intra && !merge) {
+            if (frame_type == 1) s.bits(CTX_REF_IDX, b.ref, 2);
+            s.se(CTX_MVD_X, b.mvd_x);
+            s.se(CTX_MVD_Y, b.mvd_y);
+        }
+        if (!merge && !skip) {
+            s.bits(CTX_DCT_SIZE, b.tid, 2);
+            if (b.tid & 2) s.coeffs(b.luma, 64, false, false);
+            else for (int q = 0; q < 4; ++q) s.coeffs(b.luma + 16 * q, 16, true, false);
+        }
+        s.coeffs(b.chroma, 16, true, false);
+        s.coeffs(b.chroma + 16, 16, true, false);
+    }
+}
+
+LegacyFrameSyntax legacy_frame_syntax(const tc_config_t &cfg, int is_key, int frame_type, int qp, int poc,
+                                      bool b_mode, bool wpp) {
+    LegacyFrameSyntax h;
+    h.version = cfg.bitstream_version == TC_VERSION_V0 ? 0 : 1;
+    h.W = cfg.width; h.H = cfg.height;
+    h.qp = qp; h.poc = poc; h.frame_type = frame_type;
+    h.wpp = wpp;
+    h.entropy = cfg.enable_entropy_coded != 0;
+    int flags = is_key ? TC_FLAG_KEY_FRAME : 0;
+    if (wpp) flags |= TC_FLAG_WPP;
+    if (h.version != 0) {
+        if (is_key) flags |= TC_FLAG_RAP;
+        if (cfg.enable_crc) flags |= TC_FLAG_CRC;
+        int profile = cfg.profile, level = cfg.level_idx;
+        if (profile > TC_PROFILE_MAX) profile = TC_PROFILE_BASELINE_MOBILE;
+        if (level > TC_LEVEL_MAX) level = TC_LEVEL_AUTO;
+        h.profile_level = (profile << 4) | (level & 0x0F);
+        int tools = TC_TOOL_SKIP_MERGE | TC_TOOL_CFL_CHROMA | TC_TOOL_JND_WEIGHTING | TC_TOOL_MEDIAN_MV_PRED |
+                    TC_TOOL_SIX_TAP_INTERP;
+        if (cfg.preset == TC_PRESET_SLOW && profile >= TC_PROFILE_STREAMING_MAIN) tools |= TC_TOOL_MULTI_REF;
+        if (h.entropy) tools |= TC_TOOL_ENTROPY_CODED;
+        if (frame_type == 2) tools |= TC_TOOL_BIPRED;
+        h.tools = tools;
+        h.crc = cfg.enable_crc != 0;
+        if (b_mode) {
+            flags |= TC_FLAG_EXT_HEADER;
+            h.ext = frame_type == 0 ? 0 : (frame_type == 2 ? 2 : 1);
+        }
+    }
+    h.flags = flags;
+    return h;
+}
+
+size_t write_legacy_frame(uint8_t *buf, size_t cap, const LegacyFrameSyntax &h, const legacy::LBlock *blocks,
+                          int ctu_cols, int ctu_rows, std::vector<uint8_t> &row_scratch) {
+    memset(buf, 0, cap);
+    BitWriter bw;
+    bw.init(buf, cap);
+    bw.put_bits(TC_MAGIC_0, 8); bw.put_bits(TC_MAGIC_1, 8); bw.put_bits(TC_MAGIC_2, 8);
+    bw.put_bits((uint32_t)h.version, 8);
+    bw.put_bits((uint32_t)(uint16_t)h.W, 16); bw.put_bits((uint32_t)(uint16_t)h.H, 16);
+    bw.put_bits((uint32_t)h.flags, 8);
+    bw.put_bits((uint8_t)(int8_t)(h.qp - TC_QP_DEFAULT), 8);
+    bw.put_bits((uint8_t)(h.poc & 0xFF), 8);
+    if (h.version == 0) {
+        bw.put_bits(0, 8);
+    } else {
+        bw.put_bits((uint8_t)h.profile_level, 8);
+        bw.put_bits((uint16_t)h.tools, 16);
+        if (h.ext >= 0) bw.put_bits((uint32_t)h.ext, 8);
+    }
+    bw.align();
+    const int per_ctu = legacy::BLOCKS;
+    if (h.wpp) {
+        // Entry table: rows - 1 offsets (16 bits each, relative to row 0),
+        // then every row as its own byte-aligned run of raw syntax.
+        const int noff = ctu_rows - 1;
+        bw.put_bits((uint32_t)noff, 16);
+        const size_t table = bw.byte_pos;
+        for (int i = 0; i < noff; ++i) bw.put_bits(0, 16);
+        bw.align();
+        const size_t start = bw.byte_pos;
+        const size_t per_row = cap / (size_t)(ctu_rows > 0 ? ctu_rows : 1) + 256;
+        if (row_scratch.size() < per_row) row_scratch.resize(per_row);
+        size_t offs[64];
+        for (int r = 0; r < ctu_rows; ++r) {
+            if (r < 64) offs[r] = bw.byte_pos - start;
+            BitWriter rw;
+            memset(row_scratch.data(), 0, per_row);
+            rw.init(row_scratch.data(), per_row);
+            SyntaxSink sink{&rw, nullptr, nullptr};
+            for (int c = 0; c < ctu_cols; ++c)
+                write_legacy_ctu(sink, blocks + (size_t)(r * ctu_cols + c) * per_ctu, h.frame_type);
+            rw.align();
+            if (rw.overflow) return 0;
+            const size_t n = rw.bytes();
+            if (bw.byte_pos + n > cap) return 0;
+            memcpy(buf + bw.byte_pos, row_scratch.data(), n);
+            bw.byte_pos += n;
+            if (bw.byte_pos < cap) buf[bw.byte_pos] = 0;
+        }
+        for (int i = 0; i < noff && i + 1 < 64; ++i) {
+            const uint16_t o = (uint16_t)offs[i + 1];
+            buf[table + 2 * i] = (uint8_t)(o >> 8);
+            buf[table + 2 * i + 1] = (uint8_t)(o & 0xFF);
+        }
+    } else {
+        RangeEncoder rc;
+        uint8_t ctx[TC_NUM_CONTEXTS_RC];
+        memset(ctx, 0, sizeof(ctx));
+        rc.init(&bw);
+        SyntaxSink sink{&bw, h.entropy ? &rc : nullptr, ctx};
+        for (int r = 0; r < ctu_rows; ++r)
+            for (int c = 0; c < ctu_cols; ++c)
+                write_legacy_ctu(sink, blocks + (size_t)(r * ctu_cols + c) * per_ctu, h.frame_type);
+        if (h.entropy) rc.flush();
+        bw.align();
+    }
+    if (h.version != 0 && h.crc) {
+        const uint16_t crc = crc16_ccitt(buf, bw.bytes());
+        bw.put_bits(crc >> 8, 8);
+        bw.put_bits(crc & 0xFF, 8);
+    }
+    if (bw.overflow) return 0;
+    return bw.bytes();
+}
+
 uint16_t crc16_ccitt(const uint8_t *data, size_t len) {
     uint16_t crc = 0xFFFF;
     for (size_t i = 0; i < len; ++i) {

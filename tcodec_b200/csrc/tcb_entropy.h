@@ -7,7 +7,9 @@
 #include <stdint.h>
 #include <vector>
 
+#include "../../include/tcodec_types.h"
 #include "tcb_common.cuh"
+#include "tcb_legacy_types.h"
 
 namespace tcb {
 
@@ -88,6 +90,32 @@ struct CtuGeom {
 // Emit the syntax of one CTU (reference src/encoder.c:587-653, 429-543
 // write branches, 1494-1501).
 void write_ctu_syntax(SyntaxSink &s, const CtuOut &o, const CtuGeom &g);
+
+// Emit the legacy (v0 / v1) syntax of one CTU's 8x8 blocks in raster
+// order (reference src/encoder.c:1996-2098 and 2186-2190): block mode,
+// B-frame reference selection, intra mode, P-frame ref_idx and MVD,
+// transform id and luma levels, then Cb and Cr levels.
+void write_legacy_ctu(SyntaxSink &s, const legacy::LBlock *blocks, int frame_type);
+
+// Frame-level fields of a legacy packet.
+struct LegacyFrameSyntax {
+    int version = 1;          // 0: 12-byte header; 1: profile / tools / extension byte
+    int W = 0, H = 0, flags = 0, qp = 32, poc = 0, profile_level = 0, tools = 0;
+    int ext = -1;             // frame-type code of the extension byte, -1: none
+    int frame_type = 0;
+    bool wpp = false, entropy = false, crc = false;
+};
+// Header fields of a legacy frame (reference src/encoder.c:2713-2819):
+// `wpp` when the frame's rows are coded as separate byte-aligned runs.
+LegacyFrameSyntax legacy_frame_syntax(const tc_config_t &cfg, int is_key, int frame_type, int qp, int poc,
+                                      bool b_mode, bool wpp);
+// The whole legacy packet (reference src/encoder.c:2365-2399 header,
+// 2966-3067 rows: per-row byte-aligned runs behind a 16-bit entry table
+// when `wpp`, else one run, range coded when `entropy`; CRC-16 when `crc`
+// and the version is 1).  Returns the packet size, 0 when `cap` is too
+// small.  `row_scratch` holds the per-row runs.
+size_t write_legacy_frame(uint8_t *buf, size_t cap, const LegacyFrameSyntax &h, const legacy::LBlock *blocks,
+                          int ctu_cols, int ctu_rows, std::vector<uint8_t> &row_scratch);
 
 uint16_t crc16_ccitt(const uint8_t *data, size_t len);
 

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include "tcb_common.cuh"
+#include "tcb_legacy_types.h"
 
 namespace tcb {
 
@@ -29,6 +30,11 @@ cudaError_t launch_glob_mv_multi(const GlobJob *jobs, int n, cudaStream_t st);
 cudaError_t launch_glob_mv(const uint8_t *cur, const uint8_t *ref, int W, int H, int s,
                            FrameParams *d_params, cudaStream_t st);
 cudaError_t launch_hist16(const uint8_t *y, int W, int H, int s, int *d_hist, cudaStream_t st);
+// Legacy (v0 / v1) 8x8 block path: one launch per wavefront diagonal;
+// `encode` picks the encoder (decisions + reconstruction) or the decoder
+// (reconstruction from parsed records).
+cudaError_t upload_legacy_tables();
+cudaError_t launch_legacy_ctus(const legacy::LFrame &F, const int *d_items, int n, bool encode, cudaStream_t st);
 cudaError_t launch_frame_sse(const uint8_t *a, const uint8_t *b, int W, int H, int s,
                              unsigned long long *d_out, cudaStream_t st);
 

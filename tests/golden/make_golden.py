@@ -19,6 +19,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "golden_v2.sha256")
+OUT_LEGACY = os.path.join(HERE, "golden_legacy.sha256")
 
 
 def reference_manifest() -> str:
@@ -39,6 +40,13 @@ VARIANTS = {
     "v2e": dict(entropy=True, profile=0, b_frames=False),
     "v2m": dict(entropy=True, profile=1, b_frames=False),
     "v2b": dict(entropy=True, profile=1, b_frames=True),
+}
+# Legacy 8x8 block syntax (tools/gen_golden.sh:87-111): `--bs-version 0`,
+# `--bs-version 1`, `--bs-version 1 --entropy`; default worker count.
+LEGACY_VARIANTS = {
+    "v0": dict(version=0, entropy=False),
+    "v1": dict(version=1, entropy=False),
+    "v1e": dict(version=1, entropy=True),
 }
 
 
@@ -76,10 +84,11 @@ def parse_name(name: str):
     return pat, w, h, int(qp[2:]), var
 
 
-def load():
-    """[(sha256, name, pattern, w, h, qp, variant)] from golden_v2.sha256."""
+def load(path: str = OUT):
+    """[(sha256, name, pattern, w, h, qp, variant)] from golden_v2.sha256
+    (or the legacy file)."""
     out = []
-    with open(OUT) as f:
+    with open(path) as f:
         for line in f:
             digest, name = line.split()
             out.append((digest, name) + parse_name(name))
@@ -88,7 +97,7 @@ def load():
 
 def main():
     src = reference_manifest()
-    lines = []
+    lines, legacy = [], []
     with open(src) as f:
         for line in f:
             digest, name = line.split()
@@ -97,9 +106,12 @@ def main():
             var = name[:-4].split("_")[-1]
             if var in VARIANTS:
                 lines.append(f"{digest}  {name}\n")
-    with open(OUT, "w") as f:
-        f.writelines(lines)
-    print(f"wrote {len(lines)} hashes to {OUT}")
+            elif var in LEGACY_VARIANTS:
+                legacy.append(f"{digest}  {name}\n")
+    for path, ls in ((OUT, lines), (OUT_LEGACY, legacy)):
+        with open(path, "w") as f:
+            f.writelines(ls)
+        print(f"wrote {len(ls)} hashes to {path}")
 
 
 if __name__ == "__main__":

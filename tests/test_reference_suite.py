@@ -1,6 +1,13 @@
-"""The reference's own C regression tests (its test/test_tcodec.c) for the
-v2 bitstream and the modules beneath it, through tests/reference_suite_v2.c
-(built by oracle/Makefile `suite`):
+"""The reference's own C regression tests (its test/test_tcodec.c).
+
+The whole suite (53 tests in its fast mode: the default-configuration
+legacy v1 encodes and decodes, v0 / v1 / v2 bitstreams, presets, B-frames,
+malformed-stream fuzzing, the range coder, transforms, SAO) runs as the
+reference builds it, linked with the reference's objects on the CPU and
+with libtcodec_b200.so on the GPU (oracle/Makefile `suite`).
+
+The v2 bitstream and the modules beneath it also run alone, through
+tests/reference_suite_v2.c:
 
 * linked with the reference library's objects, on the CPU: the harness and
   the selection of tests are sound (every selected test passes on the
@@ -20,6 +27,7 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF = os.path.join(ROOT, "oracle", "_ref")
 N_TESTS = 16
+N_FULL = 53
 
 
 def _run(binary):
@@ -42,3 +50,14 @@ def test_reference_suite_on_reference_library():
 def test_reference_suite_on_b200_library():
     rc, passed, run, log = _run("test_v2_suite_b200")
     assert (rc, passed, run) == (0, N_TESTS, N_TESTS), log[-3000:]
+
+
+def test_full_reference_suite_on_reference_library():
+    rc, passed, run, log = _run("test_tcodec_ref")
+    assert (rc, passed, run) == (0, N_FULL, N_FULL), log[-3000:]
+
+
+@pytest.mark.gpu
+def test_full_reference_suite_on_b200_library():
+    rc, passed, run, log = _run("test_tcodec_b200")
+    assert (rc, passed, run) == (0, N_FULL, N_FULL), log[-3000:]
