@@ -10,9 +10,10 @@
  * usable CUDA device tc_encoder_create returns NULL and encode calls return
  * TC_ERR_INTERNAL.
  *
- * Scope of this library: the v2 bitstream (bitstream_version is forced to
- * 2 when use_v2 is set).  Creating an encoder with use_v2 = 0 (legacy v0/v1
- * block coder) returns NULL.
+ * Both bitstreams of the reference are implemented: v2 (use_v2 = 1,
+ * bitstream_version forced to 2) and the legacy fixed 8x8 block syntax
+ * (use_v2 = 0, bitstream_version 0 or 1), whose block decisions and
+ * reconstruction also run on the device.  Frame sizes must be even.
  */
 #ifndef TCODEC_H
 #define TCODEC_H

@@ -1,4 +1,5 @@
-"""B200-native TCodec v2 pixel pipeline.
+"""B200-native TCodec pixel pipeline (v2 quadtree and legacy v0 / v1 block
+bitstreams).
 
 `tcodec_b200.api` binds the C ABI of libtcodec_b200.so: the reference's
 include/tcodec.h encoder / decoder entry points and the additions of

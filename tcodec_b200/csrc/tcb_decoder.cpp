@@ -1,8 +1,9 @@
-// tcb_decoder.cpp — tc_decoder_* (reference include/tcodec.h:64-111) for
-// v2 bitstreams: the serial syntax parse (range decoder / Exp-Golomb) runs
-// on the host and fills the same per-CTU records the encoder emits; the
-// reconstruction (prediction, dequantisation, inverse transform,
-// deblocking, SAO) runs on the device as the CTU wavefront of decode_kernel.
+// tcb_decoder.cpp — tc_decoder_* (reference include/tcodec.h:64-111): the
+// serial syntax parse (range decoder / Exp-Golomb) runs on the host and
+// fills the same per-CTU records the encoder emits; the reconstruction
+// (prediction, dequantisation, inverse transform, deblocking, SAO) runs on
+// the device as the CTU wavefront of decode_kernel (v2 streams) or of the
+// legacy block kernel (v0 / v1 streams, tcb_legacy.cu).
 //
 // Mirrors reference src/decoder.c: header checks (102-225), frame-level
 // flow (2541-2925), entry-point tables (2096-2190), syntax parse
@@ -324,7 +325,10 @@ struct Parser {
 // reconstruction kernel reads, motion vectors made absolute with the
 // median of the left, above and above-right blocks inside the CTU.  Blocks
 // outside the frame are not coded and count as inter blocks with a zero
-// vector (the reference's zeroed block info).
+// vector (the reference's zeroed block info).  As in the reference, a read
+// past the end of the data yields zero bits and the parse goes on: the
+// legacy decoder does not fail a frame on it (src/decoder.c:2847
+// checks the reader's error for v2 streams only).
 void parse_legacy_ctu(Parser &p, legacy::LBlock *blk, int ox, int oy, int W, int H, int ft) {
     uint8_t inter[legacy::BLOCKS];
     int mvx[legacy::BLOCKS], mvy[legacy::BLOCKS];
@@ -399,7 +403,6 @@ void parse_legacy_ctu(Parser &p, legacy::LBlock *blk, int ox, int oy, int W, int
         inter[b] = intra ? 0 : 1;
         mvx[b] = intra ? 0 : bmx;
         mvy[b] = intra ? 0 : bmy;
-        if (p.bs->error) return;
     }
 }
 
@@ -421,7 +424,8 @@ tc_error_t read_header(Reader &bs, Header &h) {
     const int8_t qd = (int8_t)bs.bits(8);
     h.frame_num = (int)bs.bits(8);
     int ext_type = -1;
-    if (h.version != TC_VERSION_V0) {
+    if (h.version == TC_VERSION_V0) (void)bs.bits(8);   // v0: reserved byte
+    else {
         const int pl = (int)bs.bits(8);
         h.tools = (int)bs.bits(16);
         if (h.tools & ~(int)TC_TOOLS_IMPLEMENTED) return TC_ERR_BITSTREAM;
@@ -802,7 +806,6 @@ tc_error_t DecImpl::legacy_body(const uint8_t *data, size_t size, Reader &bs, co
     const size_t nblk = (size_t)cols * rows * legacy::BLOCKS;
     uint8_t ctx[TC_NUM_CONTEXTS_RC];
     memset(ctx, 0, sizeof(ctx));
-    bool bad = false;
     if (hdr.flags & TC_FLAG_WPP) {
         const uint32_t noff = bs.bits(16);
         if (bs.error || noff > 63 || (int)noff != rows - 1) return TC_ERR_BITSTREAM;
@@ -814,27 +817,22 @@ tc_error_t DecImpl::legacy_body(const uint8_t *data, size_t size, Reader &bs, co
         const size_t start = bs.pos;
         for (int r = 0; r < rows; ++r)
             if (start + off[r] > size || (r > 0 && off[r] < off[r - 1])) return TC_ERR_BITSTREAM;
-        for (int r = 0; r < rows && !bad; ++r) {
+        for (int r = 0; r < rows; ++r) {
             const size_t b0 = start + off[r], b1 = r + 1 < rows ? start + off[r + 1] : size;
             Reader rr;
             rr.init(data + b0, b1 - b0);
             Parser p{&rr, nullptr, ctx, fw, fh, ft, 0, 0, dpb_ok, nullptr, 0, 0, 0};
-            for (int c = 0; c < cols && !bad; ++c) {
+            for (int c = 0; c < cols; ++c)
                 parse_legacy_ctu(p, h_lblk + (size_t)(r * cols + c) * legacy::BLOCKS, c * 64, r * 64, fw, fh, ft);
-                bad = rr.error != 0;
-            }
         }
     } else {
         RDec rc;
         if (entropy) rc.init(&bs);
         Parser p{&bs, entropy ? &rc : nullptr, ctx, fw, fh, ft, 0, 0, dpb_ok, nullptr, 0, 0, 0};
-        for (int r = 0; r < rows && !bad; ++r)
-            for (int c = 0; c < cols && !bad; ++c) {
+        for (int r = 0; r < rows; ++r)
+            for (int c = 0; c < cols; ++c)
                 parse_legacy_ctu(p, h_lblk + (size_t)(r * cols + c) * legacy::BLOCKS, c * 64, r * 64, fw, fh, ft);
-                bad = bs.error != 0;
-            }
     }
-    if (bad) return TC_ERR_BITSTREAM;
     legacy::LFrame F;
     memset(&F, 0, sizeof(F));
     F.W = fw; F.H = fh; F.sy = sy; F.sc = sc; F.ctu_cols = cols; F.ctu_rows = rows;

@@ -5,7 +5,8 @@
 // encode_poc_frame): frame type (key interval, scene cut on a device
 // histogram, B-frame schedule), QP / rate control, header and tool flags,
 // DPB bookkeeping, entropy coding of the device's CTU records, entry-point
-// tables and CRC.  Device responsibilities: everything that touches pixels.
+// tables and CRC.  Device responsibilities: everything that touches pixels
+// (the v2 CTU engine, or the legacy 8x8 block kernel when use_v2 = 0).
 // Frames stay resident in HBM: the DPB is a ring of device frame buffers
 // and only the packet, the CTU records and the host copy of the
 // reconstruction (API contract: encoder->recon) come back each frame.
