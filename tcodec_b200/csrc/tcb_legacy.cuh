@@ -67,8 +67,6 @@ LG_TABLE int8_t lg_dia[4][2] = {{0, -1}, {-1, 0}, {1, 0}, {0, 1}};
 LG_TABLE int8_t lg_qpel[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, 1}, {1, -1}, {-1, -1}};
 // Intra modes tried first (reference src/encoder.c:1563-1565).
 LG_TABLE int8_t lg_fast_modes[8] = {0, 1, 2, 5, 8, 9, 13, 17};
-// The other ten, in increasing order (tried when no fast mode is good).
-LG_TABLE int8_t lg_slow_modes[10] = {3, 4, 6, 7, 10, 11, 12, 14, 15, 16};
 
 LG_FN int qscale_of(int qp) { return lg_qscale[clampi(qp, 0, 63)]; }
 LG_FN int jnd_of(int band) {
@@ -179,21 +177,11 @@ LG_FN int intra_dc_value(const LState &S) {
 }
 
 // SAD of the block against intra mode m.
-// SADs of up to 10 intra modes at once (the modes are independent, so
-// their reductions are issued back to back).
-LG_FN void intra_sads(const LState &S, const int8_t *modes, int M, int dc, int *out) {
+LG_FN int intra_sad(const LState &S, int m, int dc) {
     const int L = lane_id();
-    int acc[10];
-#pragma unroll
-    for (int k = 0; k < 10; ++k) acc[k] = 0;
-    for (int i = L; i < 64; i += NL) {
-        const int o = S.orig[i], x = i & 7, y = i >> 3;
-#pragma unroll
-        for (int k = 0; k < 10; ++k)
-            if (k < M) acc[k] += absi(o - intra_at(S.ra + 1, S.rl + 1, 8, modes[k], dc, x, y));
-    }
-#pragma unroll
-    for (int k = 0; k < 10; ++k) out[k] = k < M ? team_sum(acc[k]) : SAD_MAX;
+    int s = 0;
+    for (int i = L; i < 64; i += NL) s += absi((int)S.orig[i] - intra_at(S.ra + 1, S.rl + 1, 8, m, dc, i & 7, i >> 3));
+    return team_sum(s);
 }
 
 // Integer SAD at (mx, my) with the reference's frame bounds check
@@ -206,10 +194,9 @@ LG_FN int sad_at(const LState &S, const uint8_t *ref, int s, int W, int H, int m
     return team_sum(a);
 }
 
-// This lane's part of the quarter-sample SAD of the refinement stage:
-// six-tap where the margins allow, bilinear otherwise (reference
-// src/motion.c:465-480, 308-341).
-LG_FN int qpel_sad_part(const LState &S, const uint8_t *ref, int s, int W, int H, int qx, int qy) {
+// Quarter-sample SAD of the refinement stage: six-tap where the margins
+// allow, bilinear otherwise (reference src/motion.c:465-480, 308-341).
+LG_FN int qpel_sad(const LState &S, const uint8_t *ref, int s, int W, int H, int qx, int qy) {
     const int fx = qx >> 2, fy = qy >> 2, dx = qx & 3, dy = qy & 3;
     const int L = lane_id();
     int a = 0;
@@ -222,53 +209,7 @@ LG_FN int qpel_sad_part(const LState &S, const uint8_t *ref, int s, int W, int H
             a += absi((int)S.orig[i] - interp_qpel(top, bot, dy));
         }
     }
-    return a;
-}
-
-// One integer stage of the search: up to `iters` passes over a pattern of
-// K points (scaled by `step`) around the current best, each point committed
-// as soon as it improves, so later points of the pass are taken around the
-// new best (reference src/motion.c:397-452).  The points still to be tried
-// are scored together (one load round trip and back-to-back reductions);
-// the first that improves is the one the sequential walk would commit, and
-// the points after it are scored again around the new best.
-LG_FN void search_stage(const LState &S, const uint8_t *ref, int s, int W, int H, const int8_t (*pat)[2], int K,
-                        int step, int iters, int &bx, int &by, int &best) {
-    const int L = lane_id();
-    for (int it = 0; it < iters; ++it) {
-        bool imp = false;
-        int p = 0;
-        while (p < K) {
-            const int cx = bx / 4, cy = by / 4;
-            int acc[6];
-            bool ok[6];
-#pragma unroll
-            for (int q = 0; q < 6; ++q) {
-                acc[q] = 0;
-                ok[q] = false;
-                if (q >= p && q < K) {
-                    const int mx = cx + pat[q][0] * step, my = cy + pat[q][1] * step;
-                    ok[q] = mx >= 0 && my >= 0 && mx + 8 <= W && my + 8 <= H;
-                    if (ok[q])
-                        for (int i = L; i < 64; i += NL)
-                            acc[q] += absi((int)S.orig[i] - (int)ref[(size_t)(my + (i >> 3)) * s + mx + (i & 7)]);
-                }
-            }
-            int f = -1, fv = 0;
-#pragma unroll
-            for (int q = 5; q >= 0; --q) {
-                const int v = ok[q] ? team_sum(acc[q]) : SAD_MAX;
-                if (q >= p && q < K && v < best) { f = q; fv = v; }
-            }
-            if (f < 0) break;
-            best = fv;
-            bx = (cx + pat[f][0] * step) * 4;
-            by = (cy + pat[f][1] * step) * 4;
-            imp = true;
-            p = f + 1;
-        }
-        if (!imp) break;
-    }
+    return team_sum(a);
 }
 
 // Hexagonal search with sequential commit inside every pass, then the
@@ -280,33 +221,39 @@ LG_FN void motion_est(const LState &S, const uint8_t *ref, int s, int W, int H, 
     int bx = cx * 4, by = cy * 4;
     int best = sad_at(S, ref, s, W, H, cx, cy);
     const int step = maxi(1, range / 4);
-    search_stage(S, ref, s, W, H, lg_hexl, 6, step, 2, bx, by, best);
-    search_stage(S, ref, s, W, H, lg_hexs, 6, 1, 3, bx, by, best);
-    search_stage(S, ref, s, W, H, lg_dia, 4, 1, 4, bx, by, best);
-    // Quarter-sample refinement: eight points committed in order, scored
-    // together and re-scored after each commit as in search_stage.
-    int p = 0;
-    while (p < 8) {
-        int acc[8];
-        bool ok[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int qx = bx + lg_qpel[q][0], qy = by + lg_qpel[q][1];
-            const int fx = qx >> 2, fy = qy >> 2;
-            ok[q] = q >= p && fx >= 0 && fy >= 0 && fx + 9 <= W && fy + 9 <= H;
-            acc[q] = ok[q] ? qpel_sad_part(S, ref, s, W, H, qx, qy) : 0;
+    for (int it = 0; it < 2; ++it) {
+        bool imp = false;
+        for (int p = 0; p < 6; ++p) {
+            const int mx = bx / 4 + lg_hexl[p][0] * step, my = by / 4 + lg_hexl[p][1] * step;
+            const int v = sad_at(S, ref, s, W, H, mx, my);
+            if (v < best) { best = v; bx = mx * 4; by = my * 4; imp = true; }
         }
-        int f = -1, fv = 0;
-#pragma unroll
-        for (int q = 7; q >= 0; --q) {
-            const int v = ok[q] ? team_sum(acc[q]) : SAD_MAX;
-            if (ok[q] && v < best) { f = q; fv = v; }
+        if (!imp) break;
+    }
+    for (int it = 0; it < 3; ++it) {
+        bool imp = false;
+        for (int p = 0; p < 6; ++p) {
+            const int mx = bx / 4 + lg_hexs[p][0], my = by / 4 + lg_hexs[p][1];
+            const int v = sad_at(S, ref, s, W, H, mx, my);
+            if (v < best) { best = v; bx = mx * 4; by = my * 4; imp = true; }
         }
-        if (f < 0) break;
-        best = fv;
-        bx += lg_qpel[f][0];
-        by += lg_qpel[f][1];
-        p = f + 1;
+        if (!imp) break;
+    }
+    for (int it = 0; it < 4; ++it) {
+        bool imp = false;
+        for (int p = 0; p < 4; ++p) {
+            const int mx = bx / 4 + lg_dia[p][0], my = by / 4 + lg_dia[p][1];
+            const int v = sad_at(S, ref, s, W, H, mx, my);
+            if (v < best) { best = v; bx = mx * 4; by = my * 4; imp = true; }
+        }
+        if (!imp) break;
+    }
+    for (int p = 0; p < 8; ++p) {
+        const int qx = bx + lg_qpel[p][0], qy = by + lg_qpel[p][1];
+        const int fx = qx >> 2, fy = qy >> 2;
+        if (fx < 0 || fy < 0 || fx + 9 > W || fy + 9 > H) continue;
+        const int v = qpel_sad(S, ref, s, W, H, qx, qy);
+        if (v < best) { best = v; bx = qx; by = qy; }
     }
     mvx = bx; mvy = by; sad_out = best;
 }
@@ -505,15 +452,16 @@ LG_NOINL void encode_block(LState &S, const LFrame &F, int bi, int fx, int fy, L
     // ---- intra search: eight fast modes, the rest when none is good
     const int dc = intra_dc_value(S);
     int best_intra = 1, best_isad = SAD_MAX;
-    int isad[10];
-    intra_sads(S, lg_fast_modes, 8, dc, isad);
-    for (int k = 0; k < 8; ++k)
-        if (isad[k] < best_isad) { best_isad = isad[k]; best_intra = lg_fast_modes[k]; }
-    if (best_isad > 256) {
-        intra_sads(S, lg_slow_modes, 10, dc, isad);
-        for (int k = 0; k < 10; ++k)
-            if (isad[k] < best_isad) { best_isad = isad[k]; best_intra = lg_slow_modes[k]; }
+    for (int k = 0; k < 8; ++k) {
+        const int v = intra_sad(S, lg_fast_modes[k], dc);
+        if (v < best_isad) { best_isad = v; best_intra = lg_fast_modes[k]; }
     }
+    if (best_isad > 256)
+        for (int m = 0; m < 18; ++m) {
+            if (m == 0 || m == 1 || m == 2 || m == 5 || m == 8 || m == 9 || m == 13 || m == 17) continue;
+            const int v = intra_sad(S, m, dc);
+            if (v < best_isad) { best_isad = v; best_intra = m; }
+        }
     for (int i = L; i < 64; i += NL) S.pred[i] = (uint8_t)intra_at(S.ra + 1, S.rl + 1, 8, best_intra, dc, i & 7, i >> 3);
     bool is_intra = true;
     int mvx = 0, mvy = 0, ref_idx = 0;
