@@ -64,7 +64,8 @@ void tcb_encoder_set_entropy_threads(tc_encoder_t *enc, int threads);
  * ------------------------------------------------------------------- */
 typedef struct tcb_batch tcb_batch_t;
 
-/* One encoder per configs[i]; NULL on invalid config or device failure. */
+/* One encoder per configs[i]; NULL on invalid config or device failure.
+ * Batches run the v2 CTU engine: every config must set use_v2. */
 tcb_batch_t *tcb_batch_create(const tc_config_t *configs, int n);
 void tcb_batch_destroy(tcb_batch_t *batch);
 int tcb_batch_size(tcb_batch_t *batch);
@@ -145,7 +146,8 @@ void tcb_server_destroy(tcb_server_t *server);
  * (0 for an invalid configuration). */
 size_t tcb_server_session_bytes(const tc_config_t *config);
 /* Queue a session (FIFO).  Returns its id (>= 0), TC_ERR_PARAM for an
- * invalid configuration, TC_ERR_MEMORY if it can never fit the budget. */
+ * invalid configuration (sessions run the v2 CTU engine: use_v2 must be
+ * set), TC_ERR_MEMORY if it can never fit the budget. */
 int tcb_server_open(tcb_server_t *server, const tc_config_t *config);
 /* Queue the session's next frame (host planes, copied before returning). */
 tc_error_t tcb_server_push(tcb_server_t *server, int session,

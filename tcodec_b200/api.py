@@ -147,7 +147,7 @@ def make_config(lib: ctypes.CDLL, width: int, height: int, qp: int = 32, preset:
 
 
 class Encoder:
-    """One v2 encode session through the C ABI."""
+    """One encode session through the C ABI (v2 or legacy, as `cfg` says)."""
 
     def __init__(self, lib: ctypes.CDLL, cfg: Config):
         self.lib = lib
