@@ -6,7 +6,10 @@
 // at the interval, DPB of four), writes packets with the library's host
 // syntax writer (tcb_entropy.cpp), and compares every packet and the final
 // reconstruction with the reference encoder linked in from its own
-// sources.  Usage: legacy_emu W H frames qp preset version entropy crc
+// sources.  Each reference packet is also decoded by the library's host
+// parser (tcb_parse.h) and the same device source's reconstruction
+// (decode_block) and compared with the reference decoder's picture.
+// Usage: legacy_emu W H frames qp preset version entropy crc
 // threads profile [seed [input.yuv|- [output]]]: frames come from the
 // synthetic clip, or from a planar 4:2:0 file; `output` receives the
 // stream as length-prefixed packets (4-byte little-endian size, then the
@@ -39,6 +42,7 @@ inline int ldct8(int k, int n) { return g_d8[k][n]; }
 
 #include "../tcodec_b200/csrc/tcb_legacy.cuh"
 #include "../tcodec_b200/csrc/tcb_entropy.h"
+#include "../tcodec_b200/csrc/tcb_parse.h"
 
 using namespace tcb;
 using namespace tcb::legacy;
@@ -126,6 +130,8 @@ int main(int argc, char **argv) {
     cfg.use_v2 = 0;
     tc_encoder_t *ref = tc_encoder_create(&cfg);
     if (!ref) { printf("reference encoder create failed\n"); return 2; }
+    tc_decoder_t *rdec = tc_decoder_create(W, H);
+    if (!rdec) { printf("reference decoder create failed\n"); return 2; }
 
     const int sy = ((W + 63) / 64) * 64, sc = ((W / 2 + 63) / 64) * 64;
     const int cols = (W + 63) / 64, rows = (H + 63) / 64;
@@ -141,6 +147,12 @@ int main(int argc, char **argv) {
     bool dpb_ok[4] = {false, false, false, false};
     std::vector<LBlock> blocks((size_t)cols * rows * BLOCKS);
     std::vector<uint8_t> pkt((size_t)W * H * 3), scratch;
+    // Decoder side: persistent picture, DPB copies with their POCs.
+    std::vector<uint8_t> dy(cy.size(), 0), dcb(ccb.size(), 0), dcr(ccb.size(), 0);
+    std::vector<Plane3> ddpb(4);
+    int ddpb_poc[4] = {-1, -1, -1, -1};
+    bool ddpb_ok[4] = {false, false, false, false};
+    std::vector<LBlock> dblocks((size_t)cols * rows * BLOCKS);
     LState S;
     int mismatch = 0;
     size_t total = 0;
@@ -217,13 +229,54 @@ int main(int argc, char **argv) {
             mismatch = 1;
             break;
         }
+        // ---- decode the reference packet both ways
+        {
+            const tc_pixel_t *oy, *ocb, *ocr;
+            int osy, oscb, oscr;
+            if (tc_decoder_decode(rdec, rp.data, rp.size, &oy, &osy, &ocb, &oscb, &ocr, &oscr) != TC_OK) {
+                printf("reference decode failed at frame %d\n", f);
+                return 2;
+            }
+            tcb::parse::Reader bs;
+            bs.init(rp.data, rp.size);
+            tcb::parse::Header hd;
+            if (tcb::parse::read_header(bs, hd) != TC_OK) { printf("frame %d: header rejected\n", f); mismatch = 1; break; }
+            bs.align();
+            const int ent = hd.version != 0 && (hd.tools & TC_TOOL_ENTROPY_CODED);
+            if (hd.frame_type == 0 && hd.frame_num > 0)
+                for (int i = 0; i < 4; ++i) { ddpb_ok[i] = false; ddpb_poc[i] = -1; }
+            if (tcb::parse::parse_legacy_frame(rp.data, rp.size, bs, hd, ent, W, H, cols, rows, dblocks.data()) != TC_OK) {
+                printf("frame %d: parse failed\n", f);
+                mismatch = 1;
+                break;
+            }
+            LFrame D;
+            memset(&D, 0, sizeof(D));
+            D.W = W; D.H = H; D.sy = sy; D.sc = sc; D.ctu_cols = cols; D.ctu_rows = rows;
+            D.rec_y = dy.data(); D.rec_cb = dcb.data(); D.rec_cr = dcr.data();
+            for (int i = 0; i < 4; ++i) D.dpb_y[i] = ddpb_ok[i] ? ddpb[i].y.data() : nullptr;
+            D.frame_type = hd.frame_type; D.qp = hd.qp; D.blocks = dblocks.data();
+            for (int r = 0; r < rows; ++r)
+                for (int c = 0; c < cols; ++c) code_ctu(S, D, r, c, false);
+            int dbad = 0;
+            for (int j = 0; j < H && !dbad; ++j) if (memcmp(&dy[(size_t)j * sy], oy + (size_t)j * osy, W)) dbad = 1 + j;
+            for (int j = 0; j < H / 2 && !dbad; ++j)
+                if (memcmp(&dcb[(size_t)j * sc], ocb + (size_t)j * oscb, W / 2) ||
+                    memcmp(&dcr[(size_t)j * sc], ocr + (size_t)j * oscr, W / 2))
+                    dbad = 10000 + j;
+            if (dbad) { printf("frame %d: decoded picture differs (row code %d)\n", f, dbad); mismatch = 1; break; }
+            for (int i = 3; i > 0; --i) { ddpb[i] = ddpb[i - 1]; ddpb_ok[i] = ddpb_ok[i - 1]; ddpb_poc[i] = ddpb_poc[i - 1]; }
+            ddpb[0].y = dy; ddpb[0].cb = dcb; ddpb[0].cr = dcr;
+            ddpb_ok[0] = true; ddpb_poc[0] = hd.frame_num;
+        }
         for (int i = 3; i > 0; --i) { dpb[i] = dpb[i - 1]; dpb_ok[i] = dpb_ok[i - 1]; dpb_poc[i] = dpb_poc[i - 1]; }
         dpb[0].y = ry; dpb[0].cb = rcb; dpb[0].cr = rcr;
         dpb_ok[0] = true; dpb_poc[0] = f;
     }
     tc_encoder_destroy(ref);
+    tc_decoder_destroy(rdec);
     if (out_file) fclose(out_file);
     if (in_file) fclose(in_file);
-    if (!mismatch) printf("identical: %d frames, %zu bytes\n", nf, total);
+    if (!mismatch) printf("identical: %d frames, %zu bytes (encoder packets and reconstruction, decoder pictures)\n", nf, total);
     return mismatch;
 }

@@ -4,8 +4,11 @@ tests/legacy_emu.cpp compiles tcodec_b200/csrc/tcb_legacy.cuh as plain C++
 (a team of one lane) with the library's host syntax writer and links the
 reference encoder from its own sources (oracle/_ref/obj, built by
 `make -C oracle ref`).  These tests run it over a configuration matrix and
-over the reference's 72 legacy conformance streams; the GPU tests
-(test_gpu_legacy.py) then check the same source on the device.
+over the reference's 72 legacy conformance streams; in the matrix every
+reference packet is also decoded with the library's host parser
+(tcb_parse.h) and the same source's reconstruction and compared with the
+reference decoder.  The GPU tests (test_gpu_legacy.py) then check the same
+source on the device.
 """
 import glob
 import hashlib
