@@ -8,9 +8,12 @@
 // reconstruction with the reference encoder linked in from its own
 // sources.  Each reference packet is also decoded by the library's host
 // parser (tcb_parse.h) and the same device source's reconstruction
-// (decode_block) and compared with the reference decoder's picture; the
-// last packet is decoded cut short by a quarter (reads past the end of a
-// legacy frame give zero bits in both decoders).
+// (decode_block) and compared with the reference decoder's picture.  The
+// last packet of a raw Exp-Golomb stream is decoded cut short by a quarter
+// (reads past the end of a legacy frame give zero bits in both decoders);
+// range-coded packets are not cut, because on its error paths the
+// reference's coefficient decoder returns without writing the block's
+// (uninitialised) coefficient array, so its picture is not defined.
 // Usage: legacy_emu W H frames qp preset version entropy crc
 // threads profile [seed [input.yuv|- [output]]]: frames come from the
 // synthetic clip, or from a planar 4:2:0 file; `output` receives the
@@ -235,7 +238,7 @@ int main(int argc, char **argv) {
         {
             const tc_pixel_t *oy, *ocb, *ocr;
             int osy, oscb, oscr;
-            const size_t dsz = f == nf - 1 ? rp.size - rp.size / 4 : rp.size;
+            const size_t dsz = f == nf - 1 && !entropy ? rp.size - rp.size / 4 : rp.size;
             const tc_error_t rerr = tc_decoder_decode(rdec, rp.data, dsz, &oy, &osy, &ocb, &oscb, &ocr, &oscr);
             tcb::parse::Reader bs;
             bs.init(rp.data, dsz);
